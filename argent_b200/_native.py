@@ -1,0 +1,202 @@
+"""ctypes bindings of include/argent_gpu.h and include/argent_host.h.
+
+The GPU library is the product path: if it cannot be loaded the package
+raises instead of falling back to anything else.
+"""
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(_HERE, "lib")
+GPU_SO = os.path.join(LIB_DIR, "libargent_gpu.so")
+HOST_SO = os.path.join(LIB_DIR, "libargent_host.so")
+
+SPEC_LEN = 471
+NK_LEN = 95
+NO_HIT = 0xFFFFFFFF
+
+OK, E_OOM, E_INVALID, E_TIMEOUT, E_CUDA, E_OVERFLOW, E_BUSY = range(7)
+MAT_METAL, MAT_GEM, MAT_PLASTIC, MAT_OPAL, MAT_DIFFUSE, MAT_BLACK = range(6)
+GEM_TRANSPARENT, GEM_OPAL, GEM_OPAQUE = range(3)
+ENV_GRADIENT, ENV_MAP = range(2)
+FILM_KAHAN, FILM_FP64 = 1, 2
+
+c_float_p = ctypes.POINTER(ctypes.c_float)
+c_u32_p = ctypes.POINTER(ctypes.c_uint32)
+c_u16_p = ctypes.POINTER(ctypes.c_uint16)
+c_u8_p = ctypes.POINTER(ctypes.c_uint8)
+
+
+class ArgentMaterial(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32), ("gem_kind", ctypes.c_int32), ("alpha", ctypes.c_float), ("eta", ctypes.c_float),
+        ("cell_mm", ctypes.c_float), ("strength", ctypes.c_float), ("has_patina", ctypes.c_int32),
+        ("patina_strength", ctypes.c_float), ("patina_lo", ctypes.c_float), ("patina_hi", ctypes.c_float),
+        ("patina_alpha", ctypes.c_float), ("patina_eta", ctypes.c_float), ("has_opaque_base", ctypes.c_int32),
+        ("nk_eta", ctypes.c_float * NK_LEN), ("nk_k", ctypes.c_float * NK_LEN),
+        ("spec_a", ctypes.c_float * SPEC_LEN), ("spec_b", ctypes.c_float * SPEC_LEN),
+        ("spec_b2", ctypes.c_float * SPEC_LEN),
+    ]
+
+
+class ArgentPanel(ctypes.Structure):
+    _fields_ = [
+        ("center", ctypes.c_float * 3), ("hu", ctypes.c_float * 3), ("hv", ctypes.c_float * 3),
+        ("emits", ctypes.c_int32), ("camera_visible", ctypes.c_int32), ("feather", ctypes.c_float),
+        ("emission", ctypes.c_float * SPEC_LEN),
+    ]
+
+
+class ArgentEnv(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32), ("power", ctypes.c_float), ("top", ctypes.c_float * SPEC_LEN),
+        ("horizon", ctypes.c_float * SPEC_LEN), ("bottom", ctypes.c_float * SPEC_LEN), ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32), ("rgb", c_float_p), ("rotation_deg", ctypes.c_float),
+    ]
+
+
+class ArgentFloor(ctypes.Structure):
+    _fields_ = [("enabled", ctypes.c_int32), ("y", ctypes.c_float), ("material", ctypes.c_int32),
+                ("fade_start", ctypes.c_float), ("fade_end", ctypes.c_float)]
+
+
+class ArgentSceneDesc(ctypes.Structure):
+    _fields_ = [
+        ("materials", ctypes.POINTER(ArgentMaterial)), ("num_materials", ctypes.c_int32),
+        ("panels", ctypes.POINTER(ArgentPanel)), ("num_panels", ctypes.c_int32),
+        ("env", ctypes.POINTER(ArgentEnv)), ("floor", ArgentFloor), ("turntable_deg", ctypes.c_float),
+        ("has_white", ctypes.c_int32), ("white_xyz", ctypes.c_float * 3),
+    ]
+
+
+class ArgentCamera(ctypes.Structure):
+    _fields_ = [
+        ("pos", ctypes.c_float * 3), ("forward", ctypes.c_float * 3), ("right", ctypes.c_float * 3),
+        ("up", ctypes.c_float * 3), ("half_w", ctypes.c_float), ("half_h", ctypes.c_float),
+        ("lens_radius", ctypes.c_float), ("focus_dist", ctypes.c_float), ("shift", ctypes.c_float * 2),
+    ]
+
+
+class ArgentPathSettings(ctypes.Structure):
+    _fields_ = [("max_depth", ctypes.c_uint32), ("clamp_indirect", ctypes.c_float), ("rr_depth", ctypes.c_uint32)]
+
+
+class ArgentRay(ctypes.Structure):
+    _fields_ = [("o", ctypes.c_float * 3), ("tmax", ctypes.c_float), ("d", ctypes.c_float * 3),
+                ("pad", ctypes.c_float)]
+
+
+class ArgentHit(ctypes.Structure):
+    _fields_ = [("t", ctypes.c_float), ("u", ctypes.c_float), ("v", ctypes.c_float), ("prim", ctypes.c_uint32)]
+
+
+class ArgentLimits(ctypes.Structure):
+    _fields_ = [("wave_paths", ctypes.c_uint64), ("memory_budget", ctypes.c_uint64)]
+
+
+class ArgentBatchItem(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_void_p), ("camera", ArgentCamera), ("film", ctypes.c_void_p),
+                ("settings", ArgentPathSettings), ("count", ctypes.c_uint32), ("seed", ctypes.c_uint32)]
+
+
+class ArgentMesh(ctypes.Structure):
+    _fields_ = [("nv", ctypes.c_uint32), ("nt", ctypes.c_uint32), ("positions", c_float_p), ("normals", c_float_p),
+                ("tris", c_u32_p), ("tri_material", c_u16_p)]
+
+
+# name -> (restype, argtypes)
+GPU_FUNCS = {
+    "argent_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ArgentLimits), ctypes.POINTER(ctypes.c_void_p)]),
+    "argent_ctx_destroy": (None, [ctypes.c_void_p]),
+    "argent_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "argent_ctx_sync": (ctypes.c_int, [ctypes.c_void_p]),
+    "argent_ctx_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "argent_ctx_kernel_launches": (ctypes.c_uint64, [ctypes.c_void_p]),
+    "argent_piece_upload": (ctypes.c_int, [ctypes.c_void_p, c_float_p, ctypes.c_uint32, c_float_p, c_u32_p,
+                                           ctypes.c_uint32, c_u16_p, c_float_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "argent_piece_destroy": (None, [ctypes.c_void_p]),
+    "argent_piece_bounds": (ctypes.c_int, [ctypes.c_void_p, c_float_p, c_float_p]),
+    "argent_piece_device_bytes": (ctypes.c_uint64, [ctypes.c_void_p]),
+    "argent_scene_upload": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ArgentSceneDesc),
+                                           ctypes.POINTER(ctypes.c_void_p)]),
+    "argent_scene_destroy": (None, [ctypes.c_void_p]),
+    "argent_scene_set_turntable": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_float]),
+    "argent_film_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                          ctypes.POINTER(ctypes.c_void_p)]),
+    "argent_film_destroy": (None, [ctypes.c_void_p]),
+    "argent_film_clear": (ctypes.c_int, [ctypes.c_void_p]),
+    "argent_film_samples": (ctypes.c_uint32, [ctypes.c_void_p]),
+    "argent_film_read": (ctypes.c_int, [ctypes.c_void_p, c_float_p, c_float_p, c_float_p]),
+    "argent_film_read_xyz": (ctypes.c_int, [ctypes.c_void_p, c_float_p]),
+    "argent_render_pass": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ArgentCamera),
+                                          ctypes.c_void_p, ctypes.POINTER(ArgentPathSettings), ctypes.c_uint32,
+                                          ctypes.c_uint32]),
+    "argent_trace_closest": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                            ctypes.c_void_p]),
+    "argent_trace_anyhit": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                           ctypes.c_void_p]),
+    "argent_trace_closest_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                   ctypes.c_uint64, ctypes.c_void_p]),
+    "argent_trace_anyhit_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_uint64, ctypes.c_void_p]),
+    "argent_render_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ArgentBatchItem), ctypes.c_uint32]),
+}
+
+HOST_FUNCS = {
+    "argent_mesh_free": (None, [ctypes.POINTER(ArgentMesh)]),
+    "argent_synth_ring": (ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32,
+                                         ctypes.c_float, ctypes.c_float, ctypes.c_uint32, ctypes.POINTER(ArgentMesh)]),
+    "argent_synth_signet": (ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32,
+                                           ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_uint32,
+                                           ctypes.c_uint32, ctypes.POINTER(ArgentMesh)]),
+}
+
+
+def _bind(path, table, required=True):
+    if not os.path.exists(path):
+        raise OSError(f"{path} is missing: run `python -m argent_b200.build` (no CPU fallback exists)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in table.items():
+        try:
+            f = getattr(lib, name)
+        except AttributeError:
+            if required:
+                raise
+            continue
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+_gpu = None
+_host = None
+
+
+def gpu():
+    """The CUDA library (raises if it is not built)."""
+    global _gpu
+    if _gpu is None:
+        _gpu = _bind(GPU_SO, GPU_FUNCS)
+    return _gpu
+
+
+def host():
+    """The host-side scene-builder library."""
+    global _host
+    if _host is None:
+        _host = _bind(HOST_SO, HOST_FUNCS)
+    return _host
+
+
+class ArgentError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"argent error {code}: {msg}")
+        self.code = code
+
+
+def check(rc, ctx=None):
+    if rc != OK:
+        msg = gpu().argent_last_error(ctx)
+        raise ArgentError(rc, msg.decode() if msg else "")
+    return rc

@@ -1,0 +1,858 @@
+// argent_gpu.cu — the C ABI of include/argent_gpu.h: context, piece, scene,
+// film, render_pass, batch and traversal entry points.  Kernels live in the
+// device/*.cuh headers included here.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/argent_gpu.h"
+#include "data/spectral_tables.h"
+#include "device/dev_math.cuh"
+#include "device/traverse.cuh"
+#include "host/bvh_build.h"
+#include "host/scene_prep.h"
+#include "internal.cuh"
+#include "render_impl.cuh"
+
+using namespace dev;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+}  // namespace
+
+// ------------------------------------------------------------------ helpers
+
+#define ARGENT_CK(ctx, call)                                                   \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      return set_error((ctx), ARGENT_E_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    }                                                                          \
+  } while (0)
+
+int set_error(const ArgentCtx* ctx, int code, const std::string& msg) {
+  g_last_error = msg;
+  if (ctx) const_cast<ArgentCtx*>(ctx)->err = msg;
+  return code;
+}
+
+// ------------------------------------------------------------------ kernels
+
+__global__ void k_trace_closest(DevPiece pc, const ArgentRay* __restrict__ rays, uint64_t n, ArgentHit* hits,
+                                uint32_t* status) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float4* rp = reinterpret_cast<const float4*>(rays + i);
+    float4 a = __ldg(rp), b = __ldg(rp + 1);
+    TraceHit h = trace_closest(pc, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, a.w, status);
+    ArgentHit o;
+    if (h.prim == ARGENT_NO_HIT_U) {
+      o.t = 0.0f;
+      o.u = 0.0f;
+      o.v = 0.0f;
+    } else {
+      o.t = h.t;
+      o.u = h.u;
+      o.v = h.v;
+    }
+    o.prim = h.prim;
+    reinterpret_cast<float4*>(hits)[i] = make_float4(o.t, o.u, o.v, __uint_as_float(o.prim));
+  }
+}
+
+__global__ void k_trace_any(DevPiece pc, const ArgentRay* __restrict__ rays, uint64_t n, uint8_t* occ,
+                            uint32_t* status) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const float4* rp = reinterpret_cast<const float4*>(rays + i);
+    float4 a = __ldg(rp), b = __ldg(rp + 1);
+    occ[i] = trace_any(pc, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, a.w, status) ? 1 : 0;
+  }
+}
+
+// ------------------------------------------------------------------ context
+
+int ctx_check_status(ArgentCtx* ctx) {
+  uint32_t st = 0;
+  ARGENT_CK(ctx, cudaMemcpyAsync(&st, ctx->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  if (st) {
+    ARGENT_CK(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(uint32_t), ctx->stream));
+    ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    std::string m = "device status:";
+    if (st & ARGENT_STATUS_STACK_OVERFLOW) m += " traversal stack overflow;";
+    if (st & ARGENT_STATUS_QUEUE_OVERFLOW) m += " queue overflow;";
+    if (st & ARGENT_STATUS_TIMEOUT) m += " bounded wait expired;";
+    return set_error(ctx, (st & ARGENT_STATUS_TIMEOUT) ? ARGENT_E_TIMEOUT : ARGENT_E_OVERFLOW, m);
+  }
+  return ARGENT_OK;
+}
+
+int grid_for(const ArgentCtx* ctx, const void* kernel, int block, uint64_t n) {
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
+  per_sm = std::max(per_sm, 1);
+  uint64_t full = (n + block - 1) / block;
+  uint64_t g = std::min<uint64_t>(full, (uint64_t)ctx->num_sms * per_sm);
+  return (int)std::max<uint64_t>(g, 1);
+}
+
+extern "C" {
+
+const char* argent_last_error(const ArgentCtx* ctx) {
+  if (ctx) return ctx->err.c_str();
+  return g_last_error.c_str();
+}
+
+int argent_ctx_create(int device, const ArgentLimits* limits, ArgentCtx** out) {
+  if (!out) return set_error(nullptr, ARGENT_E_INVALID, "argent_ctx_create: out is NULL");
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0)
+    return set_error(nullptr, ARGENT_E_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  if (device < 0 || device >= count) return set_error(nullptr, ARGENT_E_INVALID, "device index out of range");
+  ArgentCtx* ctx = new ArgentCtx();
+  ctx->device = device;
+  if (limits) ctx->limits = *limits;
+  if (ctx->limits.wave_paths == 0) ctx->limits.wave_paths = 1ull << 21;
+  cudaError_t r = cudaSetDevice(device);
+  if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (r == cudaSuccess) r = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (r == cudaSuccess) r = cudaMalloc(&ctx->d_status, sizeof(uint32_t) * 4);
+  if (r == cudaSuccess) r = cudaMemset(ctx->d_status, 0, sizeof(uint32_t) * 4);
+  if (r != cudaSuccess) {
+    std::string m = std::string("context setup failed: ") + cudaGetErrorString(r);
+    argent_ctx_destroy(ctx);
+    return set_error(nullptr, ARGENT_E_CUDA, m);
+  }
+  if (ctx->limits.memory_budget == 0) {
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    ctx->limits.memory_budget = (uint64_t)(fr / 4 * 3);
+  }
+  *out = ctx;
+  return ARGENT_OK;
+}
+
+void argent_ctx_destroy(ArgentCtx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ctx->wave.release();
+  if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+int argent_ctx_sync(ArgentCtx* ctx) {
+  if (!ctx) return set_error(nullptr, ARGENT_E_INVALID, "ctx is NULL");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return ctx_check_status(ctx);
+}
+
+void* argent_ctx_stream(ArgentCtx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+uint64_t argent_ctx_kernel_launches(const ArgentCtx* ctx) { return ctx ? ctx->launches : 0; }
+
+// ------------------------------------------------------------------ piece
+
+void argent_piece_destroy(ArgentPiece* p) {
+  if (!p) return;
+  cudaSetDevice(p->ctx->device);
+  for (void* a : p->allocs) cudaFree(a);
+  delete p;
+}
+
+int argent_piece_upload(ArgentCtx* ctx, const float* positions, uint32_t nv, const float* normals,
+                        const uint32_t* tris, uint32_t nt, const uint16_t* tri_material, const float* cavity,
+                        ArgentPiece** out) {
+  if (!ctx || !out) return set_error(ctx, ARGENT_E_INVALID, "argent_piece_upload: NULL argument");
+  *out = nullptr;
+  if ((nv && !positions) || (nt && !tris)) return set_error(ctx, ARGENT_E_INVALID, "piece arrays are NULL");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  argent::WideBvh bvh;
+  try {
+    bvh = argent::build_wide_bvh(positions, nv, tris, nt, 0);
+  } catch (const std::exception& e) {
+    return set_error(ctx, ARGENT_E_INVALID, std::string("BVH build: ") + e.what());
+  }
+  if ((uint64_t)bvh.depth * 7 + 1 > ARGENT_STACK_SIZE)
+    return set_error(ctx, ARGENT_E_INVALID, "BVH too deep for the traversal stack");
+  ArgentPiece* p = new ArgentPiece();
+  p->ctx = ctx;
+  p->nv = nv;
+  p->nt = nt;
+  p->depth = bvh.depth;
+  for (int a = 0; a < 3; ++a) {
+    p->lo[a] = bvh.lo[a];
+    p->hi[a] = bvh.hi[a];
+  }
+  std::vector<float4> pos4(nv), nrm4;
+  for (uint32_t i = 0; i < nv; ++i) pos4[i] = make_float4(positions[3 * i], positions[3 * i + 1], positions[3 * i + 2], 0);
+  if (normals) {
+    nrm4.resize(nv);
+    for (uint32_t i = 0; i < nv; ++i) nrm4[i] = make_float4(normals[3 * i], normals[3 * i + 1], normals[3 * i + 2], 0);
+  }
+  std::vector<uint4> tidx(nt);
+  for (uint32_t i = 0; i < nt; ++i)
+    tidx[i] = make_uint4(tris[3 * i], tris[3 * i + 1], tris[3 * i + 2], tri_material ? tri_material[i] : 0u);
+  p->max_material = 0;
+  for (uint32_t i = 0; tri_material && i < nt; ++i) p->max_material = std::max<uint32_t>(p->max_material, tri_material[i]);
+  auto up = [&](const void* src, size_t bytes, void** dst) -> cudaError_t {
+    *dst = nullptr;
+    if (bytes == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(dst, bytes);
+    if (e != cudaSuccess) return e;
+    p->allocs.push_back(*dst);
+    p->bytes += bytes;
+    return cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  };
+  void *dn = nullptr, *dt = nullptr, *dp = nullptr, *dnr = nullptr, *di = nullptr, *dc = nullptr;
+  cudaError_t e = up(bvh.nodes.data(), bvh.nodes.size() * sizeof(argent::WideNode), &dn);
+  if (e == cudaSuccess) e = up(bvh.tris.data(), bvh.tris.size() * sizeof(argent::TriRecord), &dt);
+  if (e == cudaSuccess) e = up(pos4.data(), pos4.size() * sizeof(float4), &dp);
+  if (e == cudaSuccess && normals) e = up(nrm4.data(), nrm4.size() * sizeof(float4), &dnr);
+  if (e == cudaSuccess) e = up(tidx.data(), tidx.size() * sizeof(uint4), &di);
+  if (e == cudaSuccess && cavity) e = up(cavity, (size_t)nv * sizeof(float), &dc);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    std::string m = std::string("piece upload: ") + cudaGetErrorString(e);
+    argent_piece_destroy(p);
+    return set_error(ctx, e == cudaErrorMemoryAllocation ? ARGENT_E_OOM : ARGENT_E_CUDA, m);
+  }
+  p->dev.nodes = (const uint4*)dn;
+  p->dev.tris = (const float4*)dt;
+  p->dev.pos = (const float4*)dp;
+  p->dev.nrm = (const float4*)dnr;
+  p->dev.tri_idx = (const uint4*)di;
+  p->dev.cavity = (const float*)dc;
+  p->dev.num_tris = nt;
+  *out = p;
+  return ARGENT_OK;
+}
+
+int argent_piece_bounds(const ArgentPiece* p, float lo[3], float hi[3]) {
+  if (!p || !lo || !hi) return set_error(nullptr, ARGENT_E_INVALID, "argent_piece_bounds: NULL argument");
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = p->lo[a];
+    hi[a] = p->hi[a];
+  }
+  return ARGENT_OK;
+}
+
+uint64_t argent_piece_device_bytes(const ArgentPiece* p) { return p ? p->bytes : 0; }
+
+// ------------------------------------------------------------------ traversal entry points
+
+int argent_trace_closest_device(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* d_rays, uint64_t n,
+                                ArgentHit* d_hits) {
+  if (!ctx || !piece) return set_error(ctx, ARGENT_E_INVALID, "NULL argument");
+  if (n == 0) return ARGENT_OK;
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  int block = 128;
+  int grid = grid_for(ctx, (const void*)k_trace_closest, block, n);
+  k_trace_closest<<<grid, block, 0, ctx->stream>>>(piece->dev, d_rays, n, d_hits, ctx->d_status);
+  ctx->launches++;
+  ARGENT_CK(ctx, cudaGetLastError());
+  return ARGENT_OK;
+}
+
+int argent_trace_anyhit_device(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* d_rays, uint64_t n,
+                               uint8_t* d_occ) {
+  if (!ctx || !piece) return set_error(ctx, ARGENT_E_INVALID, "NULL argument");
+  if (n == 0) return ARGENT_OK;
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  int block = 128;
+  int grid = grid_for(ctx, (const void*)k_trace_any, block, n);
+  k_trace_any<<<grid, block, 0, ctx->stream>>>(piece->dev, d_rays, n, d_occ, ctx->d_status);
+  ctx->launches++;
+  ARGENT_CK(ctx, cudaGetLastError());
+  return ARGENT_OK;
+}
+
+int argent_trace_closest(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* rays, uint64_t n, ArgentHit* hits) {
+  if (!ctx || !piece || (n && (!rays || !hits))) return set_error(ctx, ARGENT_E_INVALID, "NULL argument");
+  if (n == 0) return ARGENT_OK;
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  void *dr = nullptr, *dh = nullptr;
+  ARGENT_CK(ctx, cudaMallocAsync(&dr, n * sizeof(ArgentRay), ctx->stream));
+  cudaError_t e = cudaMallocAsync(&dh, n * sizeof(ArgentHit), ctx->stream);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(dr, ctx->stream);
+    return set_error(ctx, ARGENT_E_OOM, "trace buffers");
+  }
+  e = cudaMemcpyAsync(dr, rays, n * sizeof(ArgentRay), cudaMemcpyHostToDevice, ctx->stream);
+  int rc = ARGENT_OK;
+  if (e == cudaSuccess) rc = argent_trace_closest_device(ctx, piece, (const ArgentRay*)dr, n, (ArgentHit*)dh);
+  if (e == cudaSuccess && rc == ARGENT_OK)
+    e = cudaMemcpyAsync(hits, dh, n * sizeof(ArgentHit), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaFreeAsync(dr, ctx->stream);
+  cudaFreeAsync(dh, ctx->stream);
+  cudaError_t s = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess) e = s;
+  if (rc != ARGENT_OK) return rc;
+  if (e != cudaSuccess) return set_error(ctx, ARGENT_E_CUDA, std::string("trace: ") + cudaGetErrorString(e));
+  return ctx_check_status(ctx);
+}
+
+int argent_trace_anyhit(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* rays, uint64_t n, uint8_t* occluded) {
+  if (!ctx || !piece || (n && (!rays || !occluded))) return set_error(ctx, ARGENT_E_INVALID, "NULL argument");
+  if (n == 0) return ARGENT_OK;
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  void *dr = nullptr, *dh = nullptr;
+  ARGENT_CK(ctx, cudaMallocAsync(&dr, n * sizeof(ArgentRay), ctx->stream));
+  cudaError_t e = cudaMallocAsync(&dh, n, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(dr, ctx->stream);
+    return set_error(ctx, ARGENT_E_OOM, "trace buffers");
+  }
+  e = cudaMemcpyAsync(dr, rays, n * sizeof(ArgentRay), cudaMemcpyHostToDevice, ctx->stream);
+  int rc = ARGENT_OK;
+  if (e == cudaSuccess) rc = argent_trace_anyhit_device(ctx, piece, (const ArgentRay*)dr, n, (uint8_t*)dh);
+  if (e == cudaSuccess && rc == ARGENT_OK) e = cudaMemcpyAsync(occluded, dh, n, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaFreeAsync(dr, ctx->stream);
+  cudaFreeAsync(dh, ctx->stream);
+  cudaError_t s = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess) e = s;
+  if (rc != ARGENT_OK) return rc;
+  if (e != cudaSuccess) return set_error(ctx, ARGENT_E_CUDA, std::string("trace: ") + cudaGetErrorString(e));
+  return ctx_check_status(ctx);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ device tables
+
+static int ensure_tables(ArgentCtx* ctx) {
+  if (ctx->tables_ready) return ARGENT_OK;
+  uint32_t dirs[4][32];
+  argent::sobol_directions(dirs);
+  static float energy[32 * 32];
+  static std::once_flag once;
+  std::call_once(once, [] { argent::ggx_energy_table(energy); });
+  ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_sobol_dirs, dirs, sizeof(dirs)));
+  ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_energy_table, energy, sizeof(energy)));
+  ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_cmf, ARGENT_CMF_1931_2DEG, sizeof(float) * 471 * 3));
+  ctx->tables_ready = true;
+  return ARGENT_OK;
+}
+
+static int ensure_wave(ArgentCtx* ctx) {
+  WaveBuffers& w = ctx->wave;
+  uint64_t cap = ctx->limits.wave_paths;
+  if (w.cap == cap) return ARGENT_OK;
+  w.release();
+  auto alloc = [&](void** p, size_t bytes) -> bool {
+    if (cudaMalloc(p, bytes) != cudaSuccess) return false;
+    w.allocs.push_back(*p);
+    w.bytes += bytes;
+    return true;
+  };
+  bool ok = true;
+  float4** f4[] = {&w.o, &w.d, &w.beta, &w.L, &w.lambda, &w.pdf, &w.hit, &w.albedo, &w.normal, &w.sh_o, &w.sh_d, &w.sh_c};
+  for (float4** p : f4) ok = ok && alloc((void**)p, cap * sizeof(float4));
+  ok = ok && alloc((void**)&w.meta, cap * sizeof(uint4));
+  ok = ok && alloc((void**)&w.rng, cap * sizeof(unsigned long long));
+  ok = ok && alloc((void**)&w.q0, cap * sizeof(uint32_t));
+  ok = ok && alloc((void**)&w.q1, cap * sizeof(uint32_t));
+  ok = ok && alloc((void**)&w.counters, 2 * (ARGENT_MAX_DEPTH + 2) * sizeof(uint32_t));
+  if (!ok) {
+    w.release();
+    return set_error(ctx, ARGENT_E_OOM, "wave buffers: out of device memory");
+  }
+  w.cap = cap;
+  return ARGENT_OK;
+}
+
+// ------------------------------------------------------------------ wave driver
+
+namespace {
+
+struct Chunk {
+  uint32_t job, p0, pn, s0, sn;
+};
+
+// Splits every job into (pixel range, sample range) chunks of at most
+// `cap` paths and packs them, in order, into waves.
+std::vector<dev::WaveDesc> plan_waves(const std::vector<dev::DevJob>& jobs, const std::vector<uint32_t>& counts,
+                                      uint64_t cap, std::vector<uint32_t>* wave_depth) {
+  std::vector<dev::WaveDesc> waves;
+  dev::WaveDesc cur{};
+  uint32_t cur_depth = 0;
+  auto flush = [&]() {
+    if (cur.num_segments) {
+      waves.push_back(cur);
+      wave_depth->push_back(cur_depth);
+    }
+    cur = dev::WaveDesc{};
+    cur_depth = 0;
+  };
+  for (uint32_t j = 0; j < jobs.size(); ++j) {
+    uint32_t P = jobs[j].w * jobs[j].h;
+    uint32_t count = counts[j];
+    if (P == 0 || count == 0) continue;
+    uint32_t pn_max = (uint32_t)std::min<uint64_t>(P, cap);
+    for (uint32_t p0 = 0; p0 < P; p0 += pn_max) {
+      uint32_t pn = std::min(pn_max, P - p0);
+      uint32_t s0 = 0;
+      while (s0 < count) {
+        uint64_t room = cap - cur.num_slots;
+        if (room < pn || cur.num_segments == ARGENT_MAX_SEGMENTS) {
+          flush();
+          room = cap;
+        }
+        uint32_t sn = (uint32_t)std::min<uint64_t>(count - s0, room / pn);
+        dev::DevSegment& sg = cur.seg[cur.num_segments++];
+        sg.slot_begin = cur.num_slots;
+        sg.job = j;
+        sg.p0 = p0;
+        sg.pn = pn;
+        sg.s0 = s0;
+        sg.sn = sn;
+        cur.num_slots += pn * sn;
+        cur_depth = std::max(cur_depth, jobs[j].max_depth);
+        s0 += sn;
+      }
+    }
+  }
+  flush();
+  return waves;
+}
+
+}  // namespace
+
+static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const std::vector<uint32_t>& counts) {
+  int rc = ensure_tables(ctx);
+  if (rc != ARGENT_OK) return rc;
+  rc = ensure_wave(ctx);
+  if (rc != ARGENT_OK) return rc;
+  WaveBuffers& wb = ctx->wave;
+  std::vector<uint32_t> depths;
+  std::vector<dev::WaveDesc> waves = plan_waves(jobs, counts, wb.cap, &depths);
+  if (waves.empty()) return ARGENT_OK;
+  dev::DevJob* d_jobs = nullptr;
+  ARGENT_CK(ctx, cudaMallocAsync((void**)&d_jobs, jobs.size() * sizeof(dev::DevJob), ctx->stream));
+  // Pageable source: the call returns once the bytes are staged.
+  ARGENT_CK(ctx, cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(dev::DevJob), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+  dev::WaveArgs a{};
+  a.jobs = d_jobs;
+  a.o = wb.o;
+  a.d = wb.d;
+  a.beta = wb.beta;
+  a.L = wb.L;
+  a.lambda = wb.lambda;
+  a.pdf = wb.pdf;
+  a.hit = wb.hit;
+  a.albedo = wb.albedo;
+  a.normal = wb.normal;
+  a.sh_o = wb.sh_o;
+  a.sh_d = wb.sh_d;
+  a.sh_c = wb.sh_c;
+  a.meta = wb.meta;
+  a.rng = wb.rng;
+  a.counters = wb.counters;
+  a.status = ctx->d_status;
+  uint32_t cap = (uint32_t)wb.cap;
+  int g_ray = grid_for(ctx, (const void*)dev::k_raygen, 256, cap);
+  int g_int = grid_for(ctx, (const void*)dev::k_intersect, 128, cap);
+  int g_sh = grid_for(ctx, (const void*)dev::k_shade, 128, cap);
+  int g_any = grid_for(ctx, (const void*)dev::k_shadow, 128, cap);
+  int g_film = grid_for(ctx, (const void*)dev::k_film, 256, cap);
+  for (size_t wi = 0; wi < waves.size(); ++wi) {
+    const dev::WaveDesc& w = waves[wi];
+    a.q_in = wb.q0;
+    a.q_out = wb.q1;
+    dev::k_raygen<<<g_ray, 256, 0, ctx->stream>>>(a, w);
+    ctx->launches++;
+    for (uint32_t depth = 0; depth < depths[wi] && depth < ARGENT_MAX_DEPTH; ++depth) {
+      a.q_in = (depth & 1) ? wb.q1 : wb.q0;
+      a.q_out = (depth & 1) ? wb.q0 : wb.q1;
+      dev::k_intersect<<<g_int, 128, 0, ctx->stream>>>(a, (int)depth);
+      dev::k_shade<<<g_sh, 128, 0, ctx->stream>>>(a, (int)depth, cap);
+      dev::k_shadow<<<g_any, 128, 0, ctx->stream>>>(a, (int)depth);
+      ctx->launches += 3;
+    }
+    dev::k_film<<<g_film, 256, 0, ctx->stream>>>(a, w);
+    ctx->launches++;
+  }
+  cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(d_jobs, ctx->stream);
+  if (e != cudaSuccess) return set_error(ctx, ARGENT_E_CUDA, std::string("render launch: ") + cudaGetErrorString(e));
+  return ARGENT_OK;
+}
+
+extern "C" {
+
+// ------------------------------------------------------------------ scene
+
+void argent_scene_destroy(ArgentScene* s) {
+  if (!s) return;
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->ctx->stream);
+  for (void* a : s->allocs) cudaFree(a);
+  delete s;
+}
+
+static void set_turn(dev::DevScene& h, float deg) {
+  h.has_turn = deg != 0.0f ? 1 : 0;
+  float r_obj = (-deg) * (3.14159265358979323846f / 180.0f);
+  float r_w = deg * (3.14159265358979323846f / 180.0f);
+  h.to_obj_s = std::sin(r_obj);
+  h.to_obj_c = std::cos(r_obj);
+  h.to_world_s = std::sin(r_w);
+  h.to_world_c = std::cos(r_w);
+}
+
+int argent_scene_upload(ArgentCtx* ctx, ArgentPiece* piece, const ArgentSceneDesc* desc, ArgentScene** out) {
+  if (!ctx || !piece || !desc || !out) return set_error(ctx, ARGENT_E_INVALID, "argent_scene_upload: NULL argument");
+  *out = nullptr;
+  if (desc->num_materials <= 0 || !desc->materials)
+    return set_error(ctx, ARGENT_E_INVALID, "a scene needs at least one material");
+  if (desc->num_materials > 65535) return set_error(ctx, ARGENT_E_INVALID, "too many materials");
+  if (piece->max_material >= (uint32_t)desc->num_materials)
+    return set_error(ctx, ARGENT_E_INVALID, "tri_material refers past the material list");
+  if (desc->num_materials > 254) return set_error(ctx, ARGENT_E_INVALID, "at most 254 materials per scene");
+  if (desc->num_panels < 0 || desc->num_panels > ARGENT_MAX_PANELS)
+    return set_error(ctx, ARGENT_E_INVALID, "at most 16 panels per scene");
+  if (desc->num_panels > 0 && !desc->panels) return set_error(ctx, ARGENT_E_INVALID, "panels is NULL");
+  if (desc->floor.enabled && (desc->floor.material < 0 || desc->floor.material >= desc->num_materials))
+    return set_error(ctx, ARGENT_E_INVALID, "floor material out of range");
+  for (int i = 0; i < desc->num_materials; ++i) {
+    const ArgentMaterial& m = desc->materials[i];
+    if (m.kind < ARGENT_MAT_METAL || m.kind > ARGENT_MAT_BLACK)
+      return set_error(ctx, ARGENT_E_INVALID, "unknown material kind");
+    if (m.kind == ARGENT_MAT_OPAL && !(m.cell_mm > 0.0f))
+      return set_error(ctx, ARGENT_E_INVALID, "opal cell size must be positive");
+  }
+  const ArgentEnv* env = desc->env;
+  bool is_map = env && env->kind == ARGENT_ENV_MAP;
+  if (is_map && (env->width <= 0 || env->height <= 0 || !env->rgb))
+    return set_error(ctx, ARGENT_E_INVALID, "environment map needs width, height and texels");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  ArgentScene* s = new ArgentScene();
+  s->ctx = ctx;
+  s->piece = piece;
+  dev::DevScene& h = s->host;
+  std::memset(&h, 0, sizeof(h));
+  h.piece = piece->dev;
+  auto up = [&](const void* src, size_t bytes) -> void* {
+    void* d = nullptr;
+    if (cudaMalloc(&d, bytes) != cudaSuccess) return nullptr;
+    s->allocs.push_back(d);
+    s->bytes += bytes;
+    if (cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
+    return d;
+  };
+  bool ok = true;
+  h.mats = (const ArgentMaterial*)up(desc->materials, sizeof(ArgentMaterial) * desc->num_materials);
+  ok = ok && h.mats;
+  h.num_mats = desc->num_materials;
+  h.num_panels = desc->num_panels;
+  for (int i = 0; ok && i < desc->num_panels; ++i) {
+    const ArgentPanel& p = desc->panels[i];
+    dev::DevPanel& dp = h.panels[i];
+    for (int a = 0; a < 3; ++a) {
+      dp.c[a] = p.center[a];
+      dp.hu[a] = p.hu[a];
+      dp.hv[a] = p.hv[a];
+    }
+    argent::panel_frame(p, dp.n, &dp.area, &dp.hu_l2, &dp.hv_l2);
+    dp.feather = p.feather;
+    dp.emits = p.emits ? 1 : 0;
+    dp.camera_visible = p.camera_visible ? 1 : 0;
+    dp.emission = p.emits ? (const float*)up(p.emission, sizeof(float) * ARGENT_SPEC_LEN) : nullptr;
+    ok = ok && (!p.emits || dp.emission);
+  }
+  argent::LightTable lt = argent::build_lights(*desc);
+  h.num_lights = (int)lt.lights.size();
+  for (size_t i = 0; i < lt.lights.size(); ++i) {
+    h.lights[i] = lt.lights[i];
+    h.light_cdf[i] = lt.cdf[i];
+  }
+  h.env_pick = lt.env_pick;
+  static const float zeros[ARGENT_SPEC_LEN] = {0};
+  if (is_map) {
+    argent::EnvTables et = argent::build_env(env->rgb, env->width, env->height);
+    float basis[3][471], inv[3][3];
+    argent::linear_rgb(basis, inv);
+    h.env_is_map = 1;
+    h.map_w = env->width;
+    h.map_h = env->height;
+    h.map_weights = (const float*)up(et.weights.data(), et.weights.size() * sizeof(float));
+    h.map_cond = (const float*)up(et.conditional.data(), et.conditional.size() * sizeof(float));
+    h.map_marg = (const float*)up(et.marginal.data(), et.marginal.size() * sizeof(float));
+    h.lin_basis = (const float*)up(basis, sizeof(basis));
+    ok = ok && h.map_weights && h.map_cond && h.map_marg && h.lin_basis;
+    float r_l = (-env->rotation_deg) * (3.14159265358979323846f / 180.0f);
+    float r_w = env->rotation_deg * (3.14159265358979323846f / 180.0f);
+    h.map_to_local_s = std::sin(r_l);
+    h.map_to_local_c = std::cos(r_l);
+    h.map_to_world_s = std::sin(r_w);
+    h.map_to_world_c = std::cos(r_w);
+  } else {
+    h.env_is_map = 0;
+    h.env_power = env ? env->power : 1.0f;
+    h.env_top = (const float*)up(env ? env->top : zeros, sizeof(float) * ARGENT_SPEC_LEN);
+    h.env_horizon = (const float*)up(env ? env->horizon : zeros, sizeof(float) * ARGENT_SPEC_LEN);
+    h.env_bottom = (const float*)up(env ? env->bottom : zeros, sizeof(float) * ARGENT_SPEC_LEN);
+    ok = ok && h.env_top && h.env_horizon && h.env_bottom;
+  }
+  h.floor_enabled = desc->floor.enabled ? 1 : 0;
+  h.floor_y = desc->floor.y;
+  h.floor_material = desc->floor.material;
+  h.fade_start = desc->floor.fade_start;
+  h.fade_end = desc->floor.fade_end;
+  set_turn(h, desc->turntable_deg);
+  argent::camera_matrix(desc->has_white != 0, desc->white_xyz, h.cam_m);
+  std::memcpy(s->cam_m, h.cam_m, sizeof(s->cam_m));
+  if (ok) {
+    s->d_scene = (dev::DevScene*)up(&h, sizeof(h));
+    ok = s->d_scene != nullptr;
+  }
+  if (!ok) {
+    argent_scene_destroy(s);
+    return set_error(ctx, ARGENT_E_OOM, "scene upload: out of device memory");
+  }
+  *out = s;
+  return ARGENT_OK;
+}
+
+int argent_scene_set_turntable(ArgentScene* s, float deg) {
+  if (!s) return set_error(nullptr, ARGENT_E_INVALID, "scene is NULL");
+  ArgentCtx* ctx = s->ctx;
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  set_turn(s->host, deg);
+  // Stream-ordered: renders already queued keep their angle.
+  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  ARGENT_CK(ctx, cudaMemcpy(s->d_scene, &s->host, sizeof(dev::DevScene), cudaMemcpyHostToDevice));
+  return ARGENT_OK;
+}
+
+// ------------------------------------------------------------------ film
+
+void argent_film_destroy(ArgentFilm* f) {
+  if (!f) return;
+  cudaSetDevice(f->ctx->device);
+  cudaStreamSynchronize(f->ctx->stream);
+  cudaFree(f->xyz);
+  cudaFree(f->comp);
+  cudaFree(f->xyz64);
+  cudaFree(f->albedo);
+  cudaFree(f->normal);
+  delete f;
+}
+
+int argent_film_create(ArgentCtx* ctx, uint32_t width, uint32_t height, uint32_t flags, ArgentFilm** out) {
+  if (!ctx || !out) return set_error(ctx, ARGENT_E_INVALID, "argent_film_create: NULL argument");
+  *out = nullptr;
+  if (width == 0 || height == 0 || (uint64_t)width * height > (1ull << 31))
+    return set_error(ctx, ARGENT_E_INVALID, "film size out of range");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  if (flags == 0) flags = ARGENT_FILM_KAHAN;
+  ArgentFilm* f = new ArgentFilm();
+  f->ctx = ctx;
+  f->w = width;
+  f->h = height;
+  f->flags = flags;
+  size_t n = 3ull * width * height;
+  bool ok = cudaMalloc(&f->xyz, n * sizeof(float)) == cudaSuccess;
+  ok = ok && cudaMalloc(&f->albedo, n * sizeof(float)) == cudaSuccess;
+  ok = ok && cudaMalloc(&f->normal, n * sizeof(float)) == cudaSuccess;
+  if (ok && (flags & ARGENT_FILM_KAHAN)) ok = cudaMalloc(&f->comp, n * sizeof(float)) == cudaSuccess;
+  if (ok && (flags & ARGENT_FILM_FP64)) ok = cudaMalloc(&f->xyz64, n * sizeof(double)) == cudaSuccess;
+  if (!ok) {
+    argent_film_destroy(f);
+    return set_error(ctx, ARGENT_E_OOM, "film: out of device memory");
+  }
+  f->bytes = n * (3 * sizeof(float) + ((flags & ARGENT_FILM_KAHAN) ? 4 : 0) + ((flags & ARGENT_FILM_FP64) ? 8 : 0));
+  int rc = argent_film_clear(f);
+  if (rc != ARGENT_OK) {
+    argent_film_destroy(f);
+    return rc;
+  }
+  *out = f;
+  return ARGENT_OK;
+}
+
+int argent_film_clear(ArgentFilm* f) {
+  if (!f) return set_error(nullptr, ARGENT_E_INVALID, "film is NULL");
+  ArgentCtx* ctx = f->ctx;
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  size_t n = 3ull * f->w * f->h;
+  ARGENT_CK(ctx, cudaMemsetAsync(f->xyz, 0, n * sizeof(float), ctx->stream));
+  ARGENT_CK(ctx, cudaMemsetAsync(f->albedo, 0, n * sizeof(float), ctx->stream));
+  ARGENT_CK(ctx, cudaMemsetAsync(f->normal, 0, n * sizeof(float), ctx->stream));
+  if (f->comp) ARGENT_CK(ctx, cudaMemsetAsync(f->comp, 0, n * sizeof(float), ctx->stream));
+  if (f->xyz64) ARGENT_CK(ctx, cudaMemsetAsync(f->xyz64, 0, n * sizeof(double), ctx->stream));
+  f->samples = 0;
+  f->has_matrix = false;
+  return ARGENT_OK;
+}
+
+uint32_t argent_film_samples(const ArgentFilm* f) { return f ? f->samples : 0; }
+
+static int film_fetch_xyz(ArgentFilm* f, std::vector<double>& xyz) {
+  ArgentCtx* ctx = f->ctx;
+  size_t n = 3ull * f->w * f->h;
+  xyz.assign(n, 0.0);
+  if (f->xyz64) {
+    ARGENT_CK(ctx, cudaMemcpyAsync(xyz.data(), f->xyz64, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  } else {
+    std::vector<float> tmp(n);
+    ARGENT_CK(ctx, cudaMemcpyAsync(tmp.data(), f->xyz, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 0; i < n; ++i) xyz[i] = tmp[i];
+  }
+  return ctx_check_status(ctx);
+}
+
+int argent_film_read_xyz(ArgentFilm* f, float* out) {
+  if (!f || !out) return set_error(f ? f->ctx : nullptr, ARGENT_E_INVALID, "NULL argument");
+  ARGENT_CK(f->ctx, cudaSetDevice(f->ctx->device));
+  std::vector<double> xyz;
+  int rc = film_fetch_xyz(f, xyz);
+  if (rc != ARGENT_OK) return rc;
+  double k = 1.0 / (double)std::max<uint32_t>(f->samples, 1);
+  for (size_t i = 0; i < xyz.size(); ++i) out[i] = (float)(xyz[i] * k);
+  return ARGENT_OK;
+}
+
+// render.rs:36-62: averages; color is the camera matrix applied to XYZ.
+int argent_film_read(ArgentFilm* f, float* color, float* albedo, float* normal) {
+  if (!f) return set_error(nullptr, ARGENT_E_INVALID, "film is NULL");
+  ArgentCtx* ctx = f->ctx;
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  size_t np = (size_t)f->w * f->h;
+  float k = 1.0f / (float)std::max<uint32_t>(f->samples, 1);
+  if (color) {
+    std::vector<double> xyz;
+    int rc = film_fetch_xyz(f, xyz);
+    if (rc != ARGENT_OK) return rc;
+    float m[9];
+    if (f->has_matrix)
+      std::memcpy(m, f->cam_m, sizeof(m));
+    else
+      argent::camera_matrix(false, nullptr, m);
+    for (size_t i = 0; i < np; ++i) {
+      float x = (float)xyz[3 * i], y = (float)xyz[3 * i + 1], z = (float)xyz[3 * i + 2];
+      for (int c = 0; c < 3; ++c) color[3 * i + c] = (m[3 * c] * x + m[3 * c + 1] * y + m[3 * c + 2] * z) * k;
+    }
+  }
+  if (albedo) {
+    ARGENT_CK(ctx, cudaMemcpyAsync(albedo, f->albedo, 3 * np * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  std::vector<float> nrm;
+  if (normal) {
+    nrm.resize(3 * np);
+    ARGENT_CK(ctx, cudaMemcpyAsync(nrm.data(), f->normal, 3 * np * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  if (albedo)
+    for (size_t i = 0; i < 3 * np; ++i) albedo[i] *= k;
+  if (normal) {
+    for (size_t i = 0; i < np; ++i) {
+      float v[3] = {nrm[3 * i] * k, nrm[3 * i + 1] * k, nrm[3 * i + 2] * k};
+      float l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      for (int c = 0; c < 3; ++c) normal[3 * i + c] = l > 1e-6f ? v[c] / l : 0.0f;
+    }
+  }
+  return ctx_check_status(ctx);
+}
+
+// ------------------------------------------------------------------ render
+
+static int make_job(ArgentScene* scene, const ArgentCamera* cam, ArgentFilm* film, const ArgentPathSettings* ps,
+                    uint32_t seed, dev::DevJob* j) {
+  ArgentCtx* ctx = scene->ctx;
+  if (film->ctx != ctx) return set_error(ctx, ARGENT_E_INVALID, "film belongs to another context");
+  if (ps->max_depth > ARGENT_MAX_DEPTH) return set_error(ctx, ARGENT_E_INVALID, "max_depth above 64");
+  if (film->has_matrix && std::memcmp(film->cam_m, scene->cam_m, sizeof(film->cam_m)) != 0)
+    return set_error(ctx, ARGENT_E_INVALID, "film already holds samples under a different white balance");
+  std::memset(j, 0, sizeof(*j));
+  j->scene = scene->d_scene;
+  j->cam = *cam;
+  j->w = film->w;
+  j->h = film->h;
+  j->first = film->samples;
+  uint32_t x = seed ^ 0xa511e9b3u;  // render.rs:73
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  j->seed_h = x;
+  j->max_depth = ps->max_depth;
+  j->rr_depth = ps->rr_depth;
+  j->clamp_indirect = ps->clamp_indirect;
+  j->film_xyz = film->xyz;
+  j->film_comp = film->comp;
+  j->film_xyz64 = film->xyz64;
+  j->film_albedo = film->albedo;
+  j->film_normal = film->normal;
+  return ARGENT_OK;
+}
+
+int argent_render_pass(ArgentCtx* ctx, ArgentScene* scene, const ArgentCamera* camera, ArgentFilm* film,
+                       const ArgentPathSettings* settings, uint32_t count, uint32_t seed) {
+  if (!ctx || !scene || !camera || !film || !settings)
+    return set_error(ctx, ARGENT_E_INVALID, "argent_render_pass: NULL argument");
+  if (scene->ctx != ctx) return set_error(ctx, ARGENT_E_INVALID, "scene belongs to another context");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  if ((uint64_t)film->samples + count > 0xffffffffull) return set_error(ctx, ARGENT_E_INVALID, "sample index overflow");
+  std::vector<dev::DevJob> jobs(1);
+  int rc = make_job(scene, camera, film, settings, seed, &jobs[0]);
+  if (rc != ARGENT_OK) return rc;
+  std::vector<uint32_t> counts{count};
+  rc = run_jobs(ctx, jobs, counts);
+  if (rc != ARGENT_OK) return rc;
+  film->samples += count;
+  film->has_matrix = true;
+  std::memcpy(film->cam_m, scene->cam_m, sizeof(film->cam_m));
+  return ARGENT_OK;
+}
+
+int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n) {
+  if (!ctx || (n && !items)) return set_error(ctx, ARGENT_E_INVALID, "argent_render_batch: NULL argument");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  std::vector<dev::DevJob> jobs(n);
+  std::vector<uint32_t> counts(n);
+  // Items that share a film run one after another: the second starts where
+  // the first leaves film.samples.
+  std::vector<uint32_t> pending(n, 0);
+  for (uint32_t i = 0; i < n; ++i) {
+    const ArgentBatchItem& it = items[i];
+    if (!it.scene || !it.film) return set_error(ctx, ARGENT_E_INVALID, "batch item without scene or film");
+    if (it.scene->ctx != ctx) return set_error(ctx, ARGENT_E_INVALID, "scene belongs to another context");
+    uint32_t base = it.film->samples;
+    for (uint32_t k = 0; k < i; ++k)
+      if (items[k].film == it.film) base += items[k].count;
+    int rc = make_job(it.scene, &it.camera, it.film, &it.settings, it.seed, &jobs[i]);
+    if (rc != ARGENT_OK) return rc;
+    for (uint32_t k = 0; k < i; ++k)
+      if (items[k].film == it.film && std::memcmp(items[k].scene->cam_m, it.scene->cam_m, sizeof(float) * 9) != 0)
+        return set_error(ctx, ARGENT_E_INVALID, "batch items share a film under different white balances");
+    jobs[i].first = base;
+    counts[i] = it.count;
+  }
+  int rc = run_jobs(ctx, jobs, counts);
+  if (rc != ARGENT_OK) return rc;
+  for (uint32_t i = 0; i < n; ++i) {
+    items[i].film->samples += items[i].count;
+    items[i].film->has_matrix = true;
+    std::memcpy(items[i].film->cam_m, items[i].scene->cam_m, sizeof(float) * 9);
+  }
+  return ARGENT_OK;
+}
+
+}  // extern "C"

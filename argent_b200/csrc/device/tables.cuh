@@ -1,0 +1,16 @@
+// tables.cuh — device-resident lookup tables, filled by the host at context
+// creation with cudaMemcpyToSymbol (the library is one translation unit, so
+// the definitions live here rather than behind extern declarations).
+#pragma once
+#include <cstdint>
+
+namespace dev {
+
+// Sobol direction numbers of the sampler's four dimensions, [dim][bit].
+__device__ uint32_t d_sobol_dirs[4][32];
+// GGX single-scattering albedo E(mu, sqrt(alpha)), 32 x 32 (microfacet.rs:93-140).
+__device__ float d_energy_table[32 * 32];
+// CIE 1931 2-degree colour matching functions, 1 nm, 360..=830 (cie.rs:38-49).
+__device__ float d_cmf[471 * 3];
+
+}  // namespace dev

@@ -1,0 +1,163 @@
+// internal.cuh — the objects behind the opaque handles of argent_gpu.h and
+// the device-side scene, job and wave descriptors.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/argent_gpu.h"
+#include "device/traverse.cuh"
+
+// Status bits (device status word) beyond the traversal ones.
+#define ARGENT_STATUS_QUEUE_OVERFLOW 2u
+#define ARGENT_STATUS_TIMEOUT 4u
+
+#define ARGENT_MAX_PANELS 16
+#define ARGENT_MAX_DEPTH 64
+
+namespace dev {
+
+struct DevPanel {
+  float c[3], hu[3], hv[3], n[3];
+  float area, feather, hu_l2, hv_l2;
+  int32_t emits, camera_visible;
+  const float* emission;  // 471-entry table
+};
+
+// Everything a path needs from its scene, in device memory.
+struct DevScene {
+  DevPiece piece;
+  const ArgentMaterial* mats;
+  int32_t num_mats;
+  int32_t num_panels;
+  DevPanel panels[ARGENT_MAX_PANELS];
+  int32_t num_lights;
+  int32_t lights[ARGENT_MAX_PANELS];
+  float light_cdf[ARGENT_MAX_PANELS];
+  float env_pick;
+  // environment
+  int32_t env_is_map;
+  float env_power;
+  const float* env_top;
+  const float* env_horizon;
+  const float* env_bottom;
+  int32_t map_w, map_h;
+  const float* map_weights;  // 3 per texel
+  const float* map_cond;     // (w+1) per row
+  const float* map_marg;     // h+1
+  const float* lin_basis;    // 3 x 471
+  float map_to_local_s, map_to_local_c;  // rot_y(-rotation)
+  float map_to_world_s, map_to_world_c;  // rot_y(+rotation)
+  // floor
+  int32_t floor_enabled;
+  float floor_y;
+  int32_t floor_material;
+  float fade_start, fade_end;
+  // turntable
+  int32_t has_turn;
+  float to_obj_s, to_obj_c;      // rot_y(-turn)
+  float to_world_s, to_world_c;  // rot_y(+turn)
+  float cam_m[9];
+};
+
+// One render_pass worth of work.
+struct DevJob {
+  const DevScene* scene;
+  ArgentCamera cam;
+  uint32_t w, h;
+  uint32_t first;   // film.samples before this pass
+  uint32_t seed_h;  // hash32(seed ^ 0xa511e9b3)
+  uint32_t max_depth, rr_depth;
+  float clamp_indirect;
+  float* film_xyz;       // 3 per pixel
+  float* film_comp;      // Kahan compensation, 3 per pixel (or null)
+  double* film_xyz64;    // FP64 sums (or null)
+  float* film_albedo;    // 3 per pixel
+  float* film_normal;    // 3 per pixel
+};
+
+// A contiguous run of path slots in a wave: pixels [p0, p0+pn) of job
+// `job`, samples first+s0 .. first+s0+sn-1; slot = slot_begin + k*pn + p.
+struct DevSegment {
+  uint32_t slot_begin, job, p0, pn, s0, sn;
+};
+
+#define ARGENT_MAX_SEGMENTS 64
+struct WaveDesc {
+  uint32_t num_segments;
+  uint32_t num_slots;
+  DevSegment seg[ARGENT_MAX_SEGMENTS];
+};
+
+}  // namespace dev
+
+// Path state of one wave, structure of arrays (capacity = wave_paths).
+struct WaveBuffers {
+  uint64_t cap = 0;
+  float4 *o = nullptr, *d = nullptr, *beta = nullptr, *L = nullptr, *lambda = nullptr, *pdf = nullptr;
+  float4 *hit = nullptr, *albedo = nullptr, *normal = nullptr;
+  float4 *sh_o = nullptr, *sh_d = nullptr, *sh_c = nullptr;
+  uint4* meta = nullptr;
+  unsigned long long* rng = nullptr;
+  uint32_t *q0 = nullptr, *q1 = nullptr, *qs = nullptr;
+  uint32_t* counters = nullptr;  // [2 * (ARGENT_MAX_DEPTH + 2)]
+  std::vector<void*> allocs;
+  uint64_t bytes = 0;
+  void release() {
+    for (void* a : allocs) cudaFree(a);
+    allocs.clear();
+    cap = 0;
+    bytes = 0;
+  }
+};
+
+struct ArgentCtx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  ArgentLimits limits{};
+  std::string err;
+  uint64_t launches = 0;
+  uint32_t* d_status = nullptr;
+  bool tables_ready = false;
+  WaveBuffers wave;
+};
+
+struct ArgentPiece {
+  ArgentCtx* ctx = nullptr;
+  dev::DevPiece dev{};
+  std::vector<void*> allocs;
+  uint64_t bytes = 0;
+  uint32_t nv = 0, nt = 0, depth = 0, max_material = 0;
+  float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+};
+
+struct ArgentScene {
+  ArgentCtx* ctx = nullptr;
+  ArgentPiece* piece = nullptr;
+  dev::DevScene host{};           // host copy of the device descriptor
+  dev::DevScene* d_scene = nullptr;
+  std::vector<void*> allocs;
+  uint64_t bytes = 0;
+  float cam_m[9];
+};
+
+struct ArgentFilm {
+  ArgentCtx* ctx = nullptr;
+  uint32_t w = 0, h = 0, flags = 0;
+  uint32_t samples = 0;
+  float* xyz = nullptr;
+  float* comp = nullptr;
+  double* xyz64 = nullptr;
+  float* albedo = nullptr;
+  float* normal = nullptr;
+  bool has_matrix = false;
+  float cam_m[9];
+  uint64_t bytes = 0;
+};
+
+int set_error(const ArgentCtx* ctx, int code, const std::string& msg);
+int ctx_check_status(ArgentCtx* ctx);
+int grid_for(const ArgentCtx* ctx, const void* kernel, int block, uint64_t n);

@@ -1,0 +1,769 @@
+// render_impl.cuh — the wavefront path tracer.
+//
+// argent renders one path per (pixel, sample) with a recursive-free bounce
+// loop (integrator.rs:50-221) called from a rayon row loop
+// (render.rs:67-115).  Here a wave of up to `wave_paths` paths advances one
+// bounce at a time through four kernels:
+//   k_intersect  closest hit: piece BVH (object space), panels, floor
+//   k_shade      emission + MIS, BSDF, next-event sample, continuation, RR;
+//                survivors and shadow rays are appended to queues by warp
+//                ballot + one atomic per warp
+//   k_shadow     any-hit of the piece BVH for the shadow queue; unoccluded
+//                rays add their (already clamped) contribution to L
+//   k_film       per pixel: XYZ of each finished sample, non-finite samples
+//                dropped, FP32 Kahan (or FP64) accumulation into the film
+// k_raygen starts a wave.  Each path keeps its PCG state between kernels, so
+// the dimension stream is the one argent's single-threaded loop would draw.
+#pragma once
+#include "device/bsdf.cuh"
+#include "device/sampler.cuh"
+#include "device/spectral.cuh"
+#include "device/traverse.cuh"
+#include "host/scene_prep.h"
+#include "internal.cuh"
+
+namespace dev {
+
+// Hit record encoding (w component of the hit float4).
+#define HIT_MISS 0xFFFFFFFFu
+#define HIT_FLOOR 0xFFFFFFFEu
+#define HIT_PANEL 0xF0000000u
+
+// ---------------------------------------------------------------- lights
+
+// light.rs:50-63
+__device__ __forceinline__ bool panel_intersect(const DevPanel& p, V3 o, V3 d, float t_max, float* t_out) {
+  V3 n = ld3(p.n);
+  float denom = dot(d, n);
+  if (fabsf(denom) < 1e-9f) return false;
+  float t = dot(ld3(p.c) - o, n) / denom;
+  if (t <= 1e-6f || t >= t_max) return false;
+  V3 q = (o + d * t) - ld3(p.c);
+  float a = dot(q, ld3(p.hu)) / p.hu_l2;
+  float b = dot(q, ld3(p.hv)) / p.hv_l2;
+  if (fabsf(a) <= 1.0f && fabsf(b) <= 1.0f) {
+    *t_out = t;
+    return true;
+  }
+  return false;
+}
+// light.rs:76-93
+__device__ __forceinline__ float panel_profile(const DevPanel& p, V3 x) {
+  if (p.feather <= 0.0f) return 1.0f;
+  V3 q = x - ld3(p.c);
+  float a = fminf(fabsf(dot(q, ld3(p.hu)) / p.hu_l2), 1.0f);
+  float b = fminf(fabsf(dot(q, ld3(p.hv)) / p.hv_l2), 1.0f);
+  float start = 1.0f - p.feather;
+  float fa = 1.0f, fb = 1.0f;
+  if (a > start) {
+    float t = (a - start) / p.feather;
+    fa = 1.0f - 0.75f * t * t * (3.0f - 2.0f * t);
+  }
+  if (b > start) {
+    float t = (b - start) / p.feather;
+    fb = 1.0f - 0.75f * t * t * (3.0f - 2.0f * t);
+  }
+  return fa * fb;
+}
+// light.rs:67-72
+__device__ __forceinline__ Spec panel_le(const DevPanel& p, V3 x, V3 dir, const Wavelengths& wl) {
+  if (p.emits && dot(dir, ld3(p.n)) < 0.0f) return tab_sample(p.emission, wl) * panel_profile(p, x);
+  return spec(0.0f);
+}
+// light.rs:142-148
+__device__ __forceinline__ bool floor_intersect(const DevScene* sc, V3 o, V3 d, float t_max, float* t_out) {
+  if (fabsf(d.y) < 1e-9f) return false;
+  float t = (sc->floor_y - o.y) / d.y;
+  if (t > 1e-5f && t < t_max) {
+    *t_out = t;
+    return true;
+  }
+  return false;
+}
+// light.rs:152-162
+__device__ __forceinline__ float floor_presence(const DevScene* sc, V3 p) {
+  float r = sqrtf(p.x * p.x + p.z * p.z);
+  if (r <= sc->fade_start) return 1.0f;
+  if (r >= sc->fade_end) return 0.0f;
+  float t = (r - sc->fade_start) / (sc->fade_end - sc->fade_start);
+  return 1.0f - t * t * (3.0f - 2.0f * t);
+}
+
+// ---------------------------------------------------------------- environment (envmap.rs)
+__device__ __forceinline__ void env_uv(const DevScene* sc, V3 dir, float* u, float* v) {
+  V3 d = rot_y_sc(dir, sc->map_to_local_s, sc->map_to_local_c);
+  float uu = 0.5f + atan2f(d.x, -d.z) / (2.0f * ARGENT_PI_F);
+  *v = acosf(rclamp(d.y, -1.0f, 1.0f)) / ARGENT_PI_F;
+  float r = fmodf(uu, 1.0f);
+  if (r < 0.0f) r += 1.0f;
+  *u = r;
+}
+__device__ __forceinline__ uint32_t sat_u32(float f) {
+  if (!(f > 0.0f)) return 0u;
+  if (f >= 4294967296.0f) return 0xffffffffu;
+  return (uint32_t)f;
+}
+__device__ __forceinline__ float lin_eval(const DevScene* sc, const float* w, float l) {
+  float x = rclamp(l - 360.0f, 0.0f, 469.999f);
+  int i = (int)x;
+  float f = x - (float)i;
+  float v = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float* b = sc->lin_basis + 471 * c;
+    v += w[c] * (__ldg(b + i) * (1.0f - f) + __ldg(b + i + 1) * f);
+  }
+  return fmaxf(v, 0.0f);
+}
+__device__ Spec envmap_eval(const DevScene* sc, V3 dir, const Wavelengths& wl) {
+  float u, v;
+  env_uv(sc, dir, &u, &v);
+  uint32_t x = min(sat_u32(u * (float)sc->map_w), (uint32_t)sc->map_w - 1u);
+  uint32_t y = min(sat_u32(v * (float)sc->map_h), (uint32_t)sc->map_h - 1u);
+  const float* wp = sc->map_weights + 3 * ((size_t)y * sc->map_w + x);
+  float w[3] = {__ldg(wp), __ldg(wp + 1), __ldg(wp + 2)};
+  Spec r;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) r.v[k] = lin_eval(sc, w, wl.lambda[k]);
+  return r;
+}
+// envmap.rs:375-387
+__device__ float envmap_pdf(const DevScene* sc, V3 dir) {
+  float u, v;
+  env_uv(sc, dir, &u, &v);
+  float st = sinf(ARGENT_PI_F * v);
+  if (st <= 1e-6f) return 0.0f;
+  uint32_t x = min(sat_u32(u * (float)sc->map_w), (uint32_t)sc->map_w - 1u);
+  uint32_t y = min(sat_u32(v * (float)sc->map_h), (uint32_t)sc->map_h - 1u);
+  size_t row = (size_t)y * (sc->map_w + 1);
+  float pc = (__ldg(sc->map_cond + row + x + 1) - __ldg(sc->map_cond + row + x)) * (float)sc->map_w;
+  float pm = (__ldg(sc->map_marg + y + 1) - __ldg(sc->map_marg + y)) * (float)sc->map_h;
+  return pc * pm / (2.0f * ARGENT_PI_F * ARGENT_PI_F * st);
+}
+__device__ __forceinline__ uint32_t partition_le(const float* a, uint32_t n, float u) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(a + mid) <= u)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+// envmap.rs:390-402
+__device__ V3 envmap_sample(const DevScene* sc, float u1, float u2, float* pdf_out) {
+  uint32_t w = (uint32_t)sc->map_w, h = (uint32_t)sc->map_h;
+  uint32_t y = min(max(partition_le(sc->map_marg, h + 1, u1), 1u), h) - 1u;
+  const float* cond = sc->map_cond + (size_t)y * (w + 1);
+  uint32_t x = min(max(partition_le(cond, w + 1, u2), 1u), w) - 1u;
+  float my = __ldg(sc->map_marg + y), my1 = __ldg(sc->map_marg + y + 1);
+  float cx = __ldg(cond + x), cx1 = __ldg(cond + x + 1);
+  float fy = (u1 - my) / fmaxf(my1 - my, 1e-12f);
+  float fx = (u2 - cx) / fmaxf(cx1 - cx, 1e-12f);
+  float u = ((float)x + rclamp(fx, 0.0f, 0.999f)) / (float)w;
+  float v = ((float)y + rclamp(fy, 0.0f, 0.999f)) / (float)h;
+  float phi = (u - 0.5f) * 2.0f * ARGENT_PI_F;
+  float theta = v * ARGENT_PI_F;
+  float st, ct, sp, cp;
+  sincosf(theta, &st, &ct);
+  sincosf(phi, &sp, &cp);
+  V3 d = rot_y_sc(V3{st * sp, ct, -st * cp}, sc->map_to_world_s, sc->map_to_world_c);
+  *pdf_out = envmap_pdf(sc, d);
+  return d;
+}
+// light.rs:111-127
+__device__ Spec env_eval(const DevScene* sc, V3 dir, const Wavelengths& wl) {
+  if (sc->env_is_map) return envmap_eval(sc, dir, wl);
+  float y = rclamp(dir.y, -1.0f, 1.0f);
+  if (y >= 0.0f) {
+    float t = powf(y, sc->env_power);
+    return lerp(t, tab_sample(sc->env_horizon, wl), tab_sample(sc->env_top, wl));
+  }
+  float t = powf(-y, 0.5f);
+  return lerp(t, tab_sample(sc->env_horizon, wl), tab_sample(sc->env_bottom, wl));
+}
+
+// scene.rs:143-147
+__device__ __forceinline__ float light_pick_pdf(const DevScene* sc, int panel) {
+  for (int k = 0; k < sc->num_lights; ++k)
+    if (sc->lights[k] == panel) return sc->light_cdf[k] - (k == 0 ? 0.0f : sc->light_cdf[k - 1]);
+  return 0.0f;
+}
+
+// integrator.rs:35-48
+__device__ __forceinline__ void add_clamped(Spec* l, const Spec& c, bool clamp, float m) {
+  if (clamp) {
+    float mx = max_value(c);
+    *l = (mx > m) ? (*l + c * (m / mx)) : (*l + c);
+  } else {
+    *l = *l + c;
+  }
+}
+__device__ __forceinline__ Spec clamped(const Spec& c, bool clamp, float m) {
+  if (clamp) {
+    float mx = max_value(c);
+    if (mx > m) return c * (m / mx);
+  }
+  return c;
+}
+
+// ---------------------------------------------------------------- wave kernels
+
+struct WaveArgs {
+  const DevJob* jobs;
+  float4 *o, *d, *beta, *L, *lambda, *pdf, *hit, *albedo, *normal, *sh_o, *sh_d, *sh_c;
+  uint4* meta;
+  unsigned long long* rng;
+  uint32_t *q_in, *q_out, *qs;
+  uint32_t* counters;
+  uint32_t* status;
+};
+
+__device__ __forceinline__ const DevSegment& find_segment(const WaveDesc& w, uint32_t slot) {
+  uint32_t s = 0;
+  while (s + 1 < w.num_segments && slot >= w.seg[s + 1].slot_begin) ++s;
+  return w.seg[s];
+}
+
+// camera.rs:57-69
+__device__ __forceinline__ void camera_ray(const ArgentCamera& c, float sx, float sy, float lu, float lv, V3* o,
+                                           V3* d) {
+  V3 pos = ld3(c.pos), fwd = ld3(c.forward), right = ld3(c.right), up = ld3(c.up);
+  float x = (sx + c.shift[0]) * c.half_w;
+  float y = (sy + c.shift[1]) * c.half_h;
+  V3 dir = normalize(fwd + right * x + up * y);
+  if (c.lens_radius <= 0.0f) {
+    *o = pos;
+    *d = dir;
+    return;
+  }
+  float ft = c.focus_dist / dot(dir, fwd);
+  V3 p_focus = pos + dir * ft;
+  float dx, dy;
+  disk(lu, lv, &dx, &dy);
+  V3 oo = pos + right * (dx * c.lens_radius) + up * (dy * c.lens_radius);
+  *o = oo;
+  *d = normalize(p_focus - oo);
+}
+
+// render.rs:82-93: one camera sample per slot.
+__global__ void __launch_bounds__(256) k_raygen(WaveArgs a, WaveDesc w) {
+  if (blockIdx.x == 0) {
+    for (int i = threadIdx.x; i < 2 * (ARGENT_MAX_DEPTH + 2); i += blockDim.x)
+      a.counters[i] = (i == 0) ? w.num_slots : 0u;
+  }
+  for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.num_slots; slot += gridDim.x * blockDim.x) {
+    const DevSegment& sg = find_segment(w, slot);
+    const DevJob& job = a.jobs[sg.job];
+    uint32_t k = slot - sg.slot_begin;
+    uint32_t pix = sg.p0 + k % sg.pn;
+    uint32_t si = job.first + sg.s0 + k / sg.pn;
+    uint32_t x = pix % job.w, y = pix / job.w;
+    uint32_t pix_seed = hash32((y * job.w + x) ^ job.seed_h);
+    Sampler s;
+    s.init(pix_seed, si);
+    float jx = tent(s.next(), 1.0f);
+    float jy = tent(s.next(), 1.0f);
+    float lu = s.next();
+    float lv = s.next();
+    Wavelengths wl = sample_visible(s.next());
+    float aspect_sx = 2.0f / (float)job.w;
+    float aspect_sy = 2.0f / (float)job.h;
+    float sx = (((float)x + 0.5f + jx) * aspect_sx) - 1.0f;
+    float sy = 1.0f - (((float)y + 0.5f + jy) * aspect_sy);
+    V3 o, d;
+    camera_ray(job.cam, sx, sy, lu, lv, &o, &d);
+    a.o[slot] = make_float4(o.x, o.y, o.z, 0.0f);
+    a.d[slot] = make_float4(d.x, d.y, d.z, 1.0f);  // w = prev_pdf
+    a.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+    a.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    a.lambda[slot] = make_float4(wl.lambda[0], wl.lambda[1], wl.lambda[2], wl.lambda[3]);
+    a.pdf[slot] = make_float4(wl.pdf[0], wl.pdf[1], wl.pdf[2], wl.pdf[3]);
+    a.albedo[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    a.normal[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    // flags: bit0 specular, bit1 rough_seen, bits 8..15 medium (material+1), bits 16..31 job
+    a.meta[slot] = make_uint4(pix, si, pix_seed, 1u | (sg.job << 16));
+    a.rng[slot] = s.rng;
+    a.q_in[slot] = slot;
+  }
+}
+
+// scene.rs:169-218
+__global__ void __launch_bounds__(128) k_intersect(WaveArgs a, int depth) {
+  uint32_t count = a.counters[depth];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    uint32_t slot = a.q_in[i];
+    uint32_t job_id = a.meta[slot].w >> 16;
+    const DevScene* sc = a.jobs[job_id].scene;
+    float4 of = a.o[slot], df = a.d[slot];
+    V3 o{of.x, of.y, of.z}, d{df.x, df.y, df.z};
+    float t_max = INFINITY;
+    float4 rec = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(HIT_MISS));
+    V3 oo = o, od = d;
+    if (sc->has_turn) {
+      oo = rot_y_sc(o, sc->to_obj_s, sc->to_obj_c);
+      od = rot_y_sc(d, sc->to_obj_s, sc->to_obj_c);
+    }
+    TraceHit h = trace_closest(sc->piece, oo, od, INFINITY, a.status);
+    if (h.prim != ARGENT_NO_HIT_U) {
+      t_max = h.t;
+      rec = make_float4(h.t, h.u, h.v, __uint_as_float(h.prim));
+    }
+    for (int p = 0; p < sc->num_panels; ++p) {
+      const DevPanel& pn = sc->panels[p];
+      if (depth == 0 && !pn.camera_visible) continue;
+      float t;
+      if (panel_intersect(pn, o, d, t_max, &t)) {
+        t_max = t;
+        rec = make_float4(t, 0.0f, 0.0f, __uint_as_float(HIT_PANEL | (uint32_t)p));
+      }
+    }
+    if (sc->floor_enabled) {
+      float t;
+      if (floor_intersect(sc, o, d, t_max, &t)) rec = make_float4(t, 0.0f, 0.0f, __uint_as_float(HIT_FLOOR));
+    }
+    a.hit[slot] = rec;
+  }
+}
+
+// Warp-aggregated queue append: one atomic per warp, ballot prefix for the
+// lane offsets.  Every lane of the warp must call it.
+__device__ __forceinline__ void warp_append(bool pred, uint32_t value, uint32_t* counter, uint32_t* queue,
+                                            uint32_t cap, uint32_t* status) {
+  unsigned m = __ballot_sync(0xffffffffu, pred);
+  if (!m) return;
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(m) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (pred) {
+    uint32_t pos = base + __popc(m & ((1u << lane) - 1u));
+    if (pos < cap)
+      queue[pos] = value;
+    else
+      atomicOr(status, ARGENT_STATUS_QUEUE_OVERFLOW);
+  }
+}
+
+struct ShadeOut {
+  bool alive;
+  bool shadow;
+  float4 sh_o, sh_d, sh_c;
+};
+
+// integrator.rs:59-218, one bounce of one path.
+__device__ __noinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot, int depth) {
+  ShadeOut out;
+  out.alive = false;
+  out.shadow = false;
+  uint4 meta = a.meta[slot];
+  const DevJob& job = a.jobs[meta.w >> 16];
+  const DevScene* sc = job.scene;
+  uint32_t flags = meta.w;
+  bool specular = flags & 1u;
+  bool rough_seen = (flags >> 1) & 1u;
+  uint32_t medium = (flags >> 8) & 0xffu;
+  Sampler s;
+  s.resume(meta.z, meta.y, a.rng[slot]);
+  s.set_dim(8u + (uint32_t)depth * 8u);
+  float4 of = a.o[slot], df = a.d[slot], hf = a.hit[slot];
+  V3 ro{of.x, of.y, of.z}, rd{df.x, df.y, df.z};
+  float prev_pdf = df.w;
+  Spec beta = spec4(a.beta[slot]);
+  Spec L = spec4(a.L[slot]);
+  float4 lf = a.lambda[slot], pf = a.pdf[slot];
+  Wavelengths wl{{lf.x, lf.y, lf.z, lf.w}, {pf.x, pf.y, pf.z, pf.w}};
+  bool clamp = rough_seen;
+  float cl = job.clamp_indirect;
+  uint32_t kind = __float_as_uint(hf.w);
+  float t = hf.x;
+
+  if (medium && kind != HIT_MISS) {
+    Spec sig = tab_sample(sc->mats[medium - 1].spec_b, wl);
+    Spec e;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) e.v[i] = expf(-sig.v[i] * t);
+    beta = beta * e;
+  }
+  bool env_map = sc->env_is_map != 0;
+  V3 p, p_obj, ng, ns;
+  uint32_t mat_id = 0;
+  float cavity = 0.0f;
+  bool done = false;
+  if (kind == HIT_MISS) {
+    float w = 1.0f;
+    if (env_map && !specular) {
+      float pl = sc->env_pick * envmap_pdf(sc, rd);
+      w = prev_pdf * prev_pdf / (prev_pdf * prev_pdf + pl * pl);
+    }
+    add_clamped(&L, beta * env_eval(sc, rd, wl) * w, clamp, cl);
+    done = true;
+  } else if ((kind & 0xF0000000u) == HIT_PANEL && kind != HIT_FLOOR) {
+    int idx = (int)(kind & 0x0FFFFFFFu);
+    const DevPanel& pn = sc->panels[idx];
+    Spec le = panel_le(pn, ro + rd * t, rd, wl);
+    if (!is_black(le)) {
+      if (specular) {
+        add_clamped(&L, beta * le, clamp, cl);
+      } else {
+        float cos_l = fmaxf(fabsf(dot(-rd, ld3(pn.n))), 1e-8f);
+        float p_light = (1.0f - sc->env_pick) * light_pick_pdf(sc, idx) * t * t / (cos_l * pn.area);
+        float w = prev_pdf * prev_pdf / (prev_pdf * prev_pdf + p_light * p_light);
+        add_clamped(&L, beta * le * w, clamp, cl);
+      }
+    }
+    done = true;
+  } else if (kind == HIT_FLOOR) {
+    V3 fp = ro + rd * t;
+    if (s.next_random() >= floor_presence(sc, fp)) {
+      float w = 1.0f;
+      if (env_map && !specular) {
+        float pl = sc->env_pick * envmap_pdf(sc, rd);
+        w = prev_pdf * prev_pdf / (prev_pdf * prev_pdf + pl * pl);
+      }
+      add_clamped(&L, beta * env_eval(sc, rd, wl) * w, clamp, cl);
+      done = true;
+    } else {
+      V3 n = rd.y < 0.0f ? V3{0.0f, 1.0f, 0.0f} : V3{0.0f, -1.0f, 0.0f};
+      p = fp;
+      p_obj = fp;
+      ng = n;
+      ns = n;
+      mat_id = (uint32_t)sc->floor_material;
+    }
+  } else {
+    // scene.rs:174-201: hit attributes of the piece.
+    const DevPiece& pc = sc->piece;
+    uint4 tri = __ldg(pc.tri_idx + kind);
+    float4 fa = __ldg(pc.pos + tri.x), fb = __ldg(pc.pos + tri.y), fc = __ldg(pc.pos + tri.z);
+    V3 A{fa.x, fa.y, fa.z}, B{fb.x, fb.y, fb.z}, C{fc.x, fc.y, fc.z};
+    float hu = hf.y, hv = hf.z;
+    V3 ngo = normalize(cross(B - A, C - A));
+    float w = 1.0f - hu - hv;
+    mat_id = tri.w;
+    const ArgentMaterial* m = sc->mats + mat_id;
+    bool flat = m->kind == ARGENT_MAT_GEM && m->gem_kind == ARGENT_GEM_TRANSPARENT;
+    V3 nso;
+    if (flat || pc.nrm == nullptr) {
+      nso = ngo;
+    } else {
+      float4 na = __ldg(pc.nrm + tri.x), nb = __ldg(pc.nrm + tri.y), nc = __ldg(pc.nrm + tri.z);
+      V3 n = V3{na.x, na.y, na.z} * w + V3{nb.x, nb.y, nb.z} * hu + V3{nc.x, nc.y, nc.z} * hv;
+      nso = length_squared(n) > 1e-12f ? normalize(n) : ngo;
+    }
+    if (pc.cavity) cavity = __ldg(pc.cavity + tri.x) * w + __ldg(pc.cavity + tri.y) * hu + __ldg(pc.cavity + tri.z) * hv;
+    p_obj = A * w + B * hu + C * hv;
+    if (sc->has_turn) {
+      p = rot_y_sc(p_obj, sc->to_world_s, sc->to_world_c);
+      ng = rot_y_sc(ngo, sc->to_world_s, sc->to_world_c);
+      ns = rot_y_sc(nso, sc->to_world_s, sc->to_world_c);
+    } else {
+      p = p_obj;
+      ng = ngo;
+      ns = nso;
+    }
+  }
+
+  if (!done) {
+    const ArgentMaterial* mat = sc->mats + mat_id;
+    V3 wo_w = -rd;
+    bool transmissive = mat_is_transmissive(mat);
+    V3 nsu = ns, ngu = ng;
+    if (!transmissive && dot(ng, wo_w) < 0.0f) {
+      nsu = -ns;
+      ngu = -ng;
+    }
+    if (!transmissive && dot(nsu, wo_w) <= 0.0f) nsu = ngu;
+    Frame frame = make_frame(nsu);
+    V3 wo = to_local(frame, wo_w);
+    HitCtx ctx{p_obj, nsu, &frame, sc->to_world_s, sc->to_world_c};
+    if (!sc->has_turn) {
+      ctx.turn_s = 0.0f;
+      ctx.turn_c = 1.0f;
+    }
+    float ub = s.next();
+    Bsdf bsdf = material_bsdf(mat, wl, cavity, ub, ctx);
+    if (depth == 0) {
+      float g[3];
+      guide_rgb(mat, cavity, g);
+      a.albedo[slot] = make_float4(g[0], g[1], g[2], 0.0f);
+      a.normal[slot] = make_float4(nsu.x, nsu.y, nsu.z, 0.0f);
+    }
+
+    // Next-event estimation (integrator.rs:130-178).
+    if (!bsdf_is_delta(bsdf)) {
+      float ul = s.next();
+      float u1 = s.next();
+      float u2 = s.next();
+      if (env_map && ul < sc->env_pick) {
+        float pdf_dir;
+        V3 dir = envmap_sample(sc, u1, u2, &pdf_dir);
+        if (pdf_dir > 0.0f && dot(dir, ngu) > 0.0f) {
+          V3 wi = to_local(frame, dir);
+          Spec f = bsdf_eval(bsdf, wo, wi);
+          if (!is_black(f)) {
+            float p_light = sc->env_pick * pdf_dir;
+            float p_bsdf = bsdf_pdf(bsdf, wo, wi);
+            float w = p_light * p_light / (p_light * p_light + p_bsdf * p_bsdf);
+            // sky_visibility (scene.rs:123-140): panels and floor here, the
+            // piece in k_shadow.
+            V3 from = offset_origin(p, ngu, dir);
+            float vis = 1.0f;
+            for (int q = 0; q < sc->num_panels && vis > 0.0f; ++q) {
+              float tt;
+              if (panel_intersect(sc->panels[q], from, dir, INFINITY, &tt)) vis = 0.0f;
+            }
+            if (vis > 0.0f && sc->floor_enabled) {
+              float tt;
+              if (floor_intersect(sc, from, dir, INFINITY, &tt)) vis = 1.0f - floor_presence(sc, from + dir * tt);
+            }
+            if (vis > 0.0f) {
+              Spec le = envmap_eval(sc, dir, wl);
+              Spec c = beta * f * le * (fabsf(wi.z) * w * vis / p_light);
+              c = clamped(c, rough_seen, cl);
+              V3 oo = from, od = dir;
+              if (sc->has_turn) {
+                oo = rot_y_sc(from, sc->to_obj_s, sc->to_obj_c);
+                od = rot_y_sc(dir, sc->to_obj_s, sc->to_obj_c);
+              }
+              out.shadow = true;
+              out.sh_o = make_float4(oo.x, oo.y, oo.z, INFINITY);
+              out.sh_d = make_float4(od.x, od.y, od.z, __uint_as_float(slot));
+              out.sh_c = to_f4(c);
+            }
+          }
+        }
+      } else if (sc->num_lights > 0) {
+        // scene.rs:149-156
+        float u = sc->env_pick > 0.0f ? (ul - sc->env_pick) / (1.0f - sc->env_pick) : ul;
+        int k = 0;
+        {
+          int lo = 0, hi = sc->num_lights;
+          while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (sc->light_cdf[mid] < u)
+              lo = mid + 1;
+            else
+              hi = mid;
+          }
+          k = min(lo, sc->num_lights - 1);
+        }
+        float pick = sc->light_cdf[k] - (k == 0 ? 0.0f : sc->light_cdf[k - 1]);
+        int li = sc->lights[k];
+        pick = pick * (1.0f - sc->env_pick);
+        const DevPanel& pn = sc->panels[li];
+        V3 lp = ld3(pn.c) + ld3(pn.hu) * (2.0f * u1 - 1.0f) + ld3(pn.hv) * (2.0f * u2 - 1.0f);
+        V3 to = lp - p;
+        float d2 = length_squared(to);
+        V3 dir = to / sqrtf(d2);
+        float cos_l = dot(-dir, ld3(pn.n));
+        if (cos_l > 0.0f && dot(dir, ngu) > 0.0f) {
+          V3 wi = to_local(frame, dir);
+          Spec f = bsdf_eval(bsdf, wo, wi);
+          if (!is_black(f)) {
+            float p_light = pick * d2 / (cos_l * pn.area);
+            float p_bsdf = bsdf_pdf(bsdf, wo, wi);
+            float w = p_light * p_light / (p_light * p_light + p_bsdf * p_bsdf);
+            V3 origin = offset_origin(p, ngu, dir);
+            // visible (scene.rs:222-243): panels and floor here.
+            V3 dd = lp - origin;
+            float dist = length(dd);
+            V3 sdir = dd / dist;
+            float t_max = dist * (1.0f - 1e-4f);
+            bool vis = true;
+            for (int q = 0; q < sc->num_panels && vis; ++q) {
+              float tt;
+              if (q != li && panel_intersect(sc->panels[q], origin, sdir, t_max, &tt)) vis = false;
+            }
+            if (vis && sc->floor_enabled) {
+              float tt;
+              if (floor_intersect(sc, origin, sdir, t_max, &tt)) vis = false;
+            }
+            if (vis) {
+              Spec le = panel_le(pn, lp, dir, wl);
+              Spec c = beta * f * le * (fabsf(wi.z) * w / p_light);
+              c = clamped(c, rough_seen, cl);
+              V3 oo = origin, od = sdir;
+              if (sc->has_turn) {
+                oo = rot_y_sc(origin, sc->to_obj_s, sc->to_obj_c);
+                od = rot_y_sc(sdir, sc->to_obj_s, sc->to_obj_c);
+              }
+              out.shadow = true;
+              out.sh_o = make_float4(oo.x, oo.y, oo.z, t_max);
+              out.sh_d = make_float4(od.x, od.y, od.z, __uint_as_float(slot));
+              out.sh_c = to_f4(c);
+            }
+          }
+        }
+      }
+    } else {
+      s.next();
+      s.next();
+      s.next();
+    }
+
+    // Continue the path (integrator.rs:180-218).
+    float u0 = s.next();
+    float u1 = s.next();
+    float u2 = s.next();
+    BsdfSample smp;
+    bool cont = bsdf_sample(bsdf, wo, u0, u1, u2, &smp);
+    if (cont && (smp.pdf <= 0.0f || is_black(smp.f))) cont = false;
+    V3 wi_w;
+    if (cont) {
+      wi_w = to_world(frame, smp.wi);
+      float side = dot(wi_w, ngu) * dot(wo_w, ngu);
+      if ((!smp.transmit && side <= 0.0f) || (smp.transmit && side >= 0.0f)) cont = false;
+    }
+    if (cont) {
+      if (smp.terminate_secondary) terminate_secondary(&wl);
+      beta = beta * (smp.f * (fabsf(smp.wi.z) / smp.pdf));
+      if (!is_finite(beta)) cont = false;
+    }
+    if (cont) {
+      specular = smp.delta;
+      if (!smp.delta) rough_seen = true;
+      prev_pdf = smp.pdf;
+      if (smp.transmit) medium = (wo.z > 0.0f && mat_has_medium(mat)) ? mat_id + 1u : 0u;
+      ro = offset_origin(p, ngu, wi_w);
+      rd = wi_w;
+      if ((uint32_t)depth >= job.rr_depth) {
+        float survive = fminf(max_value(beta), 0.95f);
+        if (survive <= 0.0f || s.next_random() >= survive)
+          cont = false;
+        else
+          beta = beta / survive;
+      }
+    }
+    out.alive = cont && ((uint32_t)depth + 1u < job.max_depth);
+    // Store the state the next bounce (or the film) reads.
+    a.beta[slot] = to_f4(beta);
+    a.pdf[slot] = make_float4(wl.pdf[0], wl.pdf[1], wl.pdf[2], wl.pdf[3]);
+    if (out.alive) {
+      a.o[slot] = make_float4(ro.x, ro.y, ro.z, 0.0f);
+      a.d[slot] = make_float4(rd.x, rd.y, rd.z, prev_pdf);
+      uint32_t nf = (flags & 0xffff0000u) | (specular ? 1u : 0u) | (rough_seen ? 2u : 0u) | (medium << 8);
+      a.meta[slot].w = nf;
+      a.rng[slot] = s.rng;
+    }
+  }
+  a.L[slot] = to_f4(L);
+  return out;
+}
+
+__global__ void __launch_bounds__(128) k_shade(WaveArgs a, int depth, uint32_t cap) {
+  uint32_t count = a.counters[depth];
+  uint32_t* next_counter = a.counters + depth + 1;
+  uint32_t* shadow_counter = a.counters + (ARGENT_MAX_DEPTH + 2) + depth;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
+    uint32_t i = base + threadIdx.x;
+    ShadeOut r;
+    r.alive = false;
+    r.shadow = false;
+    uint32_t slot = 0;
+    if (i < count) {
+      slot = a.q_in[i];
+      r = shade_path(a, slot, depth);
+    }
+    warp_append(r.alive, slot, next_counter, a.q_out, cap, a.status);
+    // Shadow rays: the record is written at the queue position.
+    unsigned m = __ballot_sync(0xffffffffu, r.shadow);
+    if (m) {
+      int lane = threadIdx.x & 31;
+      int leader = __ffs(m) - 1;
+      uint32_t sbase = 0;
+      if (lane == leader) sbase = atomicAdd(shadow_counter, (uint32_t)__popc(m));
+      sbase = __shfl_sync(0xffffffffu, sbase, leader);
+      if (r.shadow) {
+        uint32_t pos = sbase + __popc(m & ((1u << lane) - 1u));
+        if (pos < cap) {
+          a.sh_o[pos] = r.sh_o;
+          a.sh_d[pos] = r.sh_d;
+          a.sh_c[pos] = r.sh_c;
+        } else {
+          atomicOr(a.status, ARGENT_STATUS_QUEUE_OVERFLOW);
+        }
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) k_shadow(WaveArgs a, int depth) {
+  uint32_t count = a.counters[(ARGENT_MAX_DEPTH + 2) + depth];
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    float4 so = a.sh_o[i], sd = a.sh_d[i];
+    uint32_t slot = __float_as_uint(sd.w);
+    uint32_t job_id = a.meta[slot].w >> 16;
+    const DevScene* sc = a.jobs[job_id].scene;
+    bool occ = trace_any(sc->piece, V3{so.x, so.y, so.z}, V3{sd.x, sd.y, sd.z}, so.w, a.status);
+    if (!occ) {
+      float4 c = a.sh_c[i];
+      float4 l = a.L[slot];
+      a.L[slot] = make_float4(l.x + c.x, l.y + c.y, l.z + c.z, l.w + c.w);
+    }
+  }
+}
+
+// render.rs:96-111 + Film sums.
+__global__ void __launch_bounds__(256) k_film(WaveArgs a, WaveDesc w) {
+  uint32_t total = 0;
+  for (uint32_t s = 0; s < w.num_segments; ++s) total += w.seg[s].pn;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    uint32_t s = 0, off = t;
+    while (off >= w.seg[s].pn) {
+      off -= w.seg[s].pn;
+      ++s;
+    }
+    const DevSegment& sg = w.seg[s];
+    const DevJob& job = a.jobs[sg.job];
+    const float* m = job.scene->cam_m;
+    float acc[3] = {0.0f, 0.0f, 0.0f}, aacc[3] = {0.0f, 0.0f, 0.0f}, nacc[3] = {0.0f, 0.0f, 0.0f};
+    double acc64[3] = {0.0, 0.0, 0.0};
+    for (uint32_t k = 0; k < sg.sn; ++k) {
+      uint32_t slot = sg.slot_begin + k * sg.pn + off;
+      float4 lf = a.L[slot], wlf = a.lambda[slot], pf = a.pdf[slot];
+      Spec L{{lf.x, lf.y, lf.z, lf.w}};
+      Wavelengths wl{{wlf.x, wlf.y, wlf.z, wlf.w}, {pf.x, pf.y, pf.z, pf.w}};
+      float xyz[3];
+      to_xyz(L, wl, xyz);
+      float r0 = m[0] * xyz[0] + m[1] * xyz[1] + m[2] * xyz[2];
+      float r1 = m[3] * xyz[0] + m[4] * xyz[1] + m[5] * xyz[2];
+      float r2 = m[6] * xyz[0] + m[7] * xyz[1] + m[8] * xyz[2];
+      if (isfinite(r0) && isfinite(r1) && isfinite(r2)) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          acc[c] += xyz[c];
+          acc64[c] += (double)xyz[c];
+        }
+      }
+      float4 al = a.albedo[slot], nr = a.normal[slot];
+      aacc[0] += al.x;
+      aacc[1] += al.y;
+      aacc[2] += al.z;
+      nacc[0] += nr.x;
+      nacc[1] += nr.y;
+      nacc[2] += nr.z;
+    }
+    size_t o = 3 * (size_t)(sg.p0 + off);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if (job.film_comp) {
+        // Kahan-compensated running sum.
+        float sum = job.film_xyz[o + c];
+        float y = acc[c] - job.film_comp[o + c];
+        float tt = sum + y;
+        job.film_comp[o + c] = (tt - sum) - y;
+        job.film_xyz[o + c] = tt;
+      } else {
+        job.film_xyz[o + c] += acc[c];
+      }
+      if (job.film_xyz64) job.film_xyz64[o + c] += acc64[c];
+      job.film_albedo[o + c] += aacc[c];
+      job.film_normal[o + c] += nacc[c];
+    }
+  }
+}
+
+}  // namespace dev

@@ -1,0 +1,185 @@
+"""Python handles over the C ABI (include/argent_gpu.h).
+
+These mirror argent's own objects: `Piece` (scene.rs:10-38), `Scene`
+(scene.rs:47-110), `Film` (render.rs:12-63) and `render_pass`
+(render.rs:67-115), so callers and tests read like argent's.
+"""
+
+import ctypes
+
+import numpy as np
+
+from . import _native as N
+
+
+def _p(a, t=ctypes.c_void_p):
+    if a is None:
+        return None
+    return a.ctypes.data_as(t)
+
+
+class Context:
+    """One device, one stream (argent_ctx_create)."""
+
+    def __init__(self, device=0, wave_paths=0, memory_budget=0):
+        self.lib = N.gpu()
+        lim = N.ArgentLimits(wave_paths, memory_budget)
+        h = ctypes.c_void_p()
+        N.check(self.lib.argent_ctx_create(device, ctypes.byref(lim), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.argent_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def check(self, rc):
+        return N.check(rc, self.h)
+
+    def sync(self):
+        self.check(self.lib.argent_ctx_sync(self.h))
+
+    @property
+    def kernel_launches(self):
+        return int(self.lib.argent_ctx_kernel_launches(self.h))
+
+    @property
+    def stream(self):
+        return self.lib.argent_ctx_stream(self.h)
+
+
+class Piece:
+    """`Piece::new`: mesh upload + acceleration structure build."""
+
+    def __init__(self, ctx: Context, mesh):
+        self.ctx = ctx
+        self.mesh = mesh
+        h = ctypes.c_void_p()
+        fp = ctypes.POINTER(ctypes.c_float)
+        ctx.check(ctx.lib.argent_piece_upload(
+            ctx.h, _p(mesh.positions, fp), len(mesh.positions), _p(mesh.normals, fp), _p(mesh.tris, N.c_u32_p),
+            len(mesh.tris), _p(mesh.tri_material, N.c_u16_p), _p(mesh.cavity, fp), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.argent_piece_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def bounds(self):
+        lo = (ctypes.c_float * 3)()
+        hi = (ctypes.c_float * 3)()
+        self.ctx.check(self.ctx.lib.argent_piece_bounds(self.h, lo, hi))
+        return np.array(lo[:], np.float32), np.array(hi[:], np.float32)
+
+    @property
+    def device_bytes(self):
+        return int(self.ctx.lib.argent_piece_device_bytes(self.h))
+
+    def trace_closest(self, rays: np.ndarray) -> np.ndarray:
+        """rays: (n, 8) float32 [ox oy oz tmax dx dy dz pad] -> hits (n, 4)
+        float32 [t u v prim-bits]."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        hits = np.zeros((len(rays), 4), np.float32)
+        self.ctx.check(self.ctx.lib.argent_trace_closest(self.ctx.h, self.h, _p(rays), len(rays), _p(hits)))
+        return hits
+
+    def trace_anyhit(self, rays: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, np.float32)
+        occ = np.zeros(len(rays), np.uint8)
+        self.ctx.check(self.ctx.lib.argent_trace_anyhit(self.ctx.h, self.h, _p(rays), len(rays), _p(occ)))
+        return occ
+
+
+class Scene:
+    """`Scene::new` around a piece, from an ArgentSceneDesc."""
+
+    def __init__(self, ctx: Context, piece: Piece, desc):
+        self.ctx = ctx
+        self.piece = piece
+        self.desc = desc  # keeps the description's arrays alive
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.argent_scene_upload(ctx.h, piece.h, ctypes.byref(desc.c), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.argent_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_turntable(self, deg):
+        self.ctx.check(self.ctx.lib.argent_scene_set_turntable(self.h, float(deg)))
+
+
+class Film:
+    """`Film` (render.rs:12-63): device sums, read back as averages."""
+
+    def __init__(self, ctx: Context, width, height, flags=N.FILM_KAHAN):
+        self.ctx = ctx
+        self.width, self.height = width, height
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.argent_film_create(ctx.h, width, height, flags, ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.argent_film_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def samples(self):
+        return int(self.ctx.lib.argent_film_samples(self.h))
+
+    def clear(self):
+        self.ctx.check(self.ctx.lib.argent_film_clear(self.h))
+
+    def read(self):
+        """(color, albedo, normal) as `Film::color/albedo/normal`, (h, w, 3)."""
+        shape = (self.height, self.width, 3)
+        c, a, n = np.zeros(shape, np.float32), np.zeros(shape, np.float32), np.zeros(shape, np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self.ctx.check(self.ctx.lib.argent_film_read(self.h, _p(c, fp), _p(a, fp), _p(n, fp)))
+        return c, a, n
+
+    def color(self):
+        shape = (self.height, self.width, 3)
+        c = np.zeros(shape, np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self.ctx.check(self.ctx.lib.argent_film_read(self.h, _p(c, fp), None, None))
+        return c
+
+    def xyz(self):
+        x = np.zeros((self.height, self.width, 3), np.float32)
+        self.ctx.check(self.ctx.lib.argent_film_read_xyz(self.h, _p(x, ctypes.POINTER(ctypes.c_float))))
+        return x
+
+
+def render_pass(ctx: Context, scene: Scene, cam, film: Film, settings, count, seed):
+    """argent's `render_pass(scene, cam, film, ps, count, seed)`."""
+    ctx.check(ctx.lib.argent_render_pass(ctx.h, scene.h, ctypes.byref(cam), film.h, ctypes.byref(settings),
+                                         int(count), int(seed)))
+
+
+def render_batch(ctx: Context, items):
+    """items: list of (scene, cam, film, settings, count, seed)."""
+    arr = (N.ArgentBatchItem * len(items))()
+    for i, (scene, cam, film, ps, count, seed) in enumerate(items):
+        arr[i].scene = scene.h
+        arr[i].camera = cam
+        arr[i].film = film.h
+        arr[i].settings = ps
+        arr[i].count = int(count)
+        arr[i].seed = int(seed)
+    ctx.check(ctx.lib.argent_render_batch(ctx.h, arr, len(items)))

@@ -1,0 +1,324 @@
+/*
+ * argent_gpu.h — C ABI of the B200 spectral path tracer.
+ *
+ * This is the drop-in boundary for argent's render hot path.  argent calls
+ * `render_pass(scene, cam, film, ps, count, seed)`
+ * (crates/argent-core/src/render.rs:67) and
+ * `render_image(scene, cam, q, seed)` (crates/argent-core/src/shot.rs:424) as
+ * plain Rust functions.  A Rust FFI crate binds the functions below in their
+ * place.  Everything above the boundary stays on argent's side: mesh loading,
+ * posing, the spectral table builders in argent-spectra, the studio rigs,
+ * framing, denoise and tone mapping.  Those produce the plain-old-data
+ * descriptions declared here.
+ *
+ * Conventions:
+ *  - Every function returns an int status (ARGENT_OK or ARGENT_E_*).  The
+ *    text of the last failure is available from argent_last_error(ctx), or
+ *    from argent_last_error(NULL) for failures before a context exists.
+ *  - No exception or panic crosses the ABI.
+ *  - Handles own device memory.  The caller owns all host arrays.  Uploads
+ *    copy them, so a host array may be freed when the call returns.
+ *  - A context owns one CUDA stream and is not thread-safe.  Use one
+ *    context per worker thread.
+ *  - Units are millimetres and nanometres, as in argent.
+ */
+#ifndef ARGENT_GPU_H
+#define ARGENT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Spectral sampling conventions of argent-spectra. */
+#define ARGENT_SPEC_LEN 471  /* 1 nm table over 360..=830 nm (core/src/tab.rs:8-27) */
+#define ARGENT_NK_LEN 95     /* 5 nm grid over 360..=830 nm (spectra/src/metals.rs:53-56) */
+
+/* Status codes. */
+enum {
+  ARGENT_OK = 0,
+  ARGENT_E_OOM = 1,      /* device or host allocation failed */
+  ARGENT_E_INVALID = 2,  /* bad argument or malformed description */
+  ARGENT_E_TIMEOUT = 3,  /* a bounded device wait ran out */
+  ARGENT_E_CUDA = 4,     /* a CUDA runtime call failed */
+  ARGENT_E_OVERFLOW = 5, /* a traversal stack or queue overflowed (recorded, not trapped) */
+  ARGENT_E_BUSY = 6      /* admission refused: not enough device memory budget */
+};
+
+typedef struct ArgentCtx ArgentCtx;
+typedef struct ArgentPiece ArgentPiece;
+typedef struct ArgentScene ArgentScene;
+typedef struct ArgentFilm ArgentFilm;
+
+/* ------------------------------------------------------------------ */
+/* Scene description (argent-core scene.rs / material.rs / light.rs). */
+/* ------------------------------------------------------------------ */
+
+/* Material kinds: the variants of `Material` (core/src/material.rs:27-36). */
+enum {
+  ARGENT_MAT_METAL = 0,
+  ARGENT_MAT_GEM = 1,
+  ARGENT_MAT_PLASTIC = 2,
+  ARGENT_MAT_OPAL = 3,
+  ARGENT_MAT_DIFFUSE = 4,
+  ARGENT_MAT_BLACK = 5
+};
+
+/* `GemKind` (spectra/src/gems.rs:86-93). */
+enum { ARGENT_GEM_TRANSPARENT = 0, ARGENT_GEM_OPAL = 1, ARGENT_GEM_OPAQUE = 2 };
+
+/*
+ * One material slot.  The fields a kind does not use are ignored.
+ *  METAL:   nk_eta/nk_k = the alloy's n,k on the 5 nm grid (`ComplexIor`),
+ *           alpha = GGX alpha.  Optional patina (material.rs:15-24):
+ *           spec_a = tarnish base albedo (1 nm table).
+ *  GEM:     spec_a = n(lambda) (1 nm table), spec_b = absorption in 1/mm
+ *           (1 nm table).  For ARGENT_GEM_OPAQUE, spec_b2 = body albedo table
+ *           when has_opaque_base, else a constant 0.01 is used (material.rs:127-131).
+ *  PLASTIC: spec_a = base albedo table, eta, alpha.
+ *  OPAL:    spec_a = body albedo table, cell_mm, strength.
+ *  DIFFUSE: spec_a = albedo table.
+ *  BLACK:   nothing.
+ * `alpha` is already mapped from perceptual roughness
+ * (alpha = max(clamp(r,0,1)^2, 1e-4), microfacet.rs:22-25).
+ */
+typedef struct ArgentMaterial {
+  int32_t kind;
+  int32_t gem_kind;
+  float alpha;
+  float eta;
+  float cell_mm;
+  float strength;
+  int32_t has_patina;
+  float patina_strength;
+  float patina_lo;
+  float patina_hi;
+  float patina_alpha;
+  float patina_eta;
+  int32_t has_opaque_base;
+  float nk_eta[ARGENT_NK_LEN];
+  float nk_k[ARGENT_NK_LEN];
+  float spec_a[ARGENT_SPEC_LEN];
+  float spec_b[ARGENT_SPEC_LEN];
+  float spec_b2[ARGENT_SPEC_LEN];
+} ArgentMaterial;
+
+/*
+ * A rectangular softbox or flag (`Panel`, core/src/light.rs:10-27).
+ * The library derives n = normalize(hu x hv) and area = 4 |hu x hv|
+ * exactly as `Panel::new` (light.rs:30-33) does.
+ */
+typedef struct ArgentPanel {
+  float center[3];
+  float hu[3];
+  float hv[3];
+  int32_t emits;          /* 0 = flag (black card) */
+  int32_t camera_visible;
+  float feather;
+  float emission[ARGENT_SPEC_LEN]; /* radiance table when emits */
+} ArgentPanel;
+
+/* `Env` (light.rs:103-109). */
+enum { ARGENT_ENV_GRADIENT = 0, ARGENT_ENV_MAP = 1 };
+
+typedef struct ArgentEnv {
+  int32_t kind;
+  /* Gradient: tables for the three bands and the blend power. */
+  float power;
+  float top[ARGENT_SPEC_LEN];
+  float horizon[ARGENT_SPEC_LEN];
+  float bottom[ARGENT_SPEC_LEN];
+  /* Map: equirectangular linear-sRGB texels, exposure already applied,
+   * row-major, width*height*3 floats (envmap.rs:141-177 input). */
+  int32_t width;
+  int32_t height;
+  const float* rgb;
+  float rotation_deg;
+} ArgentEnv;
+
+/* `Floor` (light.rs:133-138). */
+typedef struct ArgentFloor {
+  int32_t enabled;
+  float y;
+  int32_t material;
+  float fade_start;
+  float fade_end;
+} ArgentFloor;
+
+/* Everything `Scene::new` takes besides the piece (scene.rs:47-64, 82). */
+typedef struct ArgentSceneDesc {
+  const ArgentMaterial* materials;
+  int32_t num_materials;
+  const ArgentPanel* panels;
+  int32_t num_panels;
+  const ArgentEnv* env;
+  ArgentFloor floor;
+  float turntable_deg;
+  int32_t has_white;   /* 0 = D65 (scene.white = None) */
+  float white_xyz[3];
+} ArgentSceneDesc;
+
+/* `Camera` (core/src/camera.rs:17-29): a plain copy of its fields. */
+typedef struct ArgentCamera {
+  float pos[3];
+  float forward[3];
+  float right[3];
+  float up[3];
+  float half_w;
+  float half_h;
+  float lens_radius;
+  float focus_dist;
+  float shift[2];
+} ArgentCamera;
+
+/* `PathSettings` (core/src/integrator.rs:10-24). */
+typedef struct ArgentPathSettings {
+  uint32_t max_depth;
+  float clamp_indirect;
+  uint32_t rr_depth;
+} ArgentPathSettings;
+
+/* A ray for the traversal entry points: origin, t_max, direction. */
+typedef struct ArgentRay {
+  float o[3];
+  float tmax;
+  float d[3];
+  float pad;
+} ArgentRay;
+
+/* Closest-hit result; prim = ARGENT_NO_HIT on a miss (bvh.rs:63-70). */
+#define ARGENT_NO_HIT 0xFFFFFFFFu
+typedef struct ArgentHit {
+  float t;
+  float u;
+  float v;
+  uint32_t prim;
+} ArgentHit;
+
+/* Context limits; zero fields take defaults. */
+typedef struct ArgentLimits {
+  uint64_t wave_paths;      /* path slots per wavefront wave (default 2^21) */
+  uint64_t memory_budget;   /* bytes the serve loop may hold (default 3/4 of free) */
+} ArgentLimits;
+
+/* Film flags. */
+enum {
+  ARGENT_FILM_KAHAN = 1, /* FP32 sums with Kahan compensation (default) */
+  ARGENT_FILM_FP64 = 2   /* FP64 sums (oracle-grade accumulation) */
+};
+
+/* ------------------------------------------------------------------ */
+/* Context, piece, scene, film.                                       */
+/* ------------------------------------------------------------------ */
+
+/* New context on `device`.  Replaces nothing in argent: argent has no device. */
+int argent_ctx_create(int device, const ArgentLimits* limits, ArgentCtx** out);
+void argent_ctx_destroy(ArgentCtx* ctx);
+const char* argent_last_error(const ArgentCtx* ctx);
+/* Block until the context's stream is idle. */
+int argent_ctx_sync(ArgentCtx* ctx);
+/* The context's cudaStream_t, as a void pointer. */
+void* argent_ctx_stream(ArgentCtx* ctx);
+
+/*
+ * Upload a piece and build its acceleration structure.  Replaces
+ * `Piece::new` + `Bvh::build` (core/src/scene.rs:22-32, bvh.rs:117-146).
+ * positions: nv*3 floats; normals: nv*3 floats or NULL (flat shading, as
+ * argent does for a mesh without normals, scene.rs:181); tris: nt*3 indices;
+ * tri_material: nt slots or NULL (all 0); cavity: nv floats or NULL.
+ */
+int argent_piece_upload(ArgentCtx* ctx, const float* positions, uint32_t nv, const float* normals,
+                        const uint32_t* tris, uint32_t nt, const uint16_t* tri_material,
+                        const float* cavity, ArgentPiece** out);
+void argent_piece_destroy(ArgentPiece* piece);
+/* Root bounds, as `Piece::bounds` (scene.rs:34-37). */
+int argent_piece_bounds(const ArgentPiece* piece, float lo[3], float hi[3]);
+/* Bytes the piece holds on the device. */
+uint64_t argent_piece_device_bytes(const ArgentPiece* piece);
+
+/* Build a scene around a piece.  Replaces `Scene::new` + `rebuild_lights`
+ * (scene.rs:82-110) and, for a map environment, `EnvData::load`'s table build
+ * (envmap.rs:141-177).  The piece must outlive the scene. */
+int argent_scene_upload(ArgentCtx* ctx, ArgentPiece* piece, const ArgentSceneDesc* desc, ArgentScene** out);
+void argent_scene_destroy(ArgentScene* scene);
+/* Replace the turntable angle of an uploaded scene (scene.rs:53-55). */
+int argent_scene_set_turntable(ArgentScene* scene, float turntable_deg);
+
+/* A film of width x height pixels.  Replaces `Film::new` (render.rs:24-27). */
+int argent_film_create(ArgentCtx* ctx, uint32_t width, uint32_t height, uint32_t flags, ArgentFilm** out);
+void argent_film_destroy(ArgentFilm* film);
+/* `Film::clear` (render.rs:29-34). */
+int argent_film_clear(ArgentFilm* film);
+/* `film.samples`: the next sample index (render.rs:19-20, 70). */
+uint32_t argent_film_samples(const ArgentFilm* film);
+/*
+ * Averages as `Film::color`, `Film::albedo`, `Film::normal` (render.rs:36-62):
+ * width*height*3 floats each, any pointer may be NULL.  color is camera RGB
+ * (the scene's white balance applied, render.rs:74,96).
+ */
+int argent_film_read(ArgentFilm* film, float* color, float* albedo, float* normal);
+/* Average CIE XYZ per pixel (width*height*3), before the camera matrix. */
+int argent_film_read_xyz(ArgentFilm* film, float* xyz);
+
+/*
+ * Render `count` more samples per pixel.  Replaces `render_pass`
+ * (render.rs:67-115) with the same semantics: sample indices run from
+ * film.samples to film.samples+count-1, per-pixel seeding
+ * hash32((y*w+x) ^ hash32(seed ^ 0xa511e9b3)), non-finite samples dropped.
+ * Asynchronous on the context stream; argent_film_read synchronises.
+ */
+int argent_render_pass(ArgentCtx* ctx, ArgentScene* scene, const ArgentCamera* camera, ArgentFilm* film,
+                       const ArgentPathSettings* settings, uint32_t count, uint32_t seed);
+
+/* ------------------------------------------------------------------ */
+/* Traversal primitives.                                              */
+/* ------------------------------------------------------------------ */
+
+/*
+ * Closest hit of n object-space rays against a piece, t in (1e-7, tmax).
+ * Replaces `Bvh::intersect` (bvh.rs:159-212); prim is the original triangle
+ * index.  Host arrays; synchronous.
+ */
+int argent_trace_closest(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* rays, uint64_t n, ArgentHit* hits);
+/* Any hit; occluded[i] = 1 when some triangle has t in (1e-7, tmax).
+ * Replaces `Bvh::occluded` (bvh.rs:216-247).  Host arrays; synchronous. */
+int argent_trace_anyhit(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* rays, uint64_t n, uint8_t* occluded);
+/* Device-pointer variants (asynchronous on the context stream). */
+int argent_trace_closest_device(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* d_rays, uint64_t n,
+                                ArgentHit* d_hits);
+int argent_trace_anyhit_device(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* d_rays, uint64_t n,
+                               uint8_t* d_occluded);
+
+/* ------------------------------------------------------------------ */
+/* Batched renders (argent `turntable` / `sheet` loops).              */
+/* ------------------------------------------------------------------ */
+
+/*
+ * One item of a batch: a render_pass call.  The items of one batch run as
+ * one persistent launch sequence in which waves of different items
+ * overlap.  Each item's film receives exactly what argent_render_pass would
+ * give for the same arguments.  Replaces the per-frame `render_image` loops
+ * of `render_reel` (argent/src/jobs.rs:595-713) and `sheet_prepared`
+ * (jobs.rs:857-889).
+ */
+typedef struct ArgentBatchItem {
+  ArgentScene* scene;
+  ArgentCamera camera;
+  ArgentFilm* film;
+  ArgentPathSettings settings;
+  uint32_t count;
+  uint32_t seed;
+} ArgentBatchItem;
+
+int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n);
+
+/* Kernels the library has launched on this context since creation. */
+uint64_t argent_ctx_kernel_launches(const ArgentCtx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ARGENT_GPU_H */

@@ -1,0 +1,156 @@
+"""CPU oracle: a restatement of argent's render hot path (test infrastructure).
+
+liboracle.so restates crates/argent-core/src/{render,integrator,scene,bvh,
+camera,sampler,light,envmap,material,bsdf,microfacet,color}.rs and the
+argent-spectra primitives they call, operation by operation, compiled with
+-ffp-contract=off.  Only the tests, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg load it, as the checker; the product never does.
+
+Parity pinning: the BVH build/traversal, Fresnel, GGX, wavelength sampling,
+CIE and white-balance restatements are checked against argent's own unit-test
+known answers (tests/test_oracle_golden.py).  The sampler's Sobol values come
+from argent's unvendored sobol_burley 0.5.0 crate and are replaced by a
+published Burley-2020 construction shared with the CUDA path, so exact sample
+streams of argent's binary are unpinned (only the oracle/GPU pair is).
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SO = os.path.join(HERE, "liboracle.so")
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(SO):
+            raise OSError(f"{SO} missing: run `make -C oracle` (or python -m argent_b200.build)")
+        from argent_b200 import _native as N
+
+        L = ctypes.CDLL(SO)
+        vp, u32, u64, f = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_float
+        fp = ctypes.POINTER(ctypes.c_float)
+        sig = {
+            "oracle_bvh_create": (vp, [vp, u32, vp, u32]),
+            "oracle_bvh_destroy": (None, [vp]),
+            "oracle_bvh_intersect": (None, [vp, vp, u64, vp, ctypes.c_int]),
+            "oracle_bvh_occluded": (None, [vp, vp, u64, vp, ctypes.c_int]),
+            "oracle_bvh_intersect_binary": (None, [vp, vp, u64, vp]),
+            "oracle_brute_intersect": (None, [vp, vp, u32, vp, u64, vp, ctypes.c_int]),
+            "oracle_tri_hit": (ctypes.c_int, [vp, vp, u32, vp, fp, fp, fp]),
+            "oracle_bvh_stats": (None, [vp, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u32)]),
+            "oracle_scene_create": (vp, [vp, u32, vp, vp, u32, vp, vp, ctypes.POINTER(N.ArgentSceneDesc)]),
+            "oracle_scene_destroy": (None, [vp]),
+            "oracle_scene_set_turntable": (None, [vp, f]),
+            "oracle_render_pass": (None, [vp, ctypes.POINTER(N.ArgentCamera), ctypes.POINTER(N.ArgentPathSettings),
+                                          u32, u32, u32, u32, u32, u32, u32, vp, vp, vp, vp, ctypes.c_int]),
+            "oracle_trace_sample": (None, [vp, ctypes.POINTER(N.ArgentCamera), ctypes.POINTER(N.ArgentPathSettings),
+                                           u32, u32, u32, u32, u32, u32, fp]),
+            "oracle_camera_matrix": (None, [ctypes.c_int, fp, fp]),
+            "oracle_fresnel_dielectric": (f, [f, f]),
+            "oracle_fresnel_conductor": (f, [f, f, f]),
+            "oracle_ggx_e": (f, [f, f]),
+            "oracle_ggx_sample_h": (None, [f, fp, f, f, fp]),
+            "oracle_energy_table": (None, [fp]),
+            "oracle_sample_visible": (None, [f, fp, fp]),
+            "oracle_to_xyz": (None, [fp, fp, fp, fp]),
+            "oracle_xyz_bar": (None, [f, fp]),
+            "oracle_linear_rgb": (None, [fp, fp]),
+            "oracle_hash32": (u32, [u32]),
+            "oracle_sampler_next": (None, [u32, u32, u32, fp]),
+            "oracle_sampler_random": (None, [u32, u32, u32, fp]),
+            "oracle_sobol_4d": (None, [u32, u32, u32, fp]),
+            "oracle_sobol_raw": (None, [u32, ctypes.c_int, ctypes.POINTER(u32)]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+class Bvh:
+    """argent's BVH (bvh.rs) over a triangle mesh."""
+
+    def __init__(self, positions, tris):
+        self.positions = np.ascontiguousarray(positions, np.float32)
+        self.tris = np.ascontiguousarray(tris, np.uint32)
+        self.h = lib().oracle_bvh_create(_ptr(self.positions), len(self.positions), _ptr(self.tris), len(self.tris))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_bvh_destroy(self.h)
+            self.h = None
+
+    def intersect(self, rays, threads=0):
+        hits = np.zeros((len(rays), 4), np.float32)
+        lib().oracle_bvh_intersect(self.h, _ptr(rays), len(rays), _ptr(hits), threads)
+        return hits
+
+    def intersect_binary(self, rays):
+        hits = np.zeros((len(rays), 4), np.float32)
+        lib().oracle_bvh_intersect_binary(self.h, _ptr(rays), len(rays), _ptr(hits))
+        return hits
+
+    def occluded(self, rays, threads=0):
+        occ = np.zeros(len(rays), np.uint8)
+        lib().oracle_bvh_occluded(self.h, _ptr(rays), len(rays), _ptr(occ), threads)
+        return occ
+
+    def brute(self, rays, threads=0):
+        hits = np.zeros((len(rays), 4), np.float32)
+        lib().oracle_brute_intersect(_ptr(self.positions), _ptr(self.tris), len(self.tris), _ptr(rays), len(rays),
+                                     _ptr(hits), threads)
+        return hits
+
+    def tri_hit(self, prim, ray):
+        t, u, v = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        r = np.ascontiguousarray(ray, np.float32)
+        ok = lib().oracle_tri_hit(_ptr(self.positions), _ptr(self.tris), int(prim), _ptr(r), ctypes.byref(t),
+                                  ctypes.byref(u), ctypes.byref(v))
+        return bool(ok), t.value, u.value, v.value
+
+    def stats(self):
+        a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint32()
+        lib().oracle_bvh_stats(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return a.value, b.value, c.value
+
+
+class Scene:
+    """argent's Scene + render_pass on the CPU, from the same C-ABI description."""
+
+    def __init__(self, mesh, desc):
+        self.mesh = mesh  # keep arrays alive
+        p, n, t, m, c = mesh.positions, mesh.normals, mesh.tris, mesh.tri_material, mesh.cavity
+        self.h = lib().oracle_scene_create(_ptr(p), len(p), _ptr(n), _ptr(t), len(t), _ptr(m), _ptr(c),
+                                           ctypes.byref(desc))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_scene_destroy(self.h)
+            self.h = None
+
+    def set_turntable(self, deg):
+        lib().oracle_scene_set_turntable(self.h, float(deg))
+
+    def render_pass(self, cam, settings, w, h, first, count, seed, rows=None, threads=0, want_xyz=True):
+        """Film sums as argent accumulates them (camera RGB), plus XYZ sums
+        (float64) and the guides.  rows=(y0, y1) restricts to a band."""
+        y0, y1 = rows if rows else (0, h)
+        color = np.zeros((h, w, 3), np.float32)
+        albedo = np.zeros((h, w, 3), np.float32)
+        normal = np.zeros((h, w, 3), np.float32)
+        xyz = np.zeros((h, w, 3), np.float64) if want_xyz else None
+        lib().oracle_render_pass(self.h, ctypes.byref(cam), ctypes.byref(settings), w, h, first, count, seed, y0, y1,
+                                 _ptr(color), _ptr(albedo), _ptr(normal), _ptr(xyz), threads)
+        return color, albedo, normal, xyz

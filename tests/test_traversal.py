@@ -1,0 +1,165 @@
+"""Closest-hit / any-hit parity of the CUDA traversal against the oracle.
+
+Gate (from the hot path's correctness rule): the closest-hit triangle index
+is bit-exact against argent's CPU BVH traversal (restated in the oracle) on
+2^24 seeded rays over the 65,536-triangle ring, and the hit distance t is
+within 2 ulp.  Equal-t ties (a ray through a shared edge hits two
+triangles at the same t) are reported in their own bucket: argent keeps the
+first in its traversal order, the GPU keeps the lower triangle index.
+"""
+
+import numpy as np
+import pytest
+
+from tests.rays import compare_hits, make_rays
+
+
+@pytest.fixture(scope="module")
+def ring():
+    from argent_b200 import mesh
+
+    return mesh.ring()
+
+
+def test_ring_mesh_shape(ring):
+    assert ring.num_tris == 65536
+    assert ring.positions.shape == (512 * 64, 3)
+    lo, hi = ring.bounds()
+    assert np.all(hi - lo > 2.0)
+
+
+def test_ray_generator_is_deterministic(ring):
+    a = make_rays(ring.positions, ring.tris, 1000)
+    b = make_rays(ring.positions, ring.tris, 1000)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    d = a[:, 4:7]
+    assert np.all(np.abs(np.linalg.norm(d, axis=1) - 1) < 1e-5)
+    assert np.any(d == 0.0)  # axis-snapped rays present
+
+
+def test_oracle_bvh_on_ring_matches_brute_force(ring):
+    import oracle as O
+
+    bvh = O.Bvh(ring.positions, ring.tris)
+    rays = make_rays(ring.positions, ring.tris, 3000, seed=11)
+    a = bvh.intersect(rays)
+    b = bvh.brute(rays)
+    ah = a[:, 3].view(np.uint32)
+    bh = b[:, 3].view(np.uint32)
+    assert np.array_equal(ah != 0xFFFFFFFF, bh != 0xFFFFFFFF)
+    hit = ah != 0xFFFFFFFF
+    assert np.all(np.abs(a[hit, 0] - b[hit, 0]) < 1e-4)
+
+
+def _ctx():
+    from argent_b200.gpu import Context
+
+    return Context(0)
+
+
+@pytest.mark.gpu
+def test_closest_hit_parity_ring_2p24(ring):
+    import oracle as O
+    from argent_b200.gpu import Piece
+
+    ctx = _ctx()
+    piece = Piece(ctx, ring)
+    bvh = O.Bvh(ring.positions, ring.tris)
+    n = 1 << 24
+    rays = make_rays(ring.positions, ring.tris, n, seed=8)
+    got = piece.trace_closest(rays)
+    ref = bvh.intersect(rays)
+    r = compare_hits(ref, got, bvh, rays)
+    print("closest-hit parity (ring, 2^24 rays):", {k: v for k, v in r.items() if k != "mismatch_idx"})
+    assert r["hit_both"] > n // 4
+    assert r["mismatch"] == 0, r["mismatch_idx"]
+    assert r["t_ulp_fail"] == 0
+    assert r["tie"] <= n // 100000
+
+
+@pytest.mark.gpu
+def test_anyhit_parity_ring(ring):
+    import oracle as O
+    from argent_b200.gpu import Piece
+
+    ctx = _ctx()
+    piece = Piece(ctx, ring)
+    bvh = O.Bvh(ring.positions, ring.tris)
+    rays = make_rays(ring.positions, ring.tris, 1 << 20, seed=9)
+    # finite tmax on half the rays, as shadow rays to a light point have
+    rays[::2, 3] = np.float32(5.0)
+    got = piece.trace_anyhit(rays)
+    ref = bvh.occluded(rays)
+    assert np.array_equal(got, ref)
+    # any-hit agrees with closest-hit within tmax
+    assert got.sum() > 1000
+
+
+@pytest.mark.gpu
+def test_closest_hit_finite_tmax_and_tiny_pieces():
+    import oracle as O
+    from argent_b200.gpu import Piece
+    from argent_b200.mesh import Mesh
+
+    ctx = _ctx()
+    # one triangle
+    m = Mesh(np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32), np.array([[0, 1, 2]], np.uint32))
+    piece = Piece(ctx, m)
+    rays = np.zeros((4, 8), np.float32)
+    rays[:, 0:3] = [[0.2, 0.2, 1], [0.2, 0.2, 1], [2, 2, 1], [0.2, 0.2, -1]]
+    rays[:, 4:7] = [[0, 0, -1], [0, 0, -1], [0, 0, -1], [0, 0, -1]]
+    rays[:, 3] = [np.inf, 0.5, np.inf, np.inf]
+    got = piece.trace_closest(rays)
+    bvh = O.Bvh(m.positions, m.tris)
+    ref = bvh.intersect(rays)
+    assert np.array_equal(got[:, 3].view(np.uint32), ref[:, 3].view(np.uint32))
+    assert got[0, 3].view(np.uint32) == 0 and got[0, 0] == np.float32(1.0)
+    assert got[1, 3].view(np.uint32) == 0xFFFFFFFF  # beyond tmax
+    assert got[2, 3].view(np.uint32) == 0xFFFFFFFF  # outside
+    assert got[3, 3].view(np.uint32) == 0xFFFFFFFF  # behind (t <= 1e-7)
+    # degenerate triangle only: |det| < 1e-14 rejects, never hits
+    m2 = Mesh(np.array([[0, 0, 0], [1, 0, 0], [2, 0, 0]], np.float32), np.array([[0, 1, 2]], np.uint32))
+    p2 = Piece(ctx, m2)
+    r2 = np.zeros((1, 8), np.float32)
+    r2[0, 0:3] = [0.5, 1, 0]
+    r2[0, 4:7] = [0, -1, 0]
+    r2[0, 3] = np.inf
+    assert p2.trace_closest(r2)[0, 3].view(np.uint32) == 0xFFFFFFFF
+
+
+@pytest.mark.gpu
+def test_empty_piece_misses():
+    from argent_b200.gpu import Piece
+    from argent_b200.mesh import Mesh
+
+    ctx = _ctx()
+    m = Mesh(np.zeros((0, 3), np.float32), np.zeros((0, 3), np.uint32))
+    piece = Piece(ctx, m)
+    rays = np.zeros((16, 8), np.float32)
+    rays[:, 4] = 1.0
+    rays[:, 3] = np.inf
+    got = piece.trace_closest(rays)
+    assert np.all(got[:, 3].view(np.uint32) == 0xFFFFFFFF)
+    assert not piece.trace_anyhit(rays).any()
+
+
+@pytest.mark.gpu
+def test_closest_hit_parity_signet_2p22():
+    """The 2.1M-triangle signet piece, 2^22 rays."""
+    import oracle as O
+    from argent_b200 import mesh
+    from argent_b200.gpu import Piece
+
+    m = mesh.signet()
+    assert m.num_tris == 2097152
+    ctx = _ctx()
+    piece = Piece(ctx, m)
+    bvh = O.Bvh(m.positions, m.tris)
+    n = 1 << 22
+    rays = make_rays(m.positions, m.tris, n, seed=8)
+    got = piece.trace_closest(rays)
+    ref = bvh.intersect(rays)
+    r = compare_hits(ref, got, bvh, rays)
+    print("closest-hit parity (signet, 2^22 rays):", {k: v for k, v in r.items() if k != "mismatch_idx"})
+    assert r["mismatch"] == 0, r["mismatch_idx"]
+    assert r["t_ulp_fail"] == 0
