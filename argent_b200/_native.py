@@ -143,7 +143,36 @@ GPU_FUNCS = {
     "argent_render_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ArgentBatchItem), ctypes.c_uint32]),
 }
 
+_f, _i32, _u32, _cp = ctypes.c_float, ctypes.c_int32, ctypes.c_uint32, ctypes.c_char_p
+_i32p = ctypes.POINTER(ctypes.c_int32)
 HOST_FUNCS = {
+    "argent_metal_nk": (ctypes.c_int, [_cp, c_float_p, c_float_p]),
+    "argent_alloy_nk": (ctypes.c_int, [_cp, c_float_p, c_float_p]),
+    "argent_karat_gold_nk": (ctypes.c_int, [_f, _f, _f, c_float_p, c_float_p]),
+    "argent_nk_f0_srgb": (None, [c_float_p, c_float_p, c_float_p]),
+    "argent_luminance_y": (_f, [c_float_p]),
+    "argent_bake_emitter": (None, [_f, _f, c_float_p]),
+    "argent_bake_rgb_albedo": (None, [c_float_p, c_float_p]),
+    "argent_rgb_albedo_coefficients": (ctypes.c_int, [c_float_p, c_float_p]),
+    "argent_bake_rgb_illuminant": (None, [c_float_p, c_float_p]),
+    "argent_reflectance_srgb": (None, [c_float_p, c_float_p]),
+    "argent_blackbody_white": (None, [_f, c_float_p]),
+    "argent_gem_tables": (ctypes.c_int, [_cp, _i32p, c_float_p, c_float_p, c_float_p]),
+    "argent_gem_dispersion": (ctypes.c_int, [_cp, c_float_p, c_float_p, c_float_p]),
+    "argent_material_metal": (ctypes.c_int, [_cp, _f, _f, ctypes.POINTER(ArgentMaterial)]),
+    "argent_material_metal_nk": (ctypes.c_int, [c_float_p, c_float_p, _f, ctypes.POINTER(ArgentMaterial)]),
+    "argent_material_gem": (ctypes.c_int, [_cp, ctypes.POINTER(ArgentMaterial)]),
+    "argent_material_opal": (None, [ctypes.c_int, _f, ctypes.POINTER(ArgentMaterial)]),
+    "argent_material_plastic": (None, [c_float_p, _f, _f, ctypes.POINTER(ArgentMaterial)]),
+    "argent_material_diffuse": (None, [c_float_p, ctypes.POINTER(ArgentMaterial)]),
+    "argent_material_black": (None, [ctypes.POINTER(ArgentMaterial)]),
+    "argent_studio_build": (ctypes.c_int, [_cp, _f, _f, ctypes.POINTER(ArgentPanel), _i32p, ctypes.POINTER(ArgentEnv),
+                                           ctypes.POINTER(ArgentMaterial), ctypes.POINTER(ArgentFloor), _i32p,
+                                           c_float_p]),
+    "argent_camera_look_at": (None, [c_float_p, c_float_p, c_float_p, _f, _f, _f, ctypes.POINTER(ArgentCamera)]),
+    "argent_view_named": (ctypes.c_int, [_cp, c_float_p, c_float_p, c_float_p]),
+    "argent_frame": (None, [c_float_p, _u32, _f, _f, _f, _f, _f, _f, ctypes.POINTER(ArgentCamera)]),
+    "argent_synth_hdri": (None, [_u32, _u32, _f, _u32, c_float_p]),
     "argent_mesh_free": (None, [ctypes.POINTER(ArgentMesh)]),
     "argent_synth_ring": (ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32,
                                          ctypes.c_float, ctypes.c_float, ctypes.c_uint32, ctypes.POINTER(ArgentMesh)]),

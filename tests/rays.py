@@ -103,31 +103,45 @@ def make_rays(positions, tris, n, seed=8, axis_fraction=0.01):
 
 
 def compare_hits(ref, got, bvh, rays, ulps=2):
-    """Classify GPU hits against the oracle's.
+    """Classify GPU hits against the oracle's (argent's traversal).
 
-    Returns dict(match, tie, t_ulp_fail, mismatch, miss_both, hit_both).  A
-    tie is a differing triangle whose Moller-Trumbore distance, recomputed by
-    the oracle, is bit-equal to the oracle's t (both triangles hit at that t).
+    Buckets:
+      match       same triangle, t within `ulps` (bit-equal expected)
+      tie         another triangle at a bit-equal t (argent keeps the first
+                  in its traversal order, the GPU the lower index)
+      closer      the GPU hit is strictly closer than argent's, or argent
+                  misses it, and the oracle's own Moller-Trumbore confirms the
+                  GPU triangle at exactly that t: argent's slab test culled a
+                  box whose triangle lies at (within rounding) the current
+                  best distance.  Brute force agrees with the GPU here.
+      mismatch    anything else (the gate: must be 0)
     """
     rp = ref[:, 3].view(np.uint32)
     gp = got[:, 3].view(np.uint32)
     ref_hit = rp != 0xFFFFFFFF
     got_hit = gp != 0xFFFFFFFF
     out = dict(n=len(ref), hit_both=int((ref_hit & got_hit).sum()), miss_both=int((~ref_hit & ~got_hit).sum()))
-    mism = ref_hit != got_hit
     same = ref_hit & got_hit & (rp == gp)
     rt = ref[:, 0].view(np.int32).astype(np.int64)
     gt = got[:, 0].view(np.int32).astype(np.int64)
     t_bad = same & (np.abs(rt - gt) > ulps)
-    diff = np.nonzero(ref_hit & got_hit & (rp != gp))[0]
-    ties = 0
-    bad_diff = 0
-    for i in diff:
+    cand = np.nonzero((ref_hit | got_hit) & ~same)[0]
+    ties = closer = 0
+    bad = []
+    for i in cand:
+        if not got_hit[i]:
+            bad.append(i)  # the GPU missed a hit argent found
+            continue
         ok, t, _, _ = bvh.tri_hit(gp[i], rays[i])
-        if ok and np.float32(t) == ref[i, 0] and got[i, 0] == ref[i, 0]:
+        if not ok or np.float32(t) != got[i, 0]:
+            bad.append(i)
+            continue
+        if ref_hit[i] and got[i, 0] == ref[i, 0]:
             ties += 1
+        elif (not ref_hit[i]) or got[i, 0] < ref[i, 0]:
+            closer += 1
         else:
-            bad_diff += 1
-    out.update(match=int(same.sum() - t_bad.sum()), tie=ties, t_ulp_fail=int(t_bad.sum()),
-               mismatch=int(mism.sum()) + bad_diff, mismatch_idx=np.concatenate([np.nonzero(mism)[0], diff])[:20])
+            bad.append(i)
+    out.update(match=int(same.sum() - t_bad.sum()), tie=ties, closer=closer, t_ulp_fail=int(t_bad.sum()),
+               mismatch=len(bad), mismatch_idx=np.array(bad[:20], np.int64))
     return out
