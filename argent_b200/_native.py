@@ -141,7 +141,13 @@ GPU_FUNCS = {
     "argent_trace_anyhit_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_uint64, ctypes.c_void_p]),
     "argent_render_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ArgentBatchItem), ctypes.c_uint32]),
+    "argent_ctx_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "argent_ctx_kernel_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                               ctypes.POINTER(ctypes.c_uint64)]),
+    "argent_ctx_set_counting": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "argent_ctx_traversal_counts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
 }
+KERNEL_CLASSES = ["raygen", "intersect", "shade", "shadow", "film", "trace"]
 
 _f, _i32, _u32, _cp = ctypes.c_float, ctypes.c_int32, ctypes.c_uint32, ctypes.c_char_p
 _i32p = ctypes.POINTER(ctypes.c_int32)

@@ -104,6 +104,53 @@ int grid_for(const ArgentCtx* ctx, const void* kernel, int block, uint64_t n) {
   return (int)std::max<uint64_t>(g, 1);
 }
 
+// ------------------------------------------------------------------ kernel timing
+
+static cudaEvent_t prof_event(ArgentCtx* ctx) {
+  if (!ctx->prof.pool.empty()) {
+    cudaEvent_t e = ctx->prof.pool.back();
+    ctx->prof.pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Brackets one launch with events on the context stream when profiling.
+struct ProfScope {
+  ArgentCtx* ctx;
+  int kind;
+  cudaEvent_t a = nullptr;
+  ProfScope(ArgentCtx* c, int k) : ctx(c), kind(k) {
+    if (ctx->prof.on) {
+      a = prof_event(ctx);
+      cudaEventRecord(a, ctx->stream);
+    }
+  }
+  ~ProfScope() {
+    if (a) {
+      cudaEvent_t b = prof_event(ctx);
+      cudaEventRecord(b, ctx->stream);
+      ctx->prof.ev[kind].push_back({a, b});
+    }
+  }
+};
+
+static void prof_collect(ArgentCtx* ctx) {
+  cudaStreamSynchronize(ctx->stream);
+  for (int k = 0; k < KC_COUNT; ++k) {
+    for (auto& pr : ctx->prof.ev[k]) {
+      float ms = 0.0f;
+      if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) ctx->prof.ms[k] += ms;
+      ctx->prof.n[k] += 1;
+      ctx->prof.pool.push_back(pr.first);
+      ctx->prof.pool.push_back(pr.second);
+    }
+    ctx->prof.ev[k].clear();
+  }
+}
+
 extern "C" {
 
 const char* argent_last_error(const ArgentCtx* ctx) {
@@ -146,6 +193,8 @@ void argent_ctx_destroy(ArgentCtx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  prof_collect(ctx);
+  for (cudaEvent_t e : ctx->prof.pool) cudaEventDestroy(e);
   ctx->wave.release();
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -260,7 +309,10 @@ int argent_trace_closest_device(ArgentCtx* ctx, ArgentPiece* piece, const Argent
   ARGENT_CK(ctx, cudaSetDevice(ctx->device));
   int block = 128;
   int grid = grid_for(ctx, (const void*)k_trace_closest, block, n);
-  k_trace_closest<<<grid, block, 0, ctx->stream>>>(piece->dev, d_rays, n, d_hits, ctx->d_status);
+  {
+    ProfScope ps(ctx, KC_TRACE);
+    k_trace_closest<<<grid, block, 0, ctx->stream>>>(piece->dev, d_rays, n, d_hits, ctx->d_status);
+  }
   ctx->launches++;
   ARGENT_CK(ctx, cudaGetLastError());
   return ARGENT_OK;
@@ -273,7 +325,10 @@ int argent_trace_anyhit_device(ArgentCtx* ctx, ArgentPiece* piece, const ArgentR
   ARGENT_CK(ctx, cudaSetDevice(ctx->device));
   int block = 128;
   int grid = grid_for(ctx, (const void*)k_trace_any, block, n);
-  k_trace_any<<<grid, block, 0, ctx->stream>>>(piece->dev, d_rays, n, d_occ, ctx->d_status);
+  {
+    ProfScope ps(ctx, KC_TRACE);
+    k_trace_any<<<grid, block, 0, ctx->stream>>>(piece->dev, d_rays, n, d_occ, ctx->d_status);
+  }
   ctx->launches++;
   ARGENT_CK(ctx, cudaGetLastError());
   return ARGENT_OK;
@@ -472,17 +527,32 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
     const dev::WaveDesc& w = waves[wi];
     a.q_in = wb.q0;
     a.q_out = wb.q1;
-    dev::k_raygen<<<g_ray, 256, 0, ctx->stream>>>(a, w);
+    {
+      ProfScope ps(ctx, KC_RAYGEN);
+      dev::k_raygen<<<g_ray, 256, 0, ctx->stream>>>(a, w);
+    }
     ctx->launches++;
     for (uint32_t depth = 0; depth < depths[wi] && depth < ARGENT_MAX_DEPTH; ++depth) {
       a.q_in = (depth & 1) ? wb.q1 : wb.q0;
       a.q_out = (depth & 1) ? wb.q0 : wb.q1;
-      dev::k_intersect<<<g_int, 128, 0, ctx->stream>>>(a, (int)depth);
-      dev::k_shade<<<g_sh, 128, 0, ctx->stream>>>(a, (int)depth, cap);
-      dev::k_shadow<<<g_any, 128, 0, ctx->stream>>>(a, (int)depth);
+      {
+        ProfScope ps(ctx, KC_INTERSECT);
+        dev::k_intersect<<<g_int, 128, 0, ctx->stream>>>(a, (int)depth);
+      }
+      {
+        ProfScope ps(ctx, KC_SHADE);
+        dev::k_shade<<<g_sh, 128, 0, ctx->stream>>>(a, (int)depth, cap);
+      }
+      {
+        ProfScope ps(ctx, KC_SHADOW);
+        dev::k_shadow<<<g_any, 128, 0, ctx->stream>>>(a, (int)depth);
+      }
       ctx->launches += 3;
     }
-    dev::k_film<<<g_film, 256, 0, ctx->stream>>>(a, w);
+    {
+      ProfScope ps(ctx, KC_FILM);
+      dev::k_film<<<g_film, 256, 0, ctx->stream>>>(a, w);
+    }
     ctx->launches++;
   }
   cudaError_t e = cudaGetLastError();
@@ -852,6 +922,54 @@ int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n
     items[i].film->has_matrix = true;
     std::memcpy(items[i].film->cam_m, items[i].scene->cam_m, sizeof(float) * 9);
   }
+  return ARGENT_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int argent_ctx_set_profiling(ArgentCtx* ctx, int on) {
+  if (!ctx) return set_error(nullptr, ARGENT_E_INVALID, "ctx is NULL");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  prof_collect(ctx);
+  ctx->prof.on = on != 0;
+  for (int k = 0; k < KC_COUNT; ++k) {
+    ctx->prof.ms[k] = 0.0;
+    ctx->prof.n[k] = 0;
+  }
+  return ARGENT_OK;
+}
+
+int argent_ctx_kernel_times(ArgentCtx* ctx, double* ms, uint64_t* launches) {
+  if (!ctx || !ms || !launches) return set_error(ctx, ARGENT_E_INVALID, "NULL argument");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  prof_collect(ctx);
+  for (int k = 0; k < KC_COUNT; ++k) {
+    ms[k] = ctx->prof.ms[k];
+    launches[k] = ctx->prof.n[k];
+  }
+  return ARGENT_OK;
+}
+
+int argent_ctx_set_counting(ArgentCtx* ctx, int on) {
+  if (!ctx) return set_error(nullptr, ARGENT_E_INVALID, "ctx is NULL");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  int v = on ? 1 : 0;
+  unsigned long long z[6] = {0, 0, 0, 0, 0, 0};
+  ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_trav_counting, &v, sizeof(v)));
+  ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_trav_counts, z, sizeof(z)));
+  return ARGENT_OK;
+}
+
+int argent_ctx_traversal_counts(ArgentCtx* ctx, uint64_t* out6) {
+  if (!ctx || !out6) return set_error(ctx, ARGENT_E_INVALID, "NULL argument");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  unsigned long long z[6];
+  ARGENT_CK(ctx, cudaMemcpyFromSymbol(z, dev::d_trav_counts, sizeof(z)));
+  for (int i = 0; i < 6; ++i) out6[i] = z[i];
   return ARGENT_OK;
 }
 

@@ -12,5 +12,9 @@ __device__ uint32_t d_sobol_dirs[4][32];
 __device__ float d_energy_table[32 * 32];
 // CIE 1931 2-degree colour matching functions, 1 nm, 360..=830 (cie.rs:38-49).
 __device__ float d_cmf[471 * 3];
+// Traversal instrumentation (off unless the host enables it): closest-hit
+// rays, nodes, triangles; any-hit rays, nodes, triangles.
+__device__ int d_trav_counting;
+__device__ unsigned long long d_trav_counts[6];
 
 }  // namespace dev

@@ -14,6 +14,7 @@
 // hits in its own traversal order; the parity tests bucket such exact ties.
 #pragma once
 #include "dev_math.cuh"
+#include "tables.cuh"
 
 namespace dev {
 
@@ -136,6 +137,15 @@ struct TraceHit {
   uint32_t prim;
 };
 
+// Adds one ray's node and triangle visits to the instrumentation counters.
+__device__ __forceinline__ void count_visits(int base, uint32_t nodes, uint32_t tris) {
+  if (d_trav_counting) {
+    atomicAdd(&d_trav_counts[base], 1ull);
+    atomicAdd(&d_trav_counts[base + 1], (unsigned long long)nodes);
+    atomicAdd(&d_trav_counts[base + 2], (unsigned long long)tris);
+  }
+}
+
 // Closest hit with t in (1e-7, t_max).  Ties at equal t go to the lower
 // original triangle index.
 __device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, float t_max, uint32_t* status) {
@@ -144,6 +154,7 @@ __device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, f
   V3 inv{__fdiv_rn(1.0f, d.x), __fdiv_rn(1.0f, d.y), __fdiv_rn(1.0f, d.z)};
   uint2 stack[ARGENT_STACK_SIZE];
   int sp = 0;
+  uint32_t n_nodes = 0, n_tris = 0;
   stack[sp++] = make_uint2(0u, __float_as_uint(0.0f));
   while (sp > 0) {
     --sp;
@@ -153,6 +164,7 @@ __device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, f
     if (ref & ARGENT_LEAF_BIT) {
       uint32_t start = ref & 0x07FFFFFFu;
       uint32_t cnt = ((ref >> 27) & 15u) + 1u;
+      n_tris += cnt;
       for (uint32_t i = 0; i < cnt; ++i) {
         float t, u, v;
         uint32_t prim;
@@ -170,6 +182,7 @@ __device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, f
       continue;
     }
     NodeView n = load_node(pc.nodes, ref);
+    ++n_nodes;
     float tc[8];
     uint32_t hitmask = 0;
 #pragma unroll
@@ -198,6 +211,7 @@ __device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, f
     }
     sp += nh;
   }
+  count_visits(0, n_nodes, n_tris);
   return best;
 }
 
@@ -207,6 +221,7 @@ __device__ __noinline__ bool trace_any(const DevPiece& pc, V3 o, V3 d, float t_m
   V3 inv{__fdiv_rn(1.0f, d.x), __fdiv_rn(1.0f, d.y), __fdiv_rn(1.0f, d.z)};
   uint32_t stack[ARGENT_STACK_SIZE];
   int sp = 0;
+  uint32_t n_nodes = 0, n_tris = 0;
   stack[sp++] = 0u;
   while (sp > 0) {
     uint32_t ref = stack[--sp];
@@ -216,11 +231,16 @@ __device__ __noinline__ bool trace_any(const DevPiece& pc, V3 o, V3 d, float t_m
       for (uint32_t i = 0; i < cnt; ++i) {
         float t, u, v;
         uint32_t prim;
-        if (mt_hit(pc.tris + 3 * (size_t)(start + i), o, d, t_max, &t, &u, &v, &prim)) return true;
+        ++n_tris;
+        if (mt_hit(pc.tris + 3 * (size_t)(start + i), o, d, t_max, &t, &u, &v, &prim)) {
+          count_visits(3, n_nodes, n_tris);
+          return true;
+        }
       }
       continue;
     }
     NodeView n = load_node(pc.nodes, ref);
+    ++n_nodes;
     uint32_t hitmask = 0;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
@@ -239,6 +259,7 @@ __device__ __noinline__ bool trace_any(const DevPiece& pc, V3 o, V3 d, float t_m
       stack[sp++] = child_ref(n, c);
     }
   }
+  count_visits(3, n_nodes, n_tris);
   return false;
 }
 

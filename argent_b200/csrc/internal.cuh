@@ -113,6 +113,16 @@ struct WaveBuffers {
   }
 };
 
+// Per-kernel-class CUDA event pairs recorded while profiling is on.
+enum { KC_RAYGEN = 0, KC_INTERSECT, KC_SHADE, KC_SHADOW, KC_FILM, KC_TRACE, KC_COUNT };
+struct KernelProfile {
+  bool on = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[KC_COUNT];
+  std::vector<cudaEvent_t> pool;
+  double ms[KC_COUNT] = {0, 0, 0, 0, 0, 0};
+  uint64_t n[KC_COUNT] = {0, 0, 0, 0, 0, 0};
+};
+
 struct ArgentCtx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -123,6 +133,7 @@ struct ArgentCtx {
   uint32_t* d_status = nullptr;
   bool tables_ready = false;
   WaveBuffers wave;
+  KernelProfile prof;
 };
 
 struct ArgentPiece {

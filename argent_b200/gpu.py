@@ -50,6 +50,25 @@ class Context:
     def stream(self):
         return self.lib.argent_ctx_stream(self.h)
 
+    def set_profiling(self, on):
+        self.check(self.lib.argent_ctx_set_profiling(self.h, 1 if on else 0))
+
+    def kernel_times(self):
+        """{class: (total_ms, launches)} since the last set_profiling."""
+        ms = (ctypes.c_double * 6)()
+        n = (ctypes.c_uint64 * 6)()
+        self.check(self.lib.argent_ctx_kernel_times(self.h, ms, n))
+        return {k: (ms[i], int(n[i])) for i, k in enumerate(N.KERNEL_CLASSES)}
+
+    def set_counting(self, on):
+        self.check(self.lib.argent_ctx_set_counting(self.h, 1 if on else 0))
+
+    def traversal_counts(self):
+        out = (ctypes.c_uint64 * 6)()
+        self.check(self.lib.argent_ctx_traversal_counts(self.h, out))
+        k = ["closest_rays", "closest_nodes", "closest_tris", "any_rays", "any_nodes", "any_tris"]
+        return dict(zip(k, [int(x) for x in out]))
+
 
 class Piece:
     """`Piece::new`: mesh upload + acceleration structure build."""

@@ -317,6 +317,33 @@ int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n
 /* Kernels the library has launched on this context since creation. */
 uint64_t argent_ctx_kernel_launches(const ArgentCtx* ctx);
 
+/* ------------------------------------------------------------------ */
+/* Measurement (no counterpart in argent, whose only timing is wall   */
+/* clock around render_pass, argent/src/jobs.rs:501-504).             */
+/* ------------------------------------------------------------------ */
+
+/* Kernel classes for argent_ctx_kernel_times. */
+enum {
+  ARGENT_KC_RAYGEN = 0,
+  ARGENT_KC_INTERSECT = 1,
+  ARGENT_KC_SHADE = 2,
+  ARGENT_KC_SHADOW = 3,
+  ARGENT_KC_FILM = 4,
+  ARGENT_KC_TRACE = 5,
+  ARGENT_KC_COUNT = 6
+};
+/* While on, every launch is bracketed by CUDA events on the context stream;
+ * turning it on or off resets the totals. */
+int argent_ctx_set_profiling(ArgentCtx* ctx, int on);
+/* Summed device time (ms) and launch count per kernel class since the last
+ * reset; synchronises the stream.  ms and launches hold ARGENT_KC_COUNT. */
+int argent_ctx_kernel_times(ArgentCtx* ctx, double* ms, uint64_t* launches);
+/* Traversal visit counters: on = count, and reset to zero. */
+int argent_ctx_set_counting(ArgentCtx* ctx, int on);
+/* out[6] = closest-hit rays, nodes, triangles; any-hit rays, nodes,
+ * triangles, counted since the last argent_ctx_set_counting. */
+int argent_ctx_traversal_counts(ArgentCtx* ctx, uint64_t* out);
+
 #ifdef __cplusplus
 }
 #endif
