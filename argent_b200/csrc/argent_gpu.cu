@@ -395,6 +395,16 @@ static int ensure_tables(ArgentCtx* ctx) {
   static std::once_flag once;
   std::call_once(once, [] { argent::ggx_energy_table(energy); });
   ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_sobol_dirs, dirs, sizeof(dirs)));
+  static uint32_t bytes[4][4][256];
+  for (int d = 0; d < 4; ++d)
+    for (int k = 0; k < 4; ++k)
+      for (int v = 0; v < 256; ++v) {
+        uint32_t x = 0;
+        for (int j = 0; j < 8; ++j)
+          if ((v >> j) & 1) x ^= dirs[d][8 * k + j];
+        bytes[d][k][v] = x;
+      }
+  ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_sobol_bytes, bytes, sizeof(bytes)));
   ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_energy_table, energy, sizeof(energy)));
   ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_cmf, ARGENT_CMF_1931_2DEG, sizeof(float) * 471 * 3));
   ctx->tables_ready = true;

@@ -13,6 +13,11 @@ struct Bsdf {
   int kind;
   Ggx ggx;
   Spec eta, k;  // conductor eta/k; dielectric eta
+  // Conductor: F(1) per wavelength and E(wo.z), which argent recomputes on
+  // every eval (bsdf.rs:62-64); both depend only on the hit, so they are
+  // evaluated once per hit (same values).
+  Spec f0;
+  float e_wo;
   float eta1;   // coated eta
   Spec base;    // coated base, diffuse albedo, opal body
   V3 n;         // opal lattice normal (local)
@@ -94,9 +99,8 @@ __device__ Spec bsdf_eval(const Bsdf& b, V3 wo, V3 wi) {
       V3 h = normalize(wo + wi);
       Spec f = fresnel_conductor(dot(wo, h), b.eta, b.k);
       float base = ggx_d(b.ggx, h) * ggx_g2(b.ggx, wo, wi) / (4.0f * wo.z * wi.z);
-      float e = ggx_e(b.ggx, wo.z);
-      Spec f0 = fresnel_conductor(1.0f, b.eta, b.k);
-      return f * base * (spec(1.0f) + f0 * ((1.0f - e) / e));
+      float e = b.e_wo;
+      return f * base * (spec(1.0f) + b.f0 * ((1.0f - e) / e));
     }
     case B_COATED:
       return coated_eval(b.ggx, b.eta1, b.base, wo, wi);

@@ -44,14 +44,9 @@ __device__ __forceinline__ uint32_t hash_combine(uint32_t seed, uint32_t v) {
   return seed ^ (v + 0x9e3779b9u + (seed << 6) + (seed >> 2));
 }
 __device__ __forceinline__ uint32_t sobol_dim(uint32_t index, int d) {
-  uint32_t x = 0;
-#pragma unroll 4
-  for (int j = 0; j < 32; ++j) {
-    if (index == 0) break;
-    if (index & 1u) x ^= d_sobol_dirs[d][j];
-    index >>= 1;
-  }
-  return x;
+  const uint32_t* t = &d_sobol_bytes[d][0][0];
+  return __ldg(t + (index & 0xffu)) ^ __ldg(t + 256 + ((index >> 8) & 0xffu)) ^
+         __ldg(t + 512 + ((index >> 16) & 0xffu)) ^ __ldg(t + 768 + (index >> 24));
 }
 __device__ __forceinline__ void sample_4d(uint32_t index, uint32_t set, uint32_t seed, float out[4]) {
   uint32_t sseed = hash_combine(seed, hash32(set));

@@ -8,6 +8,10 @@ namespace dev {
 
 // Sobol direction numbers of the sampler's four dimensions, [dim][bit].
 __device__ uint32_t d_sobol_dirs[4][32];
+// The same generator matrices applied a byte at a time: entry [dim][k][v]
+// is the XOR of the direction numbers of the set bits of v << 8k, so a
+// 32-bit index costs four lookups per dimension.
+__device__ uint32_t d_sobol_bytes[4][4][256];
 // GGX single-scattering albedo E(mu, sqrt(alpha)), 32 x 32 (microfacet.rs:93-140).
 __device__ float d_energy_table[32 * 32];
 // CIE 1931 2-degree colour matching functions, 1 nm, 360..=830 (cie.rs:38-49).

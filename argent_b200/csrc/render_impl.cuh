@@ -485,6 +485,10 @@ __device__ __noinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot, in
     }
     float ub = s.next();
     Bsdf bsdf = material_bsdf(mat, wl, cavity, ub, ctx);
+    if (bsdf.kind == B_CONDUCTOR && !is_smooth(bsdf.ggx)) {
+      bsdf.f0 = fresnel_conductor(1.0f, bsdf.eta, bsdf.k);
+      bsdf.e_wo = ggx_e(bsdf.ggx, wo.z);
+    }
     if (depth == 0) {
       float g[3];
       guide_rgb(mat, cavity, g);

@@ -243,6 +243,8 @@ def run_gpu(args, world, rank, device):
     from argent_b200 import workloads as W
 
     wl = W.signet_still(piece, mesh=m) if args.workload == "signet_still" else W.ring_still()
+    if args.spp:
+        wl.spp = args.spp  # profiling runs only: the bench line uses the workload's spp
     scene = Scene(ctx, piece, wl.desc)
     film = Film(ctx, wl.width, wl.height)
     stream = torch.cuda.ExternalStream(ctx.stream)
@@ -383,6 +385,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--spp", type=int, default=0, help="override spp (short profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         # CPU only: rank 0 measures, the other ranks have nothing to do.
