@@ -141,6 +141,8 @@ GPU_FUNCS = {
     "argent_trace_anyhit_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_uint64, ctypes.c_void_p]),
     "argent_render_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ArgentBatchItem), ctypes.c_uint32]),
+    "argent_trace_closest_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                    ctypes.c_uint64, ctypes.c_void_p]),
     "argent_ctx_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "argent_ctx_kernel_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                                ctypes.POINTER(ctypes.c_uint64)]),

@@ -984,3 +984,64 @@ int argent_ctx_traversal_counts(ArgentCtx* ctx, uint64_t* out6) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ allocation-free closest hit
+//
+// A variant of argent_trace_closest for callers that must not allocate
+// device memory while they run (see argent_gpu.h).  Its staging buffers are
+// this file-scope array instead of cudaMallocAsync: rays first, then hits.
+// Every GPU that loads the library holds the array until the process exits.
+
+#define ARGENT_NOALLOC_MAX_RAYS (1u << 18)
+#define ARGENT_NOALLOC_MAX_DEVICES 64
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[(size_t)ARGENT_NOALLOC_MAX_RAYS *
+                                                                 (sizeof(ArgentRay) + sizeof(ArgentHit))];
+
+// Device address of g_noalloc_scratch per device, looked up once per device
+// with that device current (the name is only a host stand-in in host code).
+static void* g_noalloc_addr[ARGENT_NOALLOC_MAX_DEVICES];
+static std::mutex g_noalloc_mu;
+
+static int noalloc_scratch(ArgentCtx* ctx, unsigned char** out) {
+  if (ctx->device < 0 || ctx->device >= ARGENT_NOALLOC_MAX_DEVICES)
+    return set_error(ctx, ARGENT_E_INVALID, "device index beyond the allocation-free table");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[ctx->device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return set_error(ctx, ARGENT_E_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") +
+                                               cudaGetErrorString(e));
+    g_noalloc_addr[ctx->device] = p;
+  }
+  *out = (unsigned char*)g_noalloc_addr[ctx->device];
+  return ARGENT_OK;
+}
+
+extern "C" int argent_trace_closest_noalloc(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* rays, uint64_t n,
+                                            ArgentHit* hits) {
+  if (!ctx || !piece || (n && (!rays || !hits))) return set_error(ctx, ARGENT_E_INVALID, "NULL argument");
+  if (n > ARGENT_NOALLOC_MAX_RAYS)
+    return set_error(ctx, ARGENT_E_INVALID,
+                     "argent_trace_closest_noalloc: " + std::to_string(n) +
+                         " rays exceed the allocation-free maximum of " + std::to_string(ARGENT_NOALLOC_MAX_RAYS));
+  if (n == 0) return ARGENT_OK;
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  unsigned char* base = nullptr;
+  int rc = noalloc_scratch(ctx, &base);
+  if (rc != ARGENT_OK) return rc;
+  ArgentRay* d_rays = reinterpret_cast<ArgentRay*>(base);
+  ArgentHit* d_hits = reinterpret_cast<ArgentHit*>(base + (size_t)ARGENT_NOALLOC_MAX_RAYS * sizeof(ArgentRay));
+  // Every hit the call returns is written by the kernel, so nothing in the
+  // array has to start at zero; rays are overwritten by this copy.
+  ARGENT_CK(ctx, cudaMemcpyAsync(d_rays, rays, n * sizeof(ArgentRay), cudaMemcpyHostToDevice, ctx->stream));
+  int block = 128;
+  int grid = grid_for(ctx, (const void*)k_trace_closest, block, n);
+  k_trace_closest<<<grid, block, 0, ctx->stream>>>(piece->dev, d_rays, n, d_hits, ctx->d_status);
+  ctx->launches++;
+  ARGENT_CK(ctx, cudaGetLastError());
+  ARGENT_CK(ctx, cudaMemcpyAsync(hits, d_hits, n * sizeof(ArgentHit), cudaMemcpyDeviceToHost, ctx->stream));
+  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return ctx_check_status(ctx);
+}

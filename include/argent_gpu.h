@@ -285,6 +285,26 @@ int argent_trace_closest(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* ra
 /* Any hit; occluded[i] = 1 when some triangle has t in (1e-7, tmax).
  * Replaces `Bvh::occluded` (bvh.rs:216-247).  Host arrays; synchronous. */
 int argent_trace_anyhit(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* rays, uint64_t n, uint8_t* occluded);
+/*
+ * Allocation-free closest hit.  No counterpart in argent.  Same inputs,
+ * outputs and results as argent_trace_closest (host arrays, synchronous),
+ * but it allocates nothing: no cudaMalloc, cudaFree or allocating library
+ * call.  It is for callers that cannot allocate device memory while they run.
+ * One example is a serve loop that admits renders against a fixed
+ * device-memory budget and issues probe rays (autofocus, picking) between
+ * them: an allocation could fail under load or evict a resident scene, and
+ * cudaMalloc/cudaFree can synchronise the device and stall renders in
+ * flight on other streams.
+ * Limit: n <= 262,144 rays (2^18); larger n returns ARGENT_E_INVALID.  The
+ * device staging is one static array of 12 MiB (rays then hits) that every
+ * GPU loading the library holds until exit.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  All calls share
+ * the array and it keeps the last call's contents: calls that overlap on the
+ * GPU (e.g. two contexts on one device used from two threads) race.
+ */
+int argent_trace_closest_noalloc(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* rays, uint64_t n,
+                                 ArgentHit* hits);
 /* Device-pointer variants (asynchronous on the context stream). */
 int argent_trace_closest_device(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* d_rays, uint64_t n,
                                 ArgentHit* d_hits);
