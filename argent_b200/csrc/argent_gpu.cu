@@ -429,7 +429,8 @@ static int ensure_wave(ArgentCtx* ctx) {
   ok = ok && alloc((void**)&w.rng, cap * sizeof(unsigned long long));
   ok = ok && alloc((void**)&w.q0, cap * sizeof(uint32_t));
   ok = ok && alloc((void**)&w.q1, cap * sizeof(uint32_t));
-  ok = ok && alloc((void**)&w.counters, 2 * (ARGENT_MAX_DEPTH + 2) * sizeof(uint32_t));
+  ok = ok && alloc((void**)&w.qc, (size_t)NUM_CLS * cap * sizeof(uint32_t));
+  ok = ok && alloc((void**)&w.counters, CNT_TOTAL * sizeof(uint32_t));
   if (!ok) {
     w.release();
     return set_error(ctx, ARGENT_E_OOM, "wave buffers: out of device memory");
@@ -495,7 +496,8 @@ std::vector<dev::WaveDesc> plan_waves(const std::vector<dev::DevJob>& jobs, cons
 
 }  // namespace
 
-static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const std::vector<uint32_t>& counts) {
+static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const std::vector<uint32_t>& counts,
+                    const std::vector<uint32_t>& scene_classes) {
   int rc = ensure_tables(ctx);
   if (rc != ARGENT_OK) return rc;
   rc = ensure_wave(ctx);
@@ -527,14 +529,18 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   a.rng = wb.rng;
   a.counters = wb.counters;
   a.status = ctx->d_status;
+  a.qc = wb.qc;
+  a.cap = (uint32_t)wb.cap;
   uint32_t cap = (uint32_t)wb.cap;
   int g_ray = grid_for(ctx, (const void*)dev::k_raygen, 256, cap);
   int g_int = grid_for(ctx, (const void*)dev::k_intersect, 128, cap);
-  int g_sh = grid_for(ctx, (const void*)dev::k_shade, 128, cap);
+  int g_sh = grid_for(ctx, (const void*)dev::k_shade<CLS_METAL>, 128, cap);
   int g_any = grid_for(ctx, (const void*)dev::k_shadow, 128, cap);
   int g_film = grid_for(ctx, (const void*)dev::k_film, 256, cap);
   for (size_t wi = 0; wi < waves.size(); ++wi) {
     const dev::WaveDesc& w = waves[wi];
+    uint32_t classes = 1u << CLS_TERMINAL;
+    for (uint32_t sgi = 0; sgi < w.num_segments; ++sgi) classes |= scene_classes[w.seg[sgi].job];
     a.q_in = wb.q0;
     a.q_out = wb.q1;
     {
@@ -551,7 +557,13 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
       }
       {
         ProfScope ps(ctx, KC_SHADE);
-        dev::k_shade<<<g_sh, 128, 0, ctx->stream>>>(a, (int)depth, cap);
+        if (classes & (1u << CLS_TERMINAL)) dev::k_shade<CLS_TERMINAL><<<g_sh, 128, 0, ctx->stream>>>(a, (int)depth);
+        if (classes & (1u << CLS_METAL)) dev::k_shade<CLS_METAL><<<g_sh, 128, 0, ctx->stream>>>(a, (int)depth);
+        if (classes & (1u << CLS_COATED)) dev::k_shade<CLS_COATED><<<g_sh, 128, 0, ctx->stream>>>(a, (int)depth);
+        if (classes & (1u << CLS_DIELECTRIC))
+          dev::k_shade<CLS_DIELECTRIC><<<g_sh, 128, 0, ctx->stream>>>(a, (int)depth);
+        if (classes & (1u << CLS_OTHER)) dev::k_shade<CLS_OTHER><<<g_sh, 128, 0, ctx->stream>>>(a, (int)depth);
+        ctx->launches += __builtin_popcount(classes) - 1;
       }
       {
         ProfScope ps(ctx, KC_SHADOW);
@@ -693,6 +705,15 @@ int argent_scene_upload(ArgentCtx* ctx, ArgentPiece* piece, const ArgentSceneDes
   h.fade_start = desc->floor.fade_start;
   h.fade_end = desc->floor.fade_end;
   set_turn(h, desc->turntable_deg);
+  h.class_mask = 1u << CLS_TERMINAL;
+  for (int i = 0; i < desc->num_materials; ++i) {
+    int c = dev::material_class(desc->materials[i].kind, desc->materials[i].gem_kind);
+    h.mat_class[i] = (uint8_t)c;
+    if (desc->floor.enabled && i == desc->floor.material) h.class_mask |= 1u << c;
+  }
+  for (uint32_t i = 0; i <= piece->max_material && (int)i < desc->num_materials; ++i)
+    h.class_mask |= 1u << h.mat_class[i];
+  h.floor_class = desc->floor.enabled ? h.mat_class[desc->floor.material] : CLS_TERMINAL;
   argent::camera_matrix(desc->has_white != 0, desc->white_xyz, h.cam_m);
   std::memcpy(s->cam_m, h.cam_m, sizeof(s->cam_m));
   if (ok) {
@@ -894,7 +915,8 @@ int argent_render_pass(ArgentCtx* ctx, ArgentScene* scene, const ArgentCamera* c
   int rc = make_job(scene, camera, film, settings, seed, &jobs[0]);
   if (rc != ARGENT_OK) return rc;
   std::vector<uint32_t> counts{count};
-  rc = run_jobs(ctx, jobs, counts);
+  std::vector<uint32_t> classes{scene->host.class_mask};
+  rc = run_jobs(ctx, jobs, counts, classes);
   if (rc != ARGENT_OK) return rc;
   film->samples += count;
   film->has_matrix = true;
@@ -907,6 +929,7 @@ int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n
   ARGENT_CK(ctx, cudaSetDevice(ctx->device));
   std::vector<dev::DevJob> jobs(n);
   std::vector<uint32_t> counts(n);
+  std::vector<uint32_t> classes(n);
   // Items that share a film run one after another: the second starts where
   // the first leaves film.samples.
   std::vector<uint32_t> pending(n, 0);
@@ -924,8 +947,9 @@ int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n
         return set_error(ctx, ARGENT_E_INVALID, "batch items share a film under different white balances");
     jobs[i].first = base;
     counts[i] = it.count;
+    classes[i] = it.scene->host.class_mask;
   }
-  int rc = run_jobs(ctx, jobs, counts);
+  int rc = run_jobs(ctx, jobs, counts, classes);
   if (rc != ARGENT_OK) return rc;
   for (uint32_t i = 0; i < n; ++i) {
     items[i].film->samples += items[i].count;

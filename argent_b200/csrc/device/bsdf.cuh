@@ -91,10 +91,18 @@ __device__ float opal_flake_pdf(V3 n, Ggx ggx, V3 wo, V3 wi) {
   return ggx_d_visible(ggx, a, h) / (4.0f * fmaxf(dot(a, h), 1e-8f));
 }
 
+// Shading kernels are specialised per material class; KM is the set of BSDF
+// kinds (bit per BsdfKind) a class can produce, so the other kinds' code is
+// left out of that kernel.
+#define KM_ALL 0x3Fu
+#define KM_HAS(KM, K) (((KM) >> (K)) & 1u)
+
 // bsdf.rs:53-95
+template <unsigned KM = KM_ALL>
 __device__ Spec bsdf_eval(const Bsdf& b, V3 wo, V3 wi) {
   switch (b.kind) {
     case B_CONDUCTOR: {
+      if constexpr (!KM_HAS(KM, B_CONDUCTOR)) return spec(0.0f);
       if (wo.z <= 0.0f || wi.z <= 0.0f || is_smooth(b.ggx)) return spec(0.0f);
       V3 h = normalize(wo + wi);
       Spec f = fresnel_conductor(dot(wo, h), b.eta, b.k);
@@ -103,11 +111,14 @@ __device__ Spec bsdf_eval(const Bsdf& b, V3 wo, V3 wi) {
       return f * base * (spec(1.0f) + b.f0 * ((1.0f - e) / e));
     }
     case B_COATED:
+      if constexpr (!KM_HAS(KM, B_COATED)) return spec(0.0f);
       return coated_eval(b.ggx, b.eta1, b.base, wo, wi);
     case B_DIFFUSE:
+      if constexpr (!KM_HAS(KM, B_DIFFUSE)) return spec(0.0f);
       if (wo.z <= 0.0f || wi.z <= 0.0f) return spec(0.0f);
       return b.base * ARGENT_FRAC_1_PI_F;
     case B_OPAL: {
+      if constexpr (!KM_HAS(KM, B_OPAL)) return spec(0.0f);
       if (wo.z <= 0.0f || wi.z <= 0.0f) return spec(0.0f);
       Spec bb = coated_eval(ggx_from_roughness(0.12f), 1.45f, b.base, wo, wi);
       Spec flake = opal_flake_eval(b.n, b.ggx, b.spacing_nm, b.strength, b.lambda, wo, wi);
@@ -119,19 +130,24 @@ __device__ Spec bsdf_eval(const Bsdf& b, V3 wo, V3 wi) {
 }
 
 // bsdf.rs:97-131
+template <unsigned KM = KM_ALL>
 __device__ float bsdf_pdf(const Bsdf& b, V3 wo, V3 wi) {
   switch (b.kind) {
     case B_CONDUCTOR: {
+      if constexpr (!KM_HAS(KM, B_CONDUCTOR)) return 0.0f;
       if (wo.z <= 0.0f || wi.z <= 0.0f || is_smooth(b.ggx)) return 0.0f;
       V3 h = normalize(wo + wi);
       return ggx_d_visible(b.ggx, wo, h) / (4.0f * fmaxf(dot(wo, h), 1e-8f));
     }
     case B_COATED:
+      if constexpr (!KM_HAS(KM, B_COATED)) return 0.0f;
       return coated_pdf(b.ggx, b.eta1, b.base, wo, wi);
     case B_DIFFUSE:
+      if constexpr (!KM_HAS(KM, B_DIFFUSE)) return 0.0f;
       if (wo.z <= 0.0f || wi.z <= 0.0f) return 0.0f;
       return wi.z * ARGENT_FRAC_1_PI_F;
     case B_OPAL: {
+      if constexpr (!KM_HAS(KM, B_OPAL)) return 0.0f;
       if (wo.z <= 0.0f || wi.z <= 0.0f) return 0.0f;
       float pb = coated_pdf(ggx_from_roughness(0.12f), 1.45f, b.base, wo, wi);
       return pb * (1.0f - b.w) + opal_flake_pdf(b.n, b.ggx, wo, wi) * b.w;
@@ -164,10 +180,12 @@ __device__ __forceinline__ bool coated_sample(Ggx ggx, float eta, const Spec& ba
 }
 
 // bsdf.rs:133-239
+template <unsigned KM = KM_ALL>
 __device__ bool bsdf_sample(const Bsdf& b, V3 wo, float u0, float u1, float u2, BsdfSample* out) {
   out->delta = out->transmit = out->terminate_secondary = false;
   switch (b.kind) {
     case B_CONDUCTOR: {
+      if constexpr (!KM_HAS(KM, B_CONDUCTOR)) return false;
       if (wo.z <= 0.0f) return false;
       if (is_smooth(b.ggx)) {
         V3 wi{-wo.x, -wo.y, wo.z};
@@ -182,12 +200,14 @@ __device__ bool bsdf_sample(const Bsdf& b, V3 wo, float u0, float u1, float u2, 
       if (wi.z <= 0.0f) return false;
       out->wi = wi;
       out->pdf = ggx_d_visible(b.ggx, wo, h) / (4.0f * fmaxf(dot(wo, h), 1e-8f));
-      out->f = bsdf_eval(b, wo, wi);
+      out->f = bsdf_eval<KM>(b, wo, wi);
       return true;
     }
     case B_COATED:
+      if constexpr (!KM_HAS(KM, B_COATED)) return false;
       return coated_sample(b.ggx, b.eta1, b.base, wo, u0, u1, u2, out);
     case B_DIFFUSE: {
+      if constexpr (!KM_HAS(KM, B_DIFFUSE)) return false;
       if (wo.z <= 0.0f) return false;
       V3 wi = cosine_hemisphere(u1, u2);
       float p = wi.z * ARGENT_FRAC_1_PI_F;
@@ -198,6 +218,7 @@ __device__ bool bsdf_sample(const Bsdf& b, V3 wo, float u0, float u1, float u2, 
       return true;
     }
     case B_DIELECTRIC: {
+      if constexpr (!KM_HAS(KM, B_DIELECTRIC)) return false;
       bool dispersive = (max_value(b.eta) - min_value(b.eta)) > 1e-5f;
       float e0 = b.eta.v[0];
       float cos_o = wo.z;
@@ -230,6 +251,7 @@ __device__ bool bsdf_sample(const Bsdf& b, V3 wo, float u0, float u1, float u2, 
       return true;
     }
     case B_OPAL: {
+      if constexpr (!KM_HAS(KM, B_OPAL)) return false;
       if (wo.z <= 0.0f) return false;
       V3 wi;
       if (u0 < b.w) {
@@ -246,10 +268,10 @@ __device__ bool bsdf_sample(const Bsdf& b, V3 wo, float u0, float u1, float u2, 
         wi = s.wi;
       }
       if (wi.z <= 0.0f) return false;
-      float p = bsdf_pdf(b, wo, wi);
+      float p = bsdf_pdf<KM>(b, wo, wi);
       if (p <= 0.0f) return false;
       out->wi = wi;
-      out->f = bsdf_eval(b, wo, wi);
+      out->f = bsdf_eval<KM>(b, wo, wi);
       out->pdf = p;
       return true;
     }
@@ -309,7 +331,39 @@ struct HitCtx {
   float turn_s, turn_c;  // sin/cos of +turntable angle (object -> world)
 };
 
+// Material classes: the shading kernel a hit goes to.
+#define CLS_TERMINAL 0    // miss or panel: emission only, no surface
+#define CLS_METAL 1       // Metal (conductor; the patina layer is coated)
+#define CLS_COATED 2      // Plastic, opaque gem
+#define CLS_DIELECTRIC 3  // transparent gem (and a gem of opal kind)
+#define CLS_OTHER 4       // Opal, Diffuse, Black
+#define NUM_CLS 5
+
+__host__ __device__ inline int material_class(int kind, int gem_kind) {
+  switch (kind) {
+    case ARGENT_MAT_METAL:
+      return CLS_METAL;
+    case ARGENT_MAT_PLASTIC:
+      return CLS_COATED;
+    case ARGENT_MAT_GEM:
+      return gem_kind == ARGENT_GEM_OPAQUE ? CLS_COATED : CLS_DIELECTRIC;
+    default:
+      return CLS_OTHER;
+  }
+}
+
+// BSDF kinds each class can produce.
+template <int CLS>
+struct ClassKinds {
+  static constexpr unsigned value = CLS == CLS_METAL        ? ((1u << B_CONDUCTOR) | (1u << B_COATED))
+                                    : CLS == CLS_COATED     ? (1u << B_COATED)
+                                    : CLS == CLS_DIELECTRIC ? (1u << B_DIELECTRIC)
+                                    : CLS == CLS_OTHER      ? ((1u << B_OPAL) | (1u << B_DIFFUSE) | (1u << B_BLACK))
+                                                            : 0u;
+};
+
 // material.rs:96-138
+template <int CLS = -1>
 __device__ Bsdf material_bsdf(const ArgentMaterial* m, const Wavelengths& wl, float mask, float u, const HitCtx& ctx) {
   Bsdf b;
   b.kind = B_BLACK;
@@ -318,8 +372,10 @@ __device__ Bsdf material_bsdf(const ArgentMaterial* m, const Wavelengths& wl, fl
   b.w = 0.0f;
   b.spacing_nm = b.strength = 0.0f;
   b.n = V3{0, 0, 1};
+  constexpr bool any = CLS < 0;
   switch (m->kind) {
     case ARGENT_MAT_OPAL: {
+      if constexpr (!(any || CLS == CLS_OTHER)) return b;
       V3 dir;
       float spacing, brightness;
       opal_domain(ctx.p_obj / m->cell_mm, &dir, &spacing, &brightness);
@@ -338,6 +394,7 @@ __device__ Bsdf material_bsdf(const ArgentMaterial* m, const Wavelengths& wl, fl
       return b;
     }
     case ARGENT_MAT_METAL: {
+      if constexpr (!(any || CLS == CLS_METAL)) return b;
       if (m->has_patina) {
         float t = rclamp((mask - m->patina_lo) / fmaxf(m->patina_hi - m->patina_lo, 1e-4f), 0.0f, 1.0f);
         float w = m->patina_strength * t * t * (3.0f - 2.0f * t);
@@ -359,6 +416,7 @@ __device__ Bsdf material_bsdf(const ArgentMaterial* m, const Wavelengths& wl, fl
       return b;
     }
     case ARGENT_MAT_GEM: {
+      if constexpr (!(any || CLS == CLS_COATED || CLS == CLS_DIELECTRIC)) return b;
       if (m->gem_kind == ARGENT_GEM_OPAQUE) {
         b.kind = B_COATED;
         b.ggx = ggx_from_roughness(0.06f);
@@ -371,12 +429,14 @@ __device__ Bsdf material_bsdf(const ArgentMaterial* m, const Wavelengths& wl, fl
       return b;
     }
     case ARGENT_MAT_PLASTIC:
+      if constexpr (!(any || CLS == CLS_COATED)) return b;
       b.kind = B_COATED;
       b.ggx = Ggx{m->alpha};
       b.eta1 = m->eta;
       b.base = tab_sample(m->spec_a, wl);
       return b;
     case ARGENT_MAT_DIFFUSE:
+      if constexpr (!(any || CLS == CLS_OTHER)) return b;
       b.kind = B_DIFFUSE;
       b.base = tab_sample(m->spec_a, wl);
       return b;

@@ -146,8 +146,35 @@ __device__ __forceinline__ void count_visits(int base, uint32_t nodes, uint32_t 
   }
 }
 
+// Sorts 8 keys ascending (Batcher odd-even merge network, 19 comparators).
+#define ARGENT_CX(a, b)                      \
+  {                                          \
+    uint32_t lo_ = min(k[a], k[b]);          \
+    uint32_t hi_ = max(k[a], k[b]);          \
+    k[a] = lo_;                              \
+    k[b] = hi_;                              \
+  }
+__device__ __forceinline__ void sort8(uint32_t k[8]) {
+  ARGENT_CX(0, 1) ARGENT_CX(2, 3) ARGENT_CX(4, 5) ARGENT_CX(6, 7)
+  ARGENT_CX(0, 2) ARGENT_CX(1, 3) ARGENT_CX(4, 6) ARGENT_CX(5, 7)
+  ARGENT_CX(1, 2) ARGENT_CX(5, 6)
+  ARGENT_CX(0, 4) ARGENT_CX(1, 5) ARGENT_CX(2, 6) ARGENT_CX(3, 7)
+  ARGENT_CX(2, 4) ARGENT_CX(3, 5)
+  ARGENT_CX(1, 2) ARGENT_CX(3, 4) ARGENT_CX(5, 6)
+}
+#undef ARGENT_CX
+
 // Closest hit with t in (1e-7, t_max).  Ties at equal t go to the lower
 // original triangle index.
+//
+// Order of visits: the children a node's slab test keeps are sorted by
+// entry distance and the nearest is entered at once; the others are pushed
+// far-to-near.  The sort key is the entry distance with its 3 low mantissa
+// bits replaced by the child slot; the truncated distance is what the stack
+// keeps for pruning, which can only keep more nodes than the exact value.
+// The visit order changes how much is pruned, never the result: a triangle
+// whose hit is the final best has box entry <= that distance <= the running
+// best at every point, so its box is always entered.
 __device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, float t_max, uint32_t* status) {
   TraceHit best{t_max, 0.0f, 0.0f, ARGENT_NO_HIT_U};
   if (pc.num_tris == 0) return best;
@@ -155,12 +182,16 @@ __device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, f
   uint2 stack[ARGENT_STACK_SIZE];
   int sp = 0;
   uint32_t n_nodes = 0, n_tris = 0;
-  stack[sp++] = make_uint2(0u, __float_as_uint(0.0f));
-  while (sp > 0) {
-    --sp;
-    uint32_t ref = stack[sp].x;
-    float tn = __uint_as_float(stack[sp].y);
-    if (tn > best.t) continue;
+  uint32_t ref = 0u;
+  bool have = true;
+  for (;;) {
+    if (!have) {
+      if (sp == 0) break;
+      --sp;
+      ref = stack[sp].x;
+      if (__uint_as_float(stack[sp].y) > best.t) continue;
+    }
+    have = false;
     if (ref & ARGENT_LEAF_BIT) {
       uint32_t start = ref & 0x07FFFFFFu;
       uint32_t cnt = ((ref >> 27) & 15u) + 1u;
@@ -183,33 +214,29 @@ __device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, f
     }
     NodeView n = load_node(pc.nodes, ref);
     ++n_nodes;
-    float tc[8];
-    uint32_t hitmask = 0;
+    uint32_t k[8];
+    int nh = 0;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-      tc[c] = 0.0f;
-      if ((n.present >> c) & 1u) {
-        if (slab_child(n, c, o, inv, best.t, &tc[c])) hitmask |= 1u << c;
+      k[c] = 0xFFFFFFFFu;
+      float tc;
+      if (((n.present >> c) & 1u) && slab_child(n, c, o, inv, best.t, &tc)) {
+        k[c] = (__float_as_uint(tc) & ~7u) | (uint32_t)c;
+        ++nh;
       }
     }
-    int nh = __popc(hitmask);
-    if (sp + nh > ARGENT_STACK_SIZE) {
+    if (nh == 0) continue;
+    if (sp + nh - 1 > ARGENT_STACK_SIZE) {
       atomicOr(status, ARGENT_STATUS_STACK_OVERFLOW);
       break;
     }
+    sort8(k);
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      if ((hitmask >> c) & 1u) {
-        int rank = 0;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          bool before = ((hitmask >> j) & 1u) && (tc[j] < tc[c] || (tc[j] == tc[c] && j < c));
-          rank += before ? 1 : 0;
-        }
-        stack[sp + nh - 1 - rank] = make_uint2(child_ref(n, c), __float_as_uint(tc[c]));
-      }
+    for (int j = 7; j >= 1; --j) {
+      if (j < nh) stack[sp++] = make_uint2(child_ref(n, (int)(k[j] & 7u)), k[j] & ~7u);
     }
-    sp += nh;
+    ref = child_ref(n, (int)(k[0] & 7u));
+    have = true;
   }
   count_visits(0, n_nodes, n_tris);
   return best;

@@ -60,6 +60,10 @@ struct DevScene {
   float to_obj_s, to_obj_c;      // rot_y(-turn)
   float to_world_s, to_world_c;  // rot_y(+turn)
   float cam_m[9];
+  // Shading class of each material slot and of the floor's material.
+  uint8_t mat_class[256];
+  int32_t floor_class;
+  uint32_t class_mask;  // classes a path of this scene can reach
 };
 
 // One render_pass worth of work.
@@ -101,8 +105,8 @@ struct WaveBuffers {
   float4 *sh_o = nullptr, *sh_d = nullptr, *sh_c = nullptr;
   uint4* meta = nullptr;
   unsigned long long* rng = nullptr;
-  uint32_t *q0 = nullptr, *q1 = nullptr, *qs = nullptr;
-  uint32_t* counters = nullptr;  // [2 * (ARGENT_MAX_DEPTH + 2)]
+  uint32_t *q0 = nullptr, *q1 = nullptr, *qc = nullptr;
+  uint32_t* counters = nullptr;
   std::vector<void*> allocs;
   uint64_t bytes = 0;
   void release() {

@@ -36,7 +36,11 @@ __device__ __forceinline__ bool panel_intersect(const DevPanel& p, V3 o, V3 d, f
   V3 n = ld3(p.n);
   float denom = dot(d, n);
   if (fabsf(denom) < 1e-9f) return false;
-  float t = dot(ld3(p.c) - o, n) / denom;
+  float num = dot(ld3(p.c) - o, n);
+  // A zero numerator or one of the other sign gives t <= 0, which argent's
+  // t <= 1e-6 test rejects; skipping the division there changes nothing.
+  if (num == 0.0f || (signbit(num) != signbit(denom))) return false;
+  float t = num / denom;
   if (t <= 1e-6f || t >= t_max) return false;
   V3 q = (o + d * t) - ld3(p.c);
   float a = dot(q, ld3(p.hu)) / p.hu_l2;
@@ -215,10 +219,19 @@ struct WaveArgs {
   float4 *o, *d, *beta, *L, *lambda, *pdf, *hit, *albedo, *normal, *sh_o, *sh_d, *sh_c;
   uint4* meta;
   unsigned long long* rng;
-  uint32_t *q_in, *q_out, *qs;
+  uint32_t *q_in, *q_out;  // active paths entering / leaving a bounce
+  uint32_t* qc;            // NUM_CLS shade queues of `cap` entries
+  uint32_t cap;
   uint32_t* counters;
   uint32_t* status;
 };
+
+// Queue counters of one wave: active paths per bounce, shade-queue lengths
+// per bounce and class, shadow rays per bounce.
+#define CNT_ACT(d) (d)
+#define CNT_CLS(d, c) ((ARGENT_MAX_DEPTH + 2) + (d) * NUM_CLS + (c))
+#define CNT_SH(d) ((ARGENT_MAX_DEPTH + 2) * (1 + NUM_CLS) + (d))
+#define CNT_TOTAL ((ARGENT_MAX_DEPTH + 2) * (2 + NUM_CLS))
 
 __device__ __forceinline__ const DevSegment& find_segment(const WaveDesc& w, uint32_t slot) {
   uint32_t s = 0;
@@ -250,8 +263,7 @@ __device__ __forceinline__ void camera_ray(const ArgentCamera& c, float sx, floa
 // render.rs:82-93: one camera sample per slot.
 __global__ void __launch_bounds__(256) k_raygen(WaveArgs a, WaveDesc w) {
   if (blockIdx.x == 0) {
-    for (int i = threadIdx.x; i < 2 * (ARGENT_MAX_DEPTH + 2); i += blockDim.x)
-      a.counters[i] = (i == 0) ? w.num_slots : 0u;
+    for (int i = threadIdx.x; i < CNT_TOTAL; i += blockDim.x) a.counters[i] = (i == CNT_ACT(0)) ? w.num_slots : 0u;
   }
   for (uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < w.num_slots; slot += gridDim.x * blockDim.x) {
     const DevSegment& sg = find_segment(w, slot);
@@ -289,44 +301,6 @@ __global__ void __launch_bounds__(256) k_raygen(WaveArgs a, WaveDesc w) {
   }
 }
 
-// scene.rs:169-218
-__global__ void __launch_bounds__(128) k_intersect(WaveArgs a, int depth) {
-  uint32_t count = a.counters[depth];
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    uint32_t slot = a.q_in[i];
-    uint32_t job_id = a.meta[slot].w >> 16;
-    const DevScene* sc = a.jobs[job_id].scene;
-    float4 of = a.o[slot], df = a.d[slot];
-    V3 o{of.x, of.y, of.z}, d{df.x, df.y, df.z};
-    float t_max = INFINITY;
-    float4 rec = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(HIT_MISS));
-    V3 oo = o, od = d;
-    if (sc->has_turn) {
-      oo = rot_y_sc(o, sc->to_obj_s, sc->to_obj_c);
-      od = rot_y_sc(d, sc->to_obj_s, sc->to_obj_c);
-    }
-    TraceHit h = trace_closest(sc->piece, oo, od, INFINITY, a.status);
-    if (h.prim != ARGENT_NO_HIT_U) {
-      t_max = h.t;
-      rec = make_float4(h.t, h.u, h.v, __uint_as_float(h.prim));
-    }
-    for (int p = 0; p < sc->num_panels; ++p) {
-      const DevPanel& pn = sc->panels[p];
-      if (depth == 0 && !pn.camera_visible) continue;
-      float t;
-      if (panel_intersect(pn, o, d, t_max, &t)) {
-        t_max = t;
-        rec = make_float4(t, 0.0f, 0.0f, __uint_as_float(HIT_PANEL | (uint32_t)p));
-      }
-    }
-    if (sc->floor_enabled) {
-      float t;
-      if (floor_intersect(sc, o, d, t_max, &t)) rec = make_float4(t, 0.0f, 0.0f, __uint_as_float(HIT_FLOOR));
-    }
-    a.hit[slot] = rec;
-  }
-}
-
 // Warp-aggregated queue append: one atomic per warp, ballot prefix for the
 // lane offsets.  Every lane of the warp must call it.
 __device__ __forceinline__ void warp_append(bool pred, uint32_t value, uint32_t* counter, uint32_t* queue,
@@ -347,14 +321,71 @@ __device__ __forceinline__ void warp_append(bool pred, uint32_t value, uint32_t*
   }
 }
 
+// scene.rs:169-218: closest hit of every active path, then the path is
+// queued for the shading kernel of its hit's material class.
+__global__ void __launch_bounds__(128) k_intersect(WaveArgs a, int depth) {
+  uint32_t count = a.counters[CNT_ACT(depth)];
+  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
+    uint32_t i = base + threadIdx.x;
+    int cls = -1;
+    uint32_t slot = 0;
+    if (i < count) {
+      slot = a.q_in[i];
+      uint32_t job_id = a.meta[slot].w >> 16;
+      const DevScene* sc = a.jobs[job_id].scene;
+      float4 of = a.o[slot], df = a.d[slot];
+      V3 o{of.x, of.y, of.z}, d{df.x, df.y, df.z};
+      float t_max = INFINITY;
+      float4 rec = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(HIT_MISS));
+      V3 oo = o, od = d;
+      if (sc->has_turn) {
+        oo = rot_y_sc(o, sc->to_obj_s, sc->to_obj_c);
+        od = rot_y_sc(d, sc->to_obj_s, sc->to_obj_c);
+      }
+      TraceHit h = trace_closest(sc->piece, oo, od, INFINITY, a.status);
+      cls = CLS_TERMINAL;
+      if (h.prim != ARGENT_NO_HIT_U) {
+        t_max = h.t;
+        rec = make_float4(h.t, h.u, h.v, __uint_as_float(h.prim));
+        cls = sc->mat_class[__ldg(&sc->piece.tri_idx[h.prim].w)];
+      }
+      for (int p = 0; p < sc->num_panels; ++p) {
+        const DevPanel& pn = sc->panels[p];
+        if (depth == 0 && !pn.camera_visible) continue;
+        float t;
+        if (panel_intersect(pn, o, d, t_max, &t)) {
+          t_max = t;
+          rec = make_float4(t, 0.0f, 0.0f, __uint_as_float(HIT_PANEL | (uint32_t)p));
+          cls = CLS_TERMINAL;
+        }
+      }
+      if (sc->floor_enabled) {
+        float t;
+        if (floor_intersect(sc, o, d, t_max, &t)) {
+          rec = make_float4(t, 0.0f, 0.0f, __uint_as_float(HIT_FLOOR));
+          cls = sc->floor_class;
+        }
+      }
+      a.hit[slot] = rec;
+    }
+#pragma unroll
+    for (int c = 0; c < NUM_CLS; ++c)
+      warp_append(cls == c, slot, a.counters + CNT_CLS(depth, c), a.qc + (size_t)c * a.cap, a.cap, a.status);
+  }
+}
+
 struct ShadeOut {
   bool alive;
   bool shadow;
   float4 sh_o, sh_d, sh_c;
 };
 
-// integrator.rs:59-218, one bounce of one path.
-__device__ __noinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot, int depth) {
+// integrator.rs:59-218, one bounce of one path whose hit belongs to class
+// CLS: CLS_TERMINAL takes misses and panel hits, the other classes take
+// surface hits (piece or floor) of their materials.
+template <int CLS>
+__device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot, int depth) {
+  constexpr unsigned KM = ClassKinds<CLS>::value;
   ShadeOut out;
   out.alive = false;
   out.shadow = false;
@@ -392,7 +423,7 @@ __device__ __noinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot, in
   uint32_t mat_id = 0;
   float cavity = 0.0f;
   bool done = false;
-  if (kind == HIT_MISS) {
+  if (CLS == CLS_TERMINAL && kind == HIT_MISS) {
     float w = 1.0f;
     if (env_map && !specular) {
       float pl = sc->env_pick * envmap_pdf(sc, rd);
@@ -400,7 +431,7 @@ __device__ __noinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot, in
     }
     add_clamped(&L, beta * env_eval(sc, rd, wl) * w, clamp, cl);
     done = true;
-  } else if ((kind & 0xF0000000u) == HIT_PANEL && kind != HIT_FLOOR) {
+  } else if (CLS == CLS_TERMINAL) {  // panel (light.rs:67-72, integrator.rs:84-98)
     int idx = (int)(kind & 0x0FFFFFFFu);
     const DevPanel& pn = sc->panels[idx];
     Spec le = panel_le(pn, ro + rd * t, rd, wl);
@@ -466,6 +497,7 @@ __device__ __noinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot, in
     }
   }
 
+  if constexpr (CLS != CLS_TERMINAL) {
   if (!done) {
     const ArgentMaterial* mat = sc->mats + mat_id;
     V3 wo_w = -rd;
@@ -484,7 +516,7 @@ __device__ __noinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot, in
       ctx.turn_c = 1.0f;
     }
     float ub = s.next();
-    Bsdf bsdf = material_bsdf(mat, wl, cavity, ub, ctx);
+    Bsdf bsdf = material_bsdf<CLS>(mat, wl, cavity, ub, ctx);
     if (bsdf.kind == B_CONDUCTOR && !is_smooth(bsdf.ggx)) {
       bsdf.f0 = fresnel_conductor(1.0f, bsdf.eta, bsdf.k);
       bsdf.e_wo = ggx_e(bsdf.ggx, wo.z);
@@ -506,10 +538,10 @@ __device__ __noinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot, in
         V3 dir = envmap_sample(sc, u1, u2, &pdf_dir);
         if (pdf_dir > 0.0f && dot(dir, ngu) > 0.0f) {
           V3 wi = to_local(frame, dir);
-          Spec f = bsdf_eval(bsdf, wo, wi);
+          Spec f = bsdf_eval<KM>(bsdf, wo, wi);
           if (!is_black(f)) {
             float p_light = sc->env_pick * pdf_dir;
-            float p_bsdf = bsdf_pdf(bsdf, wo, wi);
+            float p_bsdf = bsdf_pdf<KM>(bsdf, wo, wi);
             float w = p_light * p_light / (p_light * p_light + p_bsdf * p_bsdf);
             // sky_visibility (scene.rs:123-140): panels and floor here, the
             // piece in k_shadow.
@@ -565,10 +597,10 @@ __device__ __noinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot, in
         float cos_l = dot(-dir, ld3(pn.n));
         if (cos_l > 0.0f && dot(dir, ngu) > 0.0f) {
           V3 wi = to_local(frame, dir);
-          Spec f = bsdf_eval(bsdf, wo, wi);
+          Spec f = bsdf_eval<KM>(bsdf, wo, wi);
           if (!is_black(f)) {
             float p_light = pick * d2 / (cos_l * pn.area);
-            float p_bsdf = bsdf_pdf(bsdf, wo, wi);
+            float p_bsdf = bsdf_pdf<KM>(bsdf, wo, wi);
             float w = p_light * p_light / (p_light * p_light + p_bsdf * p_bsdf);
             V3 origin = offset_origin(p, ngu, dir);
             // visible (scene.rs:222-243): panels and floor here.
@@ -613,7 +645,7 @@ __device__ __noinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot, in
     float u1 = s.next();
     float u2 = s.next();
     BsdfSample smp;
-    bool cont = bsdf_sample(bsdf, wo, u0, u1, u2, &smp);
+    bool cont = bsdf_sample<KM>(bsdf, wo, u0, u1, u2, &smp);
     if (cont && (smp.pdf <= 0.0f || is_black(smp.f))) cont = false;
     V3 wi_w;
     if (cont) {
@@ -653,14 +685,20 @@ __device__ __noinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot, in
       a.rng[slot] = s.rng;
     }
   }
+  }
   a.L[slot] = to_f4(L);
   return out;
 }
 
-__global__ void __launch_bounds__(128) k_shade(WaveArgs a, int depth, uint32_t cap) {
-  uint32_t count = a.counters[depth];
-  uint32_t* next_counter = a.counters + depth + 1;
-  uint32_t* shadow_counter = a.counters + (ARGENT_MAX_DEPTH + 2) + depth;
+// Surface shading is capped at 128 registers (4 blocks of 128 per SM)
+// instead of up to ~166, trading a little spilling for residency.
+template <int CLS>
+__global__ void __launch_bounds__(128, CLS == CLS_TERMINAL ? 1 : 4) k_shade(WaveArgs a, int depth) {
+  uint32_t count = a.counters[CNT_CLS(depth, CLS)];
+  const uint32_t* q = a.qc + (size_t)CLS * a.cap;
+  uint32_t cap = a.cap;
+  uint32_t* next_counter = a.counters + CNT_ACT(depth + 1);
+  uint32_t* shadow_counter = a.counters + CNT_SH(depth);
   for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
     uint32_t i = base + threadIdx.x;
     ShadeOut r;
@@ -668,8 +706,8 @@ __global__ void __launch_bounds__(128) k_shade(WaveArgs a, int depth, uint32_t c
     r.shadow = false;
     uint32_t slot = 0;
     if (i < count) {
-      slot = a.q_in[i];
-      r = shade_path(a, slot, depth);
+      slot = q[i];
+      r = shade_path<CLS>(a, slot, depth);
     }
     warp_append(r.alive, slot, next_counter, a.q_out, cap, a.status);
     // Shadow rays: the record is written at the queue position.
@@ -695,7 +733,7 @@ __global__ void __launch_bounds__(128) k_shade(WaveArgs a, int depth, uint32_t c
 }
 
 __global__ void __launch_bounds__(128) k_shadow(WaveArgs a, int depth) {
-  uint32_t count = a.counters[(ARGENT_MAX_DEPTH + 2) + depth];
+  uint32_t count = a.counters[CNT_SH(depth)];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     float4 so = a.sh_o[i], sd = a.sh_d[i];
     uint32_t slot = __float_as_uint(sd.w);
