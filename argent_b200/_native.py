@@ -184,6 +184,8 @@ HOST_FUNCS = {
     "argent_mesh_free": (None, [ctypes.POINTER(ArgentMesh)]),
     "argent_synth_ring": (ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32,
                                          ctypes.c_float, ctypes.c_float, ctypes.c_uint32, ctypes.POINTER(ArgentMesh)]),
+    "argent_synth_gem_ring": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, ctypes.c_float,
+                                             ctypes.c_uint32, ctypes.POINTER(ArgentMesh)]),
     "argent_synth_signet": (ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32,
                                            ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_uint32,
                                            ctypes.c_uint32, ctypes.POINTER(ArgentMesh)]),

@@ -2,6 +2,8 @@
 // The ring follows argent-mesh's `torus_profile` vertex and triangle order
 // (argent-mesh/src/synth.rs:153-173); the noise lattices use argent's hash32
 // (argent-core/src/sampler.rs:18-25).
+#include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -201,6 +203,234 @@ int argent_synth_signet(float R, float r, uint32_t nu, uint32_t nv, float bezel_
     const float* c = &p[3 * (size_t)t[3 * f + 2]];
     float cx = (a[0] + b[0] + c[0]) / 3.0f, cy = (a[1] + b[1] + c[1]) / 3.0f, cz = (a[2] + b[2] + c[2]) / 3.0f;
     m[f] = value_noise3(cx / 2.0f, cy / 2.0f, cz / 2.0f, mask_seed) > 0.5f ? 1 : 0;
+  }
+  return fill(out, p, t, m);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ gems workload
+namespace {
+
+struct Plane {
+  float n[3], d;  // n . x <= d
+};
+
+// Round brilliant of girdle radius 1 centred on the origin, table up (+y),
+// as the intersection of its facet half-spaces: table, 8 stars, 8 bezels,
+// 16 upper girdle halves, a 32-facet girdle band, 16 lower girdle halves and
+// 8 pavilion mains (57 cut facets + girdle).  Proportions: table 57 %, crown
+// 34.5 deg, pavilion 40.75 deg, girdle 3 %.
+std::vector<Plane> brilliant_planes() {
+  std::vector<Plane> ps;
+  const float PI_F = 3.14159265358979f;
+  auto deg = [&](float a) { return a * PI_F / 180.0f; };
+  const float girdle_half = 0.015f;
+  const float crown_a = deg(34.5f), pav_a = deg(40.75f);
+  const float table_r = 0.57f;
+  const float crown_h = girdle_half + (1.0f - table_r) * std::tan(crown_a);
+  const float culet_y = -girdle_half - std::tan(pav_a) * 1.0f;
+  // A facet inclined `tilt` from the horizontal has its outward normal
+  // tilted `tilt` from the vertical, toward azimuth az.
+  auto add = [&](float az, float tilt, float px, float py, float pz) {
+    float n[3] = {std::cos(az) * std::sin(tilt), std::cos(tilt), std::sin(az) * std::sin(tilt)};
+    ps.push_back(Plane{{n[0], n[1], n[2]}, n[0] * px + n[1] * py + n[2] * pz});
+  };
+  auto addn = [&](float az, float tilt, float px, float py, float pz) {  // pavilion side (normal points down)
+    float n[3] = {std::cos(az) * std::sin(tilt), -std::cos(tilt), std::sin(az) * std::sin(tilt)};
+    ps.push_back(Plane{{n[0], n[1], n[2]}, n[0] * px + n[1] * py + n[2] * pz});
+  };
+  ps.push_back(Plane{{0, 1, 0}, crown_h});  // table
+  for (int k = 0; k < 8; ++k) {
+    float az = deg(45.0f * k);
+    // bezel: through the girdle top at az, crown angle
+    add(az, crown_a, std::cos(az), girdle_half, std::sin(az));
+    // star: shallower, through the table edge between two bezels
+    float az2 = az + deg(22.5f);
+    add(az2, deg(21.7f), table_r * std::cos(az2), crown_h, table_r * std::sin(az2));
+    // pavilion main: through the culet
+    addn(az, pav_a, 0.0f, culet_y, 0.0f);
+  }
+  for (int k = 0; k < 16; ++k) {
+    float az = deg(22.5f * k + 11.25f);
+    add(az, deg(42.0f), std::cos(az), girdle_half, std::sin(az));    // upper girdle half
+    addn(az, deg(42.0f), std::cos(az), -girdle_half, std::sin(az));  // lower girdle half
+  }
+  for (int k = 0; k < 32; ++k) {  // girdle band
+    float az = deg(11.25f * k);
+    ps.push_back(Plane{{std::cos(az), 0.0f, std::sin(az)}, 1.0f});
+  }
+  return ps;
+}
+
+// Convex polytope -> triangles (fan per facet).
+void polytope(const std::vector<Plane>& ps, std::vector<float>& pos, std::vector<uint32_t>& tri) {
+  const size_t n = ps.size();
+  std::vector<std::vector<std::array<float, 3>>> face(n);
+  for (size_t a = 0; a < n; ++a)
+    for (size_t b = a + 1; b < n; ++b)
+      for (size_t c = b + 1; c < n; ++c) {
+        const float* A = ps[a].n;
+        const float* B = ps[b].n;
+        const float* C = ps[c].n;
+        double det = A[0] * ((double)B[1] * C[2] - (double)B[2] * C[1]) - A[1] * ((double)B[0] * C[2] - (double)B[2] * C[0]) +
+                     A[2] * ((double)B[0] * C[1] - (double)B[1] * C[0]);
+        if (std::fabs(det) < 1e-9) continue;
+        double da = ps[a].d, db = ps[b].d, dc = ps[c].d;
+        double x = (da * ((double)B[1] * C[2] - (double)B[2] * C[1]) - A[1] * (db * C[2] - (double)B[2] * dc) +
+                    A[2] * (db * C[1] - (double)B[1] * dc)) / det;
+        double y = (A[0] * (db * C[2] - (double)B[2] * dc) - da * ((double)B[0] * C[2] - (double)B[2] * C[0]) +
+                    A[2] * ((double)B[0] * dc - db * C[0])) / det;
+        double z = (A[0] * ((double)B[1] * dc - db * C[1]) - A[1] * ((double)B[0] * dc - db * C[0]) +
+                    da * ((double)B[0] * C[1] - (double)B[1] * C[0])) / det;
+        bool inside = true;
+        for (size_t q = 0; q < n && inside; ++q)
+          if (ps[q].n[0] * x + ps[q].n[1] * y + ps[q].n[2] * z > ps[q].d + 1e-5) inside = false;
+        if (!inside) continue;
+        std::array<float, 3> v = {(float)x, (float)y, (float)z};
+        for (size_t f : {a, b, c}) {
+          bool dup = false;
+          for (auto& w : face[f])
+            if (std::fabs(w[0] - v[0]) + std::fabs(w[1] - v[1]) + std::fabs(w[2] - v[2]) < 1e-5f) dup = true;
+          if (!dup) face[f].push_back(v);
+        }
+      }
+  for (size_t f = 0; f < n; ++f) {
+    auto& vs = face[f];
+    if (vs.size() < 3) continue;
+    float c[3] = {0, 0, 0};
+    for (auto& v : vs)
+      for (int k = 0; k < 3; ++k) c[k] += v[k] / (float)vs.size();
+    // in-plane basis
+    const float* nn = ps[f].n;
+    float t[3] = {1, 0, 0};
+    if (std::fabs(nn[0]) > 0.9f) t[0] = 0, t[1] = 1;
+    float u[3] = {t[1] * nn[2] - t[2] * nn[1], t[2] * nn[0] - t[0] * nn[2], t[0] * nn[1] - t[1] * nn[0]};
+    float w[3] = {nn[1] * u[2] - nn[2] * u[1], nn[2] * u[0] - nn[0] * u[2], nn[0] * u[1] - nn[1] * u[0]};
+    std::sort(vs.begin(), vs.end(), [&](const std::array<float, 3>& p, const std::array<float, 3>& q) {
+      float px = (p[0] - c[0]) * u[0] + (p[1] - c[1]) * u[1] + (p[2] - c[2]) * u[2];
+      float py = (p[0] - c[0]) * w[0] + (p[1] - c[1]) * w[1] + (p[2] - c[2]) * w[2];
+      float qx = (q[0] - c[0]) * u[0] + (q[1] - c[1]) * u[1] + (q[2] - c[2]) * u[2];
+      float qy = (q[0] - c[0]) * w[0] + (q[1] - c[1]) * w[1] + (q[2] - c[2]) * w[2];
+      return std::atan2(py, px) < std::atan2(qy, qx);
+    });
+    uint32_t base = (uint32_t)(pos.size() / 3);
+    for (auto& v : vs)
+      for (int k = 0; k < 3; ++k) pos.push_back(v[k]);
+    // orient the fan so its winding gives the outward normal
+    for (size_t i = 1; i + 1 < vs.size(); ++i) {
+      float e1[3], e2[3];
+      for (int k = 0; k < 3; ++k) {
+        e1[k] = vs[i][k] - vs[0][k];
+        e2[k] = vs[i + 1][k] - vs[0][k];
+      }
+      float cn[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+      bool out = cn[0] * nn[0] + cn[1] * nn[1] + cn[2] * nn[2] > 0.0f;
+      tri.push_back(base);
+      tri.push_back(base + (uint32_t)(out ? i : i + 1));
+      tri.push_back(base + (uint32_t)(out ? i + 1 : i));
+    }
+  }
+}
+
+void append_torus(std::vector<float>& p, std::vector<uint32_t>& t, std::vector<uint16_t>& m, float R, float r,
+                  uint32_t nu, uint32_t nv, const float c[3], const float ax[3], const float ay[3], const float az[3],
+                  uint16_t mat) {
+  // torus around local z, placed with basis (ax, ay, az) at c
+  uint32_t base = (uint32_t)(p.size() / 3);
+  for (uint32_t i = 0; i < nu; ++i) {
+    float u = TAU_F * (float)i / (float)nu;
+    for (uint32_t j = 0; j < nv; ++j) {
+      float v = TAU_F * (float)j / (float)nv;
+      float rad = R + r * std::cos(v);
+      float l[3] = {rad * std::cos(u), rad * std::sin(u), r * std::sin(v)};
+      for (int k = 0; k < 3; ++k) p.push_back(c[k] + ax[k] * l[0] + ay[k] * l[1] + az[k] * l[2]);
+    }
+  }
+  auto id = [&](uint32_t i, uint32_t j) { return base + (i % nu) * nv + (j % nv); };
+  for (uint32_t i = 0; i < nu; ++i)
+    for (uint32_t j = 0; j < nv; ++j) {
+      uint32_t q[6] = {id(i, j), id(i + 1, j), id(i + 1, j + 1), id(i, j), id(i + 1, j + 1), id(i, j + 1)};
+      for (int k = 0; k < 6; ++k) t.push_back(q[k]);
+      m.push_back(mat);
+      m.push_back(mat);
+    }
+}
+
+void append_stone(std::vector<float>& p, std::vector<uint32_t>& t, std::vector<uint16_t>& m,
+                  const std::vector<float>& sp, const std::vector<uint32_t>& st, float radius, const float c[3],
+                  const float ax[3], const float ay[3], const float az[3], uint16_t mat) {
+  uint32_t base = (uint32_t)(p.size() / 3);
+  for (size_t i = 0; i < sp.size(); i += 3) {
+    float l[3] = {sp[i] * radius, sp[i + 1] * radius, sp[i + 2] * radius};
+    for (int k = 0; k < 3; ++k) p.push_back(c[k] + ax[k] * l[0] + ay[k] * l[1] + az[k] * l[2]);
+  }
+  for (uint32_t i : st) t.push_back(base + i);
+  for (size_t i = 0; i < st.size() / 3; ++i) m.push_back(mat);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Gems workload: an 18k setting (torus shank + 37 prong cups, each a small
+// torus collar and four torus prongs) holding one round brilliant of
+// girdle radius `center_mm` on top and 36 smaller brilliants of girdle radius
+// `stone_mm` around the shank.  Materials: 0 = metal, 1 = centre stone,
+// 2..5 = the four side-stone gems, chosen per stone by `seed`.  `shank_nu`,
+// `shank_nv` set the shank tessellation (the setting's triangle count).
+int argent_synth_gem_ring(uint32_t shank_nu, uint32_t shank_nv, float center_mm, float stone_mm, uint32_t seed,
+                          ArgentMesh* out) {
+  if (!out || shank_nu < 3 || shank_nv < 3) return ARGENT_E_INVALID;
+  std::vector<float> p;
+  std::vector<uint32_t> t;
+  std::vector<uint16_t> m;
+  const float R = 9.0f, r = 1.1f;
+  const float X[3] = {1, 0, 0}, Y[3] = {0, 1, 0}, Z[3] = {0, 0, 1};
+  const float O[3] = {0, 0, 0};
+  append_torus(p, t, m, R, r, shank_nu, shank_nv, O, X, Y, Z, 0);
+  std::vector<float> sp;
+  std::vector<uint32_t> st;
+  polytope(brilliant_planes(), sp, st);
+  // centre stone on top of the shank, table up
+  const float ctop[3] = {0.0f, R + r + 0.9f * center_mm, 0.0f};
+  append_stone(p, t, m, sp, st, center_mm, ctop, X, Y, Z, 1);
+  auto cup = [&](const float c[3], const float ax[3], const float ay[3], const float az[3], float rad, uint32_t res) {
+    // collar under the girdle (local y is the stone's up axis)
+    float cc[3] = {c[0] - ay[0] * 0.05f * rad, c[1] - ay[1] * 0.05f * rad, c[2] - ay[2] * 0.05f * rad};
+    // the torus axis is local z: map (x, y, z)_torus -> (ax, az, ay) so it lies in the girdle plane
+    append_torus(p, t, m, rad * 1.05f, 0.08f * rad + 0.05f, res, res / 4, cc, ax, az, ay, 0);
+    for (int k = 0; k < 4; ++k) {
+      float a = TAU_F * (float)k / 4.0f + 0.39f;
+      float px = std::cos(a) * rad * 1.02f, pz = std::sin(a) * rad * 1.02f;
+      float pc[3];
+      for (int q = 0; q < 3; ++q) pc[q] = c[q] + ax[q] * px + az[q] * pz + ay[q] * 0.1f * rad;
+      float prx[3] = {-std::sin(a) * ax[0] + std::cos(a) * az[0], -std::sin(a) * ax[1] + std::cos(a) * az[1],
+                      -std::sin(a) * ax[2] + std::cos(a) * az[2]};
+      float pry[3] = {std::cos(a) * ax[0] + std::sin(a) * az[0], std::cos(a) * ax[1] + std::sin(a) * az[1],
+                      std::cos(a) * ax[2] + std::sin(a) * az[2]};
+      append_torus(p, t, m, 0.25f * rad, 0.06f * rad + 0.03f, res / 2, res / 8 + 3, pc, pry, ay, prx, 0);
+    }
+  };
+  cup(ctop, X, Y, Z, center_mm, 256);
+  // 36 side stones around the shank's outer surface, tables facing outward
+  uint32_t h = seed * 0x9e3779b9u + 0x7f4a7c15u;
+  for (int i = 0; i < 36; ++i) {
+    float a = TAU_F * ((float)i + 0.5f) / 36.0f;
+    float dir[3] = {std::cos(a), std::sin(a), 0.0f};
+    // skip the centre stone's seat on top
+    float rr = R + r + 0.35f * stone_mm;
+    float c[3] = {dir[0] * rr, dir[1] * rr, 0.0f};
+    const float* up = dir;
+    float ax2[3] = {-dir[1], dir[0], 0.0f};
+    h ^= h >> 16;
+    h *= 0x7feb352du;
+    h ^= h >> 15;
+    h *= 0x846ca68bu;
+    h ^= h >> 16;
+    uint16_t gem_slot = (uint16_t)(2 + (h >> 30));
+    append_stone(p, t, m, sp, st, stone_mm, c, ax2, up, Z, gem_slot);
+    cup(c, ax2, up, Z, stone_mm, 64);
   }
   return fill(out, p, t, m);
 }

@@ -69,3 +69,15 @@ def signet(R=9.0, r=1.2, nu=2048, nv=512, bezel_w=14.0, bezel_d=12.0, emboss_mm=
     if rc != N.OK:
         raise N.ArgentError(rc, "argent_synth_signet failed")
     return _take(m)
+
+
+def gem_ring(shank_nu=768, shank_nv=440, center_mm=2.0, stone_mm=0.75, seed=4) -> Mesh:
+    """The gems workload's piece: an 18k setting (torus shank + 37 prong
+    cups, about 0.9M triangles) holding a 4 mm round brilliant and 36 side
+    stones of 1.5 mm (argent_synth_gem_ring).  Material slots: 0 metal,
+    1 centre stone, 2..5 side-stone gems."""
+    m = N.ArgentMesh()
+    rc = N.host().argent_synth_gem_ring(shank_nu, shank_nv, center_mm, stone_mm, seed, ctypes.byref(m))
+    if rc != N.OK:
+        raise N.ArgentError(rc, "argent_synth_gem_ring failed")
+    return _take(m)

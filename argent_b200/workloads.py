@@ -12,6 +12,11 @@ Workloads (seeded, procedural; no argent assets are needed):
   ring_still     256 x 256, 16 spp, depth 8: 65,536-tri ring, sterling, noir, pinhole
   signet_still   1920 x 1080, 256 spp, depth 12: 2.1M-tri signet, 14k gold
                  (polished 0.05 / satin 0.35 slots), noir, 100 mm f/16, autofocus
+  gems_still     1080 x 1920, 512 spp, depth 32: 18k setting, brilliant and
+                 36 side stones, white studio, 100 mm pinhole
+  reel_batch     4 alloys x 36 turntable frames x 3 pieces (61k, 1.1M, 3.0M
+                 triangles), 1080 x 1920, 64 spp, depth 12, noir panels plus
+                 a 2048 x 1024 synthetic HDRI (env_pick 0.5), render seed 11
 """
 
 import ctypes
@@ -213,6 +218,21 @@ def signet_still(piece_gpu=None, spp=256, width=1920, height=1080, mesh=None):
     return Workload("signet_still_1920x1080_256spp", m, desc, cam, width, height, spp, settings(12), 7)
 
 
+SIDE_GEMS = ("ruby", "sapphire", "emerald", "garnet")
+
+
+def gems_still(piece_gpu=None, spp=512, width=1080, height=1920, mesh=None, max_depth=32):
+    """The gems workload: 18k gold setting (about 0.9M triangles) with a
+    diamond brilliant (argent's DIAMOND Sellmeier) and 36 side stones drawn
+    from ruby / sapphire / emerald / garnet; white studio, 1080 x 1920,
+    512 spp, max depth 32, 100 mm pinhole, hero view."""
+    m = mesh if mesh is not None else M.gem_ring()
+    cam, turn = shot(piece_gpu, hull(m), "hero", 100.0, 0.0, width / height)
+    mats = [metal("gold18k", 0.07, 0.8), gem("diamond")] + [gem(g) for g in SIDE_GEMS]
+    desc = _studio_scene(m, mats, "white", turn)
+    return Workload(f"gems_still_{width}x{height}_{spp}spp", m, desc, cam, width, height, spp, settings(max_depth), 7)
+
+
 def sphere(r=10.0, n=64):
     """tests/furnace.rs:19-44: a UV sphere with analytic normals."""
     f = np.float32
@@ -254,3 +274,87 @@ def furnace(material):
     N.host().argent_camera_look_at(_f3([0, 0, 200]), _f3([0, 0, 0]), _f3([0, 1, 0]), 100.0, 0.0, 1.0,
                                    ctypes.byref(cam))
     return Workload("furnace", m, desc, cam, 64, 64, 256, settings(32), 1)
+
+
+# ---------------------------------------------------------------- batched turntable reels
+
+REEL_ALLOYS = ("sterling", "gold14k", "rose14k", "bronze")
+# (label, nu, nv): the signet generator at 2 * nu * nv triangles
+REEL_PIECES = (("61k", 256, 120), ("1.1M", 1024, 540), ("3.0M", 2048, 732))
+REEL_FRAMES = 36
+
+
+def reel_piece(label):
+    """One of the batched workload's pieces (argent_synth_signet)."""
+    for name, nu, nv in REEL_PIECES:
+        if name == label:
+            return M.signet(nu=nu, nv=nv)
+    raise KeyError(label)
+
+
+def hdri(width=2048, height=1024, sigma=2.0, seed=5):
+    """The synthetic equirect map (argent_synth_hdri): (height, width, 3)
+    linear sRGB float32."""
+    rgb = np.zeros((height, width, 3), np.float32)
+    N.host().argent_synth_hdri(width, height, sigma, seed, rgb.ctypes.data_as(N.c_float_p))
+    return rgb
+
+
+def map_env(rgb, rotation_deg=0.0):
+    """Env::Map over `rgb` (kept alive by the caller)."""
+    env = N.ArgentEnv()
+    env.kind = N.ENV_MAP
+    env.power = 1.0
+    env.height, env.width = int(rgb.shape[0]), int(rgb.shape[1])
+    env.rgb = rgb.ctypes.data_as(N.c_float_p)
+    env.rotation_deg = float(rotation_deg)
+    return env
+
+
+def turntable_camera(points, view="hero", focal_mm=100.0, f_stop=0.0, aspect=1.0):
+    """Prepared::turntable_camera (shot.rs:318-327): frame the hull turned
+    through 24 steps of 15 degrees from the front (azimuth 0).  Returns the
+    camera and the view's azimuth."""
+    az, el, fill = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+    N.check(N.host().argent_view_named(view.encode(), ctypes.byref(az), ctypes.byref(el), ctypes.byref(fill)))
+    pts = np.concatenate([rot_y(points, 15.0 * k) for k in range(24)])
+    return frame(pts, 0.0, el.value, fill.value, focal_mm, f_stop, aspect), az.value
+
+
+def reel_frame_turn(azimuth, i, n=REEL_FRAMES):
+    """render_reel's turntable rig (jobs.rs:617-621): -azimuth + 360 i / n."""
+    return -azimuth + 360.0 * float(i) / float(n)
+
+
+def reel_scene(m, alloy, env_rgb, turn):
+    """The batched workload's scene for one piece and alloy: polished (0.05)
+    and satin (0.35) slots of the alloy, the noir studio's panels and floor,
+    and the map as the environment, so NEE picks the map with probability
+    0.5 (scene.rs:105-109)."""
+    radius, floor_y = piece_radius(m)
+    panels, _, fm, fl, white = studio("noir", radius, floor_y)
+    mats = [metal(alloy, 0.05, 0.8), metal(alloy, 0.35, 0.8), fm]
+    fl.material = len(mats) - 1
+    desc = SceneDesc(mats, panels, map_env(env_rgb), fl, turn, white)
+    desc.keep(env_rgb)
+    return desc
+
+
+def reel_batch(pieces=None, alloys=REEL_ALLOYS, frames=range(REEL_FRAMES), width=1080, height=1920, spp=64,
+               env_rgb=None):
+    """The batched workload as a list of Workloads, piece-major then alloy
+    then frame.  `pieces` maps label -> Mesh (built when None)."""
+    if pieces is None:
+        pieces = {label: reel_piece(label) for label, _, _ in REEL_PIECES}
+    if env_rgb is None:
+        env_rgb = hdri()
+    out = []
+    for label, m in pieces.items():
+        cam, az = turntable_camera(hull(m), "hero", 100.0, 0.0, width / height)
+        for alloy in alloys:
+            for i in frames:
+                turn = reel_frame_turn(az, i)
+                desc = reel_scene(m, alloy, env_rgb, turn)
+                out.append(Workload(f"reel_{label}_{alloy}_f{i:02d}_{width}x{height}_{spp}spp", m, desc, cam, width,
+                                    height, spp, settings(12), 11, {"piece": label, "alloy": alloy, "frame": i}))
+    return out

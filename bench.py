@@ -170,12 +170,29 @@ def cpu_sample(wl, seconds=12.0, threads=0, rows=None):
     return wl.width * rows * wl.spp / dt, rows, nthr, sc
 
 
-def build_workload(name, tracer=None, spp=None):
+WORKLOADS = ("signet_still", "ring_still", "gems_still", "reel_batch")
+DATA = {"signet_still": "seeded procedural signet, noir studio",
+        "ring_still": "seeded procedural ring, noir studio",
+        "gems_still": "seeded procedural 18k setting with a brilliant and 36 side stones, white studio",
+        "reel_batch": "seeded procedural signets of 61k/1.1M/3.0M triangles, seeded synthetic HDRI"}
+
+
+def build_mesh(name):
+    from argent_b200 import mesh as M
+
+    return {"signet_still": M.signet, "ring_still": M.ring, "gems_still": M.gem_ring}[name]()
+
+
+def build_workload(name, mesh, tracer=None):
+    """The named workload on `mesh`; `tracer` (anything with
+    trace_closest) enables thin-lens autofocus where the shot uses it."""
     from argent_b200 import workloads as W
 
     if name == "ring_still":
-        return W.ring_still(spp=spp or 16)
-    return W.signet_still(tracer, spp=spp or 256)
+        return W.ring_still()
+    if name == "gems_still":
+        return W.gems_still(tracer, mesh=mesh)
+    return W.signet_still(tracer, mesh=mesh)
 
 
 class OracleTracer:
@@ -190,37 +207,73 @@ class OracleTracer:
         return self.bvh.intersect(np.ascontiguousarray(rays, np.float32))
 
 
+def reference_wls(name):
+    """The renders the reference arm samples: the still itself, or for the
+    batched workload one render per piece (14k gold), whose turntable frame
+    follows the step index."""
+    if name != "reel_batch":
+        m = build_mesh(name)
+        return [build_workload(name, m, OracleTracer(m))]
+    from argent_b200 import workloads as W
+
+    pieces = {label: W.reel_piece(label) for label, _, _ in W.REEL_PIECES}
+    return W.reel_batch(pieces, alloys=("gold14k",), frames=[0])
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    from argent_b200 import mesh as M
+    import oracle as O
 
-    m = M.signet() if args.workload == "signet_still" else None
-    tracer = OracleTracer(m) if m is not None else None
-    from argent_b200 import workloads as W
-
-    wl = W.signet_still(tracer, mesh=m) if m is not None else W.ring_still()
+    wls = reference_wls(args.workload)
+    scenes = [O.Scene(wl.mesh, wl.desc.c) for wl in wls]
     threads = os.cpu_count() or 1
-    _, rows, nthr, sc = cpu_sample(wl, seconds=args.ref_seconds, threads=threads)
+    reel = args.workload == "reel_batch"
+    turn = {}
+    if reel:
+        from argent_b200 import workloads as W
+
+        for wl in wls:
+            _, turn[wl.name] = W.turntable_camera(W.hull(wl.mesh), "hero", 100.0, 0.0, wl.width / wl.height)
+
+    def band(k, rows):
+        for wl, sc in zip(wls, scenes):
+            if reel:
+                sc.set_turntable(W.reel_frame_turn(turn[wl.name], k % W.REEL_FRAMES))
+            mid = wl.height // 2
+            sc.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, wl.spp, wl.seed, rows=(mid, mid + rows),
+                           threads=threads, want_xyz=False)
+
+    t0 = time.perf_counter()
+    band(0, 1)
+    dt = time.perf_counter() - t0
+    rows = int(max(1, min(wls[0].height // 2, args.ref_seconds / max(dt, 1e-3))))
     times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        sc.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, wl.spp, wl.seed,
-                       rows=(wl.height // 2, wl.height // 2 + rows), threads=threads, want_xyz=False)
+        band(i, rows)
         if i >= args.warmup:
             times.append(time.perf_counter() - t0)
-    per = wl.width * rows * wl.spp
+    per = sum(wl.width * rows * wl.spp for wl in wls)
     value = per * len(times) / sum(times)
-    sample = f"rows {wl.height // 2}..{wl.height // 2 + rows} of the {wl.width}x{wl.height} frame at {wl.spp} spp ({per} path-samples per step)"
+    wl = wls[0]
+    what = (f"{len(wls)} renders (one per piece, 14k gold, turntable frame = step)" if reel else "the frame")
+    sample = (f"rows {wl.height // 2}..{wl.height // 2 + rows} of {what}, {wl.width} wide at {wl.spp} spp "
+              f"({per} path-samples per step)")
+    cfg = {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp,
+           "triangles": int(wl.mesh.num_tris), "max_depth": int(wl.settings.max_depth),
+           "parallelism": "cpu-threads"}
+    if reel:
+        cfg["workload"] = (f"reel_batch_{len(W.REEL_PIECES) * len(W.REEL_ALLOYS)}x{W.REEL_FRAMES}frames_"
+                           f"{wl.width}x{wl.height}_{wl.spp}spp")
+        cfg["triangles"] = {w.extra["piece"]: int(w.mesh.num_tris) for w in wls}
     out = {
         "impl": "reference", "metric": "path-samples/s", "value": value, "unit": "path-samples/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": value / PUBLISHED_CPU, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp,
-                   "triangles": int(wl.mesh.num_tris), "max_depth": int(wl.settings.max_depth),
-                   "parallelism": "cpu-threads"},
-        "cpu_baseline": {"value": value, "unit": "path-samples/s", "cores": nthr, "kind": "port",
+        "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "path-samples/s", "cores": threads, "kind": "port",
                          "sample": sample + "; argent's Rust path cannot be built here (no cargo), so the C++ "
                                             "restatement (oracle/) runs, OpenMP over rows"},
         "e2e": {"value": value, "unit": "path-samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -230,41 +283,137 @@ def run_reference(args, world, rank):
 
 # ------------------------------------------------------------------ GPU arm
 
+class StillPlan:
+    """One still per step: film cleared, one render_pass."""
+
+    def __init__(self, ctx, name):
+        from argent_b200.gpu import Film, Piece, Scene
+
+        self.mesh = build_mesh(name)
+        self.piece = Piece(ctx, self.mesh)
+        self.wl = build_workload(name, self.mesh, self.piece)
+        self.scene = Scene(ctx, self.piece, self.wl.desc)
+        self.films = [Film(ctx, self.wl.width, self.wl.height)]
+        self.cpu_wl = self.wl
+        self.name = self.wl.name
+        self.renders = 1
+        self.triangles = int(self.mesh.num_tris)
+        self.device_bytes = self.piece.device_bytes
+
+    def set_spp(self, spp):
+        self.wl.spp = spp
+
+    def items(self, k, films=None, spp=None):
+        wl = self.wl
+        return [(self.scene, wl.camera, (films or self.films)[0], wl.settings, spp or wl.spp, wl.seed)]
+
+    @property
+    def path_samples(self):
+        return self.wl.path_samples
+
+    @property
+    def pixels(self):
+        return self.wl.width * self.wl.height
+
+    def config(self):
+        wl = self.wl
+        return {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp,
+                "triangles": self.triangles, "max_depth": int(wl.settings.max_depth)}
+
+
+class ReelPlan:
+    """The batched workload: step k renders turntable frame k (mod 36) of
+    every piece x alloy (3 x 4 = 12 renders) as one render_batch."""
+
+    def __init__(self, ctx):
+        from argent_b200 import workloads as W
+        from argent_b200.gpu import Film, Piece, Scene
+
+        self.W = W
+        pieces = {label: W.reel_piece(label) for label, _, _ in W.REEL_PIECES}
+        env = W.hdri()
+        self.wls = W.reel_batch(pieces, frames=[0], env_rgb=env)
+        self.gpu_pieces = {label: Piece(ctx, m) for label, m in pieces.items()}
+        self.scenes = [Scene(ctx, self.gpu_pieces[wl.extra["piece"]], wl.desc) for wl in self.wls]
+        self.az = {}
+        for label, m in pieces.items():
+            _, self.az[label] = W.turntable_camera(W.hull(m), "hero", 100.0, 0.0, 1080 / 1920)
+        self.films = [Film(ctx, wl.width, wl.height) for wl in self.wls]
+        self.cpu_wl = next(wl for wl in self.wls if wl.extra["piece"] == "1.1M")
+        wl0 = self.wls[0]
+        self.name = f"reel_batch_{len(self.wls)}x{W.REEL_FRAMES}frames_{wl0.width}x{wl0.height}_{wl0.spp}spp"
+        self.renders = len(self.wls)
+        self.triangles = {label: int(m.num_tris) for label, m in pieces.items()}
+        self.device_bytes = sum(p.device_bytes for p in self.gpu_pieces.values())
+        self.spp = wl0.spp
+
+    def set_spp(self, spp):
+        self.spp = spp
+
+    def items(self, k, films=None, spp=None):
+        frame = k % self.W.REEL_FRAMES
+        out = []
+        for wl, sc, f in zip(self.wls, self.scenes, films or self.films):
+            sc.set_turntable(self.W.reel_frame_turn(self.az[wl.extra["piece"]], frame))
+            out.append((sc, wl.camera, f, wl.settings, spp or self.spp, wl.seed))
+        return out
+
+    @property
+    def path_samples(self):
+        return sum(wl.width * wl.height for wl in self.wls) * self.spp
+
+    @property
+    def pixels(self):
+        return sum(wl.width * wl.height for wl in self.wls)
+
+    def config(self):
+        wl = self.wls[0]
+        return {"workload": self.name, "width": wl.width, "height": wl.height, "spp": self.spp,
+                "triangles": self.triangles, "max_depth": int(wl.settings.max_depth),
+                "renders_per_step": self.renders, "alloys": list(self.W.REEL_ALLOYS),
+                "env": "2048x1024 synthetic HDRI + noir panels (env_pick 0.5)",
+                "subset": f"each step is one turntable frame of all {self.renders} piece x alloy renders; "
+                          f"steps walk the {self.W.REEL_FRAMES} frames"}
+
+
+def run_plan(ctx, plan, k, films=None, spp=None):
+    from argent_b200.gpu import render_batch, render_pass
+
+    items = plan.items(k, films, spp)
+    for it in items:
+        it[2].clear()
+    if len(items) == 1:
+        render_pass(ctx, *items[0])
+    else:
+        render_batch(ctx, items)
+
+
 def run_gpu(args, world, rank, device):
     import torch
 
-    from argent_b200 import mesh as M
-    from argent_b200.gpu import Context, Film, Piece, Scene, render_pass
+    from argent_b200 import _native as N
+    from argent_b200.gpu import Context, Film
 
     torch.cuda.set_device(device)
     ctx = Context(device)
-    m = M.signet() if args.workload == "signet_still" else M.ring()
-    piece = Piece(ctx, m)
-    from argent_b200 import workloads as W
-
-    wl = W.signet_still(piece, mesh=m) if args.workload == "signet_still" else W.ring_still()
+    plan = ReelPlan(ctx) if args.workload == "reel_batch" else StillPlan(ctx, args.workload)
     if args.spp:
-        wl.spp = args.spp  # profiling runs only: the bench line uses the workload's spp
-    scene = Scene(ctx, piece, wl.desc)
-    film = Film(ctx, wl.width, wl.height)
+        plan.set_spp(args.spp)  # profiling runs only: the bench line uses the workload's spp
     stream = torch.cuda.ExternalStream(ctx.stream)
 
-    def step():
-        film.clear()
-        render_pass(ctx, scene, wl.camera, film, wl.settings, wl.spp, wl.seed)
-
-    for _ in range(args.warmup):
-        step()
+    for i in range(args.warmup):
+        run_plan(ctx, plan, i)
     ctx.sync()
 
     # Instrumented pass (not timed): traversal visits per ray, rays per sample.
-    cf = Film(ctx, wl.width, wl.height)
+    cfilms = [Film(ctx, f.width, f.height) for f in plan.films]
     ctx.set_counting(True)
-    render_pass(ctx, scene, wl.camera, cf, wl.settings, 1, wl.seed)
+    run_plan(ctx, plan, 0, cfilms, 1)
     counts = ctx.traversal_counts()
     ctx.set_counting(False)
-    cf.close()
-    px = wl.width * wl.height
+    for f in cfilms:
+        f.close()
+    px = plan.pixels
 
     # Timed region (device time, CUDA events on the library stream).
     barrier(world, device)
@@ -278,8 +427,8 @@ def run_gpu(args, world, rank, device):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
-        step()
+    for i in range(args.steps):
+        run_plan(ctx, plan, args.warmup + i)
     e1.record(stream)
     e1.synchronize()
     ctx.sync()
@@ -290,7 +439,7 @@ def run_gpu(args, world, rank, device):
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(ms, world, device)
     barrier(world, device)
-    samples_per_step = wl.path_samples
+    samples_per_step = plan.path_samples
     value = world * samples_per_step * args.steps / (ms_max / 1000.0)
 
     # Roofline of the dominant kernel.
@@ -308,53 +457,53 @@ def run_gpu(args, world, rank, device):
     # hit attributes (index 16 B + 3 positions + 3 normals 96 B), spectral tables (~64 B)
     per_sample["shade"] = rays_c * (152 + 112 + 112 + 64)
     per_sample["raygen"] = 176.0
-    per_sample["film"] = 64.0 + 12.0 * 3 / max(wl.spp, 1)
+    per_sample["film"] = 64.0 + 12.0 * 3 / max(plan.config()["spp"], 1)
     alg_bytes_total = per_sample[dom] * path_samples_timed
     achieved = alg_bytes_total / (dom_ms / 1000.0) / 1e9  # GB/s
     peak, peak_kind = peaks()
     traffic = None
     tr = ncu_traffic()
-    if tr and tr.get("kernel") == dom and tr.get("workload") == wl.name:
+    if tr and tr.get("kernel") == dom and tr.get("workload") == plan.name:
         traffic = tr.get("dram_bytes_per_launch")
 
     # End-to-end through the C ABI with host buffers.
     e2e_value = None
-    h2d = ctypes.sizeof(type(wl.camera)) + ctypes.sizeof(type(wl.settings)) + 8
+    h2d = plan.renders * (ctypes.sizeof(N.ArgentCamera) + ctypes.sizeof(N.ArgentPathSettings) + 8)
     d2h = 3 * px * 3 * 4
     if args.e2e_steps > 0:
-        c = np.zeros((wl.height, wl.width, 3), np.float32)
-        a = np.zeros_like(c)
-        nrm = np.zeros_like(c)
+        bufs = [tuple(np.zeros((f.height, f.width, 3), np.float32) for _ in range(3)) for f in plan.films]
         fp = ctypes.POINTER(ctypes.c_float)
         barrier(world, device)
         t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            film.clear()
-            render_pass(ctx, scene, wl.camera, film, wl.settings, wl.spp, wl.seed)
-            ctx.check(ctx.lib.argent_film_read(film.h, c.ctypes.data_as(fp), a.ctypes.data_as(fp),
-                                               nrm.ctypes.data_as(fp)))
+        for i in range(args.e2e_steps):
+            run_plan(ctx, plan, i)
+            for f, (c, a, nrm) in zip(plan.films, bufs):
+                ctx.check(ctx.lib.argent_film_read(f.h, c.ctypes.data_as(fp), a.ctypes.data_as(fp),
+                                                   nrm.ctypes.data_as(fp)))
         dt = time.perf_counter() - t0
         dt = max_over_ranks(dt, world, device)
         e2e_value = world * samples_per_step * args.e2e_steps / dt
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
+        wl = plan.cpu_wl
         v, rows, nthr, _ = cpu_sample(wl, seconds=args.ref_seconds, threads=os.cpu_count() or 1)
         cpu = {"value": v, "unit": "path-samples/s", "cores": nthr, "kind": "port",
-               "sample": f"rows {wl.height // 2}..{wl.height // 2 + rows} of the frame at {wl.spp} spp; argent's "
-                         f"algorithm as restated in oracle/ (Rust reference not buildable here), OpenMP over rows"}
+               "sample": f"{wl.name}: rows {wl.height // 2}..{wl.height // 2 + rows} of the frame at {wl.spp} spp; "
+                         f"argent's algorithm as restated in oracle/ (Rust reference not buildable here), "
+                         f"OpenMP over rows"}
 
     if rank == 0:
+        cfg = plan.config()
+        cfg.update({"parallelism": f"replicas{world}", "l2": "inputs larger than L2 (path state "
+                    f"{ctx_wave_mb(ctx)} MB per wave + BVH/triangles {plan.device_bytes / 1e6:.0f} MB)",
+                    "vs_baseline_ref": "README.md:5-6 ~17.7M path-samples/s on 32 CPU cores"})
         out = {
             "metric": "path-samples/s", "value": value, "unit": "path-samples/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": value / PUBLISHED_CPU, "dtype": "f32",
-            "data": "synthetic (seeded procedural signet, noir studio)",
-            "config": {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp,
-                       "triangles": int(m.num_tris), "max_depth": int(wl.settings.max_depth),
-                       "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (path state "
-                       f"{ctx_wave_mb(ctx)} MB per wave + BVH/triangles {piece.device_bytes / 1e6:.0f} MB)",
-                       "vs_baseline_ref": "README.md:5-6 ~17.7M path-samples/s on 32 CPU cores"},
+            "data": f"synthetic ({DATA[args.workload]})",
+            "config": cfg,
             "clocks": ck,
             "e2e": {"value": e2e_value, "unit": "path-samples/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -381,7 +530,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="argent", choices=["argent", "reference"])
-    ap.add_argument("--workload", default="signet_still", choices=["signet_still", "ring_still"])
+    ap.add_argument("--workload", default="signet_still", choices=list(WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")

@@ -130,6 +130,18 @@ void argent_frame(const float* points, uint32_t n, float azimuth_deg, float elev
  * photographed HDR, which the workloads do not ship. */
 void argent_synth_hdri(uint32_t width, uint32_t height, float sigma, uint32_t seed, float* rgb);
 
+/*
+ * Gems workload piece: a torus shank (shank_nu x shank_nv quads) with 37
+ * prong cups (a torus collar and four torus prongs each), one round
+ * brilliant of girdle radius center_mm on top and 36 brilliants of girdle
+ * radius stone_mm around the shank.  The brilliant is the polytope of its
+ * facet half-spaces: table, 8 stars, 8 bezels, 16 upper and 16 lower girdle
+ * halves, 8 pavilion mains (57 facets) and a 32-facet girdle band.
+ * Material slots: 0 metal, 1 centre stone, 2..5 side stones (by seed).
+ */
+int argent_synth_gem_ring(uint32_t shank_nu, uint32_t shank_nv, float center_mm, float stone_mm, uint32_t seed,
+                          ArgentMesh* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -136,3 +136,66 @@ def test_batch_equals_separate_passes():
     assert np.array_equal(f1.xyz(), g1.xyz())
     assert np.array_equal(f2.xyz(), g2.xyz())
     assert not np.array_equal(f1.xyz(), f2.xyz())
+
+
+@pytest.mark.gpu
+def test_gems_render_matches_oracle():
+    """The gems workload (diamond + ruby/sapphire/emerald/garnet in an 18k
+    setting, white studio, depth 32) at reduced size: 108 x 192, 8 spp."""
+    import oracle as O
+
+    wl = W.gems_still(spp=8, width=108, height=192)
+    xyz_gpu, _, _ = _gpu_render(wl)
+    sc = O.Scene(wl.mesh, wl.desc.c)
+    _, _, _, xyz = sc.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, wl.spp, wl.seed)
+    e = rel_rmse(xyz_gpu, xyz / wl.spp)
+    print("gems_still 108x192x8 relRMSE XYZ vs oracle:", e)
+    assert np.all(e <= RELRMSE_TOL), e
+
+
+@pytest.mark.gpu
+def test_signet_render_matches_oracle_on_a_band():
+    """The bench workload itself (2.1M triangles, thin lens, two metal slots)
+    on rows 500..520 of the 1920 x 1080 frame at 8 spp."""
+    import oracle as O
+    from argent_b200 import mesh as M
+    from argent_b200.gpu import Context, Film, Piece, Scene, render_pass
+
+    m = M.signet()
+    ctx = Context(0)
+    piece = Piece(ctx, m)
+    wl = W.signet_still(piece, spp=8, mesh=m)
+    scene = Scene(ctx, piece, wl.desc)
+    film = Film(ctx, wl.width, wl.height)
+    render_pass(ctx, scene, wl.camera, film, wl.settings, wl.spp, wl.seed)
+    xyz_gpu = film.xyz()
+    sc = O.Scene(m, wl.desc.c)
+    _, _, _, xyz = sc.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, wl.spp, wl.seed, rows=(500, 520))
+    e = rel_rmse(xyz_gpu[500:520], xyz[500:520] / wl.spp)
+    print("signet_still rows 500..520 x 8 spp relRMSE XYZ vs oracle:", e)
+    assert np.all(e <= RELRMSE_TOL), e
+
+
+@pytest.mark.gpu
+def test_reel_batch_matches_oracle():
+    """The batched workload's scenes (HDRI map plus panels, env_pick 0.5,
+    turntable frames, two alloys) through one render_batch at 108 x 192 and
+    8 spp; each film against the oracle's render of the same frame."""
+    import oracle as O
+    from argent_b200.gpu import Context, Film, Piece, Scene, render_batch
+
+    m = W.reel_piece("61k")
+    env = W.hdri()
+    wls = W.reel_batch({"61k": m}, alloys=("sterling", "bronze"), frames=[0, 9], width=108, height=192, spp=8,
+                       env_rgb=env)
+    ctx = Context(0)
+    piece = Piece(ctx, m)
+    scenes = [Scene(ctx, piece, wl.desc) for wl in wls]
+    films = [Film(ctx, wl.width, wl.height) for wl in wls]
+    render_batch(ctx, [(sc, wl.camera, f, wl.settings, wl.spp, wl.seed) for sc, wl, f in zip(scenes, wls, films)])
+    for wl, f in zip(wls, films):
+        sc = O.Scene(m, wl.desc.c)
+        _, _, _, xyz = sc.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, wl.spp, wl.seed)
+        e = rel_rmse(f.xyz(), xyz / wl.spp)
+        print(wl.name, "relRMSE XYZ vs oracle:", e)
+        assert np.all(e <= RELRMSE_TOL), (wl.name, e)
