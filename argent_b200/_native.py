@@ -100,6 +100,26 @@ class ArgentBatchItem(ctypes.Structure):
                 ("settings", ArgentPathSettings), ("count", ctypes.c_uint32), ("seed", ctypes.c_uint32)]
 
 
+class ArgentServeConfig(ctypes.Structure):
+    _fields_ = [("film_budget", ctypes.c_uint64), ("max_active", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("step_path_samples", ctypes.c_uint64)]
+
+
+class ArgentServeRequest(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_void_p), ("camera", ArgentCamera), ("settings", ArgentPathSettings),
+                ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("spp", ctypes.c_uint32),
+                ("seed", ctypes.c_uint32), ("film_flags", ctypes.c_uint32), ("priority", ctypes.c_int32)]
+
+
+class ArgentServeStatus(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int32), ("samples", ctypes.c_uint32), ("spp", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("t_submit", ctypes.c_double), ("t_start", ctypes.c_double),
+                ("t_done", ctypes.c_double)]
+
+
+REQ_QUEUED, REQ_ACTIVE, REQ_DONE, REQ_CANCELLED, REQ_FAILED = range(5)
+
+
 class ArgentMesh(ctypes.Structure):
     _fields_ = [("nv", ctypes.c_uint32), ("nt", ctypes.c_uint32), ("positions", c_float_p), ("normals", c_float_p),
                 ("tris", c_u32_p), ("tri_material", c_u16_p)]
@@ -148,6 +168,20 @@ GPU_FUNCS = {
                                                ctypes.POINTER(ctypes.c_uint64)]),
     "argent_ctx_set_counting": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "argent_ctx_traversal_counts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
+    "argent_ctx_traversal_histogram": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
+    "argent_serve_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ArgentServeConfig),
+                                           ctypes.POINTER(ctypes.c_void_p)]),
+    "argent_serve_destroy": (None, [ctypes.c_void_p]),
+    "argent_serve_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ArgentServeRequest),
+                                           ctypes.POINTER(ctypes.c_uint64)]),
+    "argent_serve_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ArgentServeStatus)]),
+    "argent_serve_cancel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "argent_serve_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
+    "argent_serve_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, c_float_p, c_float_p, c_float_p]),
+    "argent_serve_release": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "argent_serve_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
+                                          ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+    "argent_serve_now": (ctypes.c_double, [ctypes.c_void_p]),
 }
 KERNEL_CLASSES = ["raygen", "intersect", "shade", "shadow", "film", "trace"]
 

@@ -1,6 +1,7 @@
 """Build the native libraries in-tree.
 
-  argent_b200/lib/libargent_gpu.so   CUDA kernels + C ABI (include/argent_gpu.h), sm_100a
+  argent_b200/lib/libargent_gpu.so   CUDA kernels + C ABI (include/argent_gpu.h), sm_100a,
+                                     with the serve scheduler (host/serve.cpp) over that ABI
   argent_b200/lib/libargent_host.so  host-side scene builders (include/argent_host.h)
 
 The CUDA library is compiled with --fmad=false: argent's Rust code rounds
@@ -26,6 +27,7 @@ GPU_SOURCES = [
     os.path.join(CSRC, "argent_gpu.cu"),
     os.path.join(CSRC, "host", "bvh_build.cpp"),
     os.path.join(CSRC, "host", "scene_prep.cpp"),
+    os.path.join(CSRC, "host", "serve.cpp"),
 ]
 HOST_SOURCES = [
     os.path.join(CSRC, "host", "synth.cpp"),

@@ -117,21 +117,22 @@ static cudaEvent_t prof_event(ArgentCtx* ctx) {
   return e;
 }
 
-// Brackets one launch with events on the context stream when profiling.
+// Brackets one launch with events on its stream when profiling.
 struct ProfScope {
   ArgentCtx* ctx;
   int kind;
+  cudaStream_t s;
   cudaEvent_t a = nullptr;
-  ProfScope(ArgentCtx* c, int k) : ctx(c), kind(k) {
+  ProfScope(ArgentCtx* c, int k, cudaStream_t st = nullptr) : ctx(c), kind(k), s(st ? st : c->stream) {
     if (ctx->prof.on) {
       a = prof_event(ctx);
-      cudaEventRecord(a, ctx->stream);
+      cudaEventRecord(a, s);
     }
   }
   ~ProfScope() {
     if (a) {
       cudaEvent_t b = prof_event(ctx);
-      cudaEventRecord(b, ctx->stream);
+      cudaEventRecord(b, s);
       ctx->prof.ev[kind].push_back({a, b});
     }
   }
@@ -172,6 +173,13 @@ int argent_ctx_create(int device, const ArgentLimits* limits, ArgentCtx** out) {
   if (ctx->limits.wave_paths == 0) ctx->limits.wave_paths = 1ull << 21;
   cudaError_t r = cudaSetDevice(device);
   if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  ctx->lane_stream[0] = ctx->stream;
+  for (int l = 1; l < ARGENT_LANES && r == cudaSuccess; ++l)
+    r = cudaStreamCreateWithFlags(&ctx->lane_stream[l], cudaStreamNonBlocking);
+  if (r == cudaSuccess) r = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming);
+  if (r == cudaSuccess) r = cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming);
+  for (int l = 0; l < ARGENT_LANES && r == cudaSuccess; ++l)
+    r = cudaEventCreateWithFlags(&ctx->film_ev[l], cudaEventDisableTiming);
   if (r == cudaSuccess) r = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (r == cudaSuccess) r = cudaMalloc(&ctx->d_status, sizeof(uint32_t) * 4);
   if (r == cudaSuccess) r = cudaMemset(ctx->d_status, 0, sizeof(uint32_t) * 4);
@@ -195,8 +203,14 @@ void argent_ctx_destroy(ArgentCtx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   prof_collect(ctx);
   for (cudaEvent_t e : ctx->prof.pool) cudaEventDestroy(e);
-  ctx->wave.release();
+  for (int l = 0; l < ARGENT_LANES; ++l) ctx->wave[l].release();
   if (ctx->d_status) cudaFree(ctx->d_status);
+  for (int l = 1; l < ARGENT_LANES; ++l)
+    if (ctx->lane_stream[l]) cudaStreamDestroy(ctx->lane_stream[l]);
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+  if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
+  for (int l = 0; l < ARGENT_LANES; ++l)
+    if (ctx->film_ev[l]) cudaEventDestroy(ctx->film_ev[l]);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -411,8 +425,8 @@ static int ensure_tables(ArgentCtx* ctx) {
   return ARGENT_OK;
 }
 
-static int ensure_wave(ArgentCtx* ctx) {
-  WaveBuffers& w = ctx->wave;
+static int ensure_wave(ArgentCtx* ctx, int lane) {
+  WaveBuffers& w = ctx->wave[lane];
   uint64_t cap = ctx->limits.wave_paths;
   if (w.cap == cap) return ARGENT_OK;
   w.release();
@@ -496,23 +510,7 @@ std::vector<dev::WaveDesc> plan_waves(const std::vector<dev::DevJob>& jobs, cons
 
 }  // namespace
 
-static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const std::vector<uint32_t>& counts,
-                    const std::vector<uint32_t>& scene_classes) {
-  int rc = ensure_tables(ctx);
-  if (rc != ARGENT_OK) return rc;
-  rc = ensure_wave(ctx);
-  if (rc != ARGENT_OK) return rc;
-  WaveBuffers& wb = ctx->wave;
-  std::vector<uint32_t> depths;
-  std::vector<dev::WaveDesc> waves = plan_waves(jobs, counts, wb.cap, &depths);
-  if (waves.empty()) return ARGENT_OK;
-  dev::DevJob* d_jobs = nullptr;
-  ARGENT_CK(ctx, cudaMallocAsync((void**)&d_jobs, jobs.size() * sizeof(dev::DevJob), ctx->stream));
-  // Pageable source: the call returns once the bytes are staged.
-  ARGENT_CK(ctx, cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(dev::DevJob), cudaMemcpyHostToDevice,
-                                 ctx->stream));
-  dev::WaveArgs a{};
-  a.jobs = d_jobs;
+static void fill_args(dev::WaveArgs& a, const WaveBuffers& wb) {
   a.o = wb.o;
   a.d = wb.d;
   a.beta = wb.beta;
@@ -528,10 +526,41 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   a.meta = wb.meta;
   a.rng = wb.rng;
   a.counters = wb.counters;
-  a.status = ctx->d_status;
   a.qc = wb.qc;
   a.cap = (uint32_t)wb.cap;
-  uint32_t cap = (uint32_t)wb.cap;
+}
+
+// Renders every job's samples, wave by wave.  Wave i runs on lane i % 2
+// (its own stream and path state); the film kernels of successive waves are
+// chained by events, so films accumulate in wave order exactly as on one
+// stream.  The lanes fork from and join back into the context stream.
+static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const std::vector<uint32_t>& counts,
+                    const std::vector<uint32_t>& scene_classes) {
+  int rc = ensure_tables(ctx);
+  if (rc != ARGENT_OK) return rc;
+  for (int l = 0; l < ARGENT_LANES; ++l) {
+    rc = ensure_wave(ctx, l);
+    if (rc != ARGENT_OK) return rc;
+  }
+  uint32_t cap = (uint32_t)ctx->wave[0].cap;
+  std::vector<uint32_t> depths;
+  std::vector<dev::WaveDesc> waves = plan_waves(jobs, counts, cap, &depths);
+  if (waves.empty()) return ARGENT_OK;
+  dev::DevJob* d_jobs = nullptr;
+  ARGENT_CK(ctx, cudaMallocAsync((void**)&d_jobs, jobs.size() * sizeof(dev::DevJob), ctx->stream));
+  // Pageable source: the call returns once the bytes are staged.
+  ARGENT_CK(ctx, cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(dev::DevJob), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+  int lanes = (int)std::min<size_t>(ARGENT_LANES, waves.size());
+  ARGENT_CK(ctx, cudaEventRecord(ctx->fork_ev, ctx->stream));
+  for (int l = 1; l < lanes; ++l) ARGENT_CK(ctx, cudaStreamWaitEvent(ctx->lane_stream[l], ctx->fork_ev, 0));
+  dev::WaveArgs args[ARGENT_LANES];
+  for (int l = 0; l < ARGENT_LANES; ++l) {
+    args[l] = dev::WaveArgs{};
+    args[l].jobs = d_jobs;
+    args[l].status = ctx->d_status;
+    fill_args(args[l], ctx->wave[l]);
+  }
   int g_ray = grid_for(ctx, (const void*)dev::k_raygen, 256, cap);
   int g_int = grid_for(ctx, (const void*)dev::k_intersect, 128, cap);
   int g_sh = grid_for(ctx, (const void*)dev::k_shade<CLS_METAL>, 128, cap);
@@ -539,43 +568,53 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   int g_film = grid_for(ctx, (const void*)dev::k_film, 256, cap);
   for (size_t wi = 0; wi < waves.size(); ++wi) {
     const dev::WaveDesc& w = waves[wi];
+    int lane = (int)(wi % lanes);
+    cudaStream_t st = ctx->lane_stream[lane];
+    dev::WaveArgs& a = args[lane];
+    const WaveBuffers& wb = ctx->wave[lane];
     uint32_t classes = 1u << CLS_TERMINAL;
     for (uint32_t sgi = 0; sgi < w.num_segments; ++sgi) classes |= scene_classes[w.seg[sgi].job];
     a.q_in = wb.q0;
     a.q_out = wb.q1;
     {
-      ProfScope ps(ctx, KC_RAYGEN);
-      dev::k_raygen<<<g_ray, 256, 0, ctx->stream>>>(a, w);
+      ProfScope ps(ctx, KC_RAYGEN, st);
+      dev::k_raygen<<<g_ray, 256, 0, st>>>(a, w);
     }
     ctx->launches++;
     for (uint32_t depth = 0; depth < depths[wi] && depth < ARGENT_MAX_DEPTH; ++depth) {
       a.q_in = (depth & 1) ? wb.q1 : wb.q0;
       a.q_out = (depth & 1) ? wb.q0 : wb.q1;
       {
-        ProfScope ps(ctx, KC_INTERSECT);
-        dev::k_intersect<<<g_int, 128, 0, ctx->stream>>>(a, (int)depth);
+        ProfScope ps(ctx, KC_INTERSECT, st);
+        dev::k_intersect<<<g_int, 128, 0, st>>>(a, (int)depth);
       }
       {
-        ProfScope ps(ctx, KC_SHADE);
-        if (classes & (1u << CLS_TERMINAL)) dev::k_shade<CLS_TERMINAL><<<g_sh, 128, 0, ctx->stream>>>(a, (int)depth);
-        if (classes & (1u << CLS_METAL)) dev::k_shade<CLS_METAL><<<g_sh, 128, 0, ctx->stream>>>(a, (int)depth);
-        if (classes & (1u << CLS_COATED)) dev::k_shade<CLS_COATED><<<g_sh, 128, 0, ctx->stream>>>(a, (int)depth);
-        if (classes & (1u << CLS_DIELECTRIC))
-          dev::k_shade<CLS_DIELECTRIC><<<g_sh, 128, 0, ctx->stream>>>(a, (int)depth);
-        if (classes & (1u << CLS_OTHER)) dev::k_shade<CLS_OTHER><<<g_sh, 128, 0, ctx->stream>>>(a, (int)depth);
+        ProfScope ps(ctx, KC_SHADE, st);
+        if (classes & (1u << CLS_TERMINAL)) dev::k_shade<CLS_TERMINAL><<<g_sh, 128, 0, st>>>(a, (int)depth);
+        if (classes & (1u << CLS_METAL)) dev::k_shade<CLS_METAL><<<g_sh, 128, 0, st>>>(a, (int)depth);
+        if (classes & (1u << CLS_COATED)) dev::k_shade<CLS_COATED><<<g_sh, 128, 0, st>>>(a, (int)depth);
+        if (classes & (1u << CLS_DIELECTRIC)) dev::k_shade<CLS_DIELECTRIC><<<g_sh, 128, 0, st>>>(a, (int)depth);
+        if (classes & (1u << CLS_OTHER)) dev::k_shade<CLS_OTHER><<<g_sh, 128, 0, st>>>(a, (int)depth);
         ctx->launches += __builtin_popcount(classes) - 1;
       }
       {
-        ProfScope ps(ctx, KC_SHADOW);
-        dev::k_shadow<<<g_any, 128, 0, ctx->stream>>>(a, (int)depth);
+        ProfScope ps(ctx, KC_SHADOW, st);
+        dev::k_shadow<<<g_any, 128, 0, st>>>(a, (int)depth);
       }
       ctx->launches += 3;
     }
+    // Films accumulate in wave order: wait for the previous wave's film pass.
+    if (wi > 0 && lanes > 1) ARGENT_CK(ctx, cudaStreamWaitEvent(st, ctx->film_ev[(lane + lanes - 1) % lanes], 0));
     {
-      ProfScope ps(ctx, KC_FILM);
-      dev::k_film<<<g_film, 256, 0, ctx->stream>>>(a, w);
+      ProfScope ps(ctx, KC_FILM, st);
+      dev::k_film<<<g_film, 256, 0, st>>>(a, w);
     }
+    ARGENT_CK(ctx, cudaEventRecord(ctx->film_ev[lane], st));
     ctx->launches++;
+  }
+  for (int l = 1; l < lanes; ++l) {
+    ARGENT_CK(ctx, cudaEventRecord(ctx->join_ev, ctx->lane_stream[l]));
+    ARGENT_CK(ctx, cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0));
   }
   cudaError_t e = cudaGetLastError();
   cudaFreeAsync(d_jobs, ctx->stream);
@@ -991,9 +1030,26 @@ int argent_ctx_set_counting(ArgentCtx* ctx, int on) {
   ARGENT_CK(ctx, cudaSetDevice(ctx->device));
   ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
   int v = on ? 1 : 0;
-  unsigned long long z[6] = {0, 0, 0, 0, 0, 0};
+  unsigned long long z[16] = {};
+  unsigned int zm[2] = {0, 0};
   ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_trav_counting, &v, sizeof(v)));
-  ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_trav_counts, z, sizeof(z)));
+  ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_trav_counts, z, 6 * sizeof(unsigned long long)));
+  ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_trav_hist, z, sizeof(z)));
+  ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_trav_max, zm, sizeof(zm)));
+  return ARGENT_OK;
+}
+
+int argent_ctx_traversal_histogram(ArgentCtx* ctx, uint64_t* out18) {
+  if (!ctx || !out18) return set_error(ctx, ARGENT_E_INVALID, "NULL argument");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  unsigned long long h[16];
+  unsigned int m[2];
+  ARGENT_CK(ctx, cudaMemcpyFromSymbol(h, dev::d_trav_hist, sizeof(h)));
+  ARGENT_CK(ctx, cudaMemcpyFromSymbol(m, dev::d_trav_max, sizeof(m)));
+  for (int i = 0; i < 16; ++i) out18[i] = h[i];
+  out18[16] = m[0];
+  out18[17] = m[1];
   return ARGENT_OK;
 }
 

@@ -20,5 +20,9 @@ __device__ float d_cmf[471 * 3];
 // rays, nodes, triangles; any-hit rays, nodes, triangles.
 __device__ int d_trav_counting;
 __device__ unsigned long long d_trav_counts[6];
+// Rays by node visits (bins 0, 1, 2-3, 4-7, 8-15, 16-63, 64-255, 256+),
+// closest-hit then any-hit, and the largest visit count of each kind.
+__device__ unsigned long long d_trav_hist[16];
+__device__ unsigned int d_trav_max[2];
 
 }  // namespace dev

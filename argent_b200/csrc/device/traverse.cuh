@@ -4,14 +4,16 @@
 //
 // Exactness.  The triangle test is argent's Moller-Trumbore in argent's
 // operation order (bvh.rs:391-410), rounded exactly like the f32 Rust code
-// (the library is compiled with --fmad=false; the box decode uses explicit
-// round-to-nearest intrinsics).  Child boxes are quantised conservatively
-// (decoded lo <= true lo, decoded hi >= true hi), and the slab test keeps
-// argent's arithmetic ((plane - o) * inv, SSE min/max), so every box argent's
-// traversal enters is entered here too.  The closest hit is the minimum of
-// (t, original triangle index) over all triangles that pass the test, which
-// does not depend on the tree.  argent instead keeps the first of equal-t
-// hits in its own traversal order; the parity tests bucket such exact ties.
+// (the library is compiled with --fmad=false).  The closest hit is the
+// minimum of (t, original triangle index) over all triangles that pass the
+// test, which does not depend on the tree; argent instead keeps the first of
+// equal-t hits in its own traversal order, and the parity tests bucket such
+// exact ties.  The tree only decides which triangles are tested, so box
+// culling must be conservative: child boxes are quantised outward (decoded
+// lo <= true lo, decoded hi >= true hi), and the slab interval is widened by
+// a bound on its own rounding error (node_ray), so a box whose exact
+// interval holds a hit distance is entered whenever argent's slab test
+// (bvh.rs:280-299), whose rounding is within that bound, would enter it.
 #pragma once
 #include "dev_math.cuh"
 #include "tables.cuh"
@@ -91,13 +93,6 @@ __device__ __forceinline__ NodeView load_node(const uint4* nodes, uint32_t idx) 
   return n;
 }
 
-__device__ __forceinline__ uint32_t qbyte(uint32_t w0, uint32_t w1, int c) {
-  return ((c < 4 ? w0 : w1) >> (8 * (c & 3))) & 0xffu;
-}
-__device__ __forceinline__ float decode(float origin, uint32_t q, float scale) {
-  return __fadd_rn(origin, __fmul_rn((float)q, scale));
-}
-
 // Reference to a child: an interior node index, or a leaf
 // (LEAF_BIT | (count-1) << 27 | first triangle).
 __device__ __forceinline__ uint32_t child_ref(const NodeView& n, int c) {
@@ -111,23 +106,93 @@ __device__ __forceinline__ uint32_t child_ref(const NodeView& n, int c) {
   return ARGENT_LEAF_BIT | (cnt1 << 27) | (n.tri_base + off);
 }
 
-// Slab test of child c, bvh.rs:280-299 (SSE min/max).  Returns tmin or -1
-// (as "no hit") in *hit.
-__device__ __forceinline__ bool slab_child(const NodeView& n, int c, V3 o, V3 inv, float t_max, float* tmin_out) {
-  float lx = decode(n.ox, qbyte(n.qlx0, n.qlx1, c), n.sx);
-  float hx = decode(n.ox, qbyte(n.qhx0, n.qhx1, c), n.sx);
-  float ly = decode(n.oy, qbyte(n.qly0, n.qly1, c), n.sy);
-  float hy = decode(n.oy, qbyte(n.qhy0, n.qhy1, c), n.sy);
-  float lz = decode(n.oz, qbyte(n.qlz0, n.qlz1, c), n.sz);
-  float hz = decode(n.oz, qbyte(n.qhz0, n.qhz1, c), n.sz);
-  float tx0 = __fmul_rn(__fsub_rn(lx, o.x), inv.x);
-  float tx1 = __fmul_rn(__fsub_rn(hx, o.x), inv.x);
-  float ty0 = __fmul_rn(__fsub_rn(ly, o.y), inv.y);
-  float ty1 = __fmul_rn(__fsub_rn(hy, o.y), inv.y);
-  float tz0 = __fmul_rn(__fsub_rn(lz, o.z), inv.z);
-  float tz1 = __fmul_rn(__fsub_rn(hz, o.z), inv.z);
-  float tmin = sse_max(sse_max(sse_max(sse_min(tx0, tx1), sse_min(ty0, ty1)), sse_min(tz0, tz1)), 0.0f);
-  float tmax = sse_min(sse_min(sse_min(sse_max(tx0, tx1), sse_max(ty0, ty1)), sse_max(tz0, tz1)), t_max);
+// Byte c of the packed plane words (w0: children 0-3, w1: 4-7) as an exact
+// float, without an integer-to-float conversion (those issue on the narrow
+// XU pipe): the byte is placed in the mantissa of 2^23, and 2^23 is
+// subtracted exactly.
+__device__ __forceinline__ float qf(uint32_t w0, uint32_t w1, int c) {
+  return __fadd_rn(__uint_as_float(__byte_perm(c < 4 ? w0 : w1, 0x4B000000u, 0x7440u | (uint32_t)(c & 3))),
+                   -8388608.0f);
+}
+
+// A ray prepared for the node-space slab test: the inverse direction with
+// magnitudes capped at 2^64 (a zero component gives +-2^64, so no 0 * inf
+// arises), and per axis whether the ray runs toward -axis.
+struct RayQ {
+  V3 o;
+  float ix, iy, iz;
+  bool nx, ny, nz;
+};
+
+__device__ __forceinline__ float capped_inv(float d) {
+  const float cap = 18446744073709551616.0f;  // 2^64
+  return fminf(fmaxf(__fdiv_rn(1.0f, d), -cap), cap);
+}
+
+__device__ __forceinline__ RayQ make_rayq(V3 o, V3 d) {
+  RayQ r;
+  r.o = o;
+  r.ix = capped_inv(d.x);
+  r.iy = capped_inv(d.y);
+  r.iz = capped_inv(d.z);
+  r.nx = signbit(r.ix);
+  r.ny = signbit(r.iy);
+  r.nz = signbit(r.iz);
+  return r;
+}
+
+// One axis of a node seen from a ray.  A plane q of the axis is at
+// t = (origin + q * scale - o) * inv = q * a + b, with a = scale * inv
+// (exact: scale is a power of two) and b = (origin - o) * inv.  Computed as
+// fma(q, a, b), t differs from the exact value by at most about
+// 3 * 2^-24 * (|origin - o| + 255 * scale) * |inv|; the slack e is 2^-18
+// times that magnitude (64 units of rounding), and is subtracted from the
+// near plane's bias and added to the far plane's.  The near plane is the
+// low one unless the ray runs toward -axis.
+struct AxisQ {
+  float a, bn, bf;
+  uint32_t n0, n1, f0, f1;
+};
+
+__device__ __forceinline__ AxisQ axis_q(float origin, float scale, float o, float inv, bool neg, uint32_t lo0,
+                                        uint32_t lo1, uint32_t hi0, uint32_t hi1) {
+  AxisQ q;
+  float dd = __fsub_rn(origin, o);
+  float b = __fmul_rn(dd, inv);
+  float e = __fmul_rn(__fmul_rn(__fadd_rn(fabsf(dd), __fmul_rn(256.0f, scale)), fabsf(inv)), 3.814697265625e-06f);
+  q.a = __fmul_rn(scale, inv);
+  q.bn = __fsub_rn(b, e);
+  q.bf = __fadd_rn(b, e);
+  q.n0 = neg ? hi0 : lo0;
+  q.n1 = neg ? hi1 : lo1;
+  q.f0 = neg ? lo0 : hi0;
+  q.f1 = neg ? lo1 : hi1;
+  return q;
+}
+
+struct NodeQ {
+  AxisQ x, y, z;
+};
+
+__device__ __forceinline__ NodeQ node_ray(const NodeView& n, const RayQ& r) {
+  NodeQ q;
+  q.x = axis_q(n.ox, n.sx, r.o.x, r.ix, r.nx, n.qlx0, n.qlx1, n.qhx0, n.qhx1);
+  q.y = axis_q(n.oy, n.sy, r.o.y, r.iy, r.ny, n.qly0, n.qly1, n.qhy0, n.qhy1);
+  q.z = axis_q(n.oz, n.sz, r.o.z, r.iz, r.nz, n.qlz0, n.qlz1, n.qhz0, n.qhz1);
+  return q;
+}
+
+// Widened slab interval of child c, clipped to [0, t_max]; true when it is
+// not empty.  *tmin_out = its entry distance.
+__device__ __forceinline__ bool child_q(const NodeQ& q, int c, float t_max, float* tmin_out) {
+  float tnx = __fmaf_rn(qf(q.x.n0, q.x.n1, c), q.x.a, q.x.bn);
+  float tny = __fmaf_rn(qf(q.y.n0, q.y.n1, c), q.y.a, q.y.bn);
+  float tnz = __fmaf_rn(qf(q.z.n0, q.z.n1, c), q.z.a, q.z.bn);
+  float tfx = __fmaf_rn(qf(q.x.f0, q.x.f1, c), q.x.a, q.x.bf);
+  float tfy = __fmaf_rn(qf(q.y.f0, q.y.f1, c), q.y.a, q.y.bf);
+  float tfz = __fmaf_rn(qf(q.z.f0, q.z.f1, c), q.z.a, q.z.bf);
+  float tmin = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
+  float tmax = fminf(fminf(tfx, tfy), fminf(tfz, t_max));
   *tmin_out = tmin;
   return tmin <= tmax;
 }
@@ -143,6 +208,11 @@ __device__ __forceinline__ void count_visits(int base, uint32_t nodes, uint32_t 
     atomicAdd(&d_trav_counts[base], 1ull);
     atomicAdd(&d_trav_counts[base + 1], (unsigned long long)nodes);
     atomicAdd(&d_trav_counts[base + 2], (unsigned long long)tris);
+    int kind = base / 3;
+    int bin = nodes == 0 ? 0 : nodes < 2 ? 1 : nodes < 4 ? 2 : nodes < 8 ? 3 : nodes < 16 ? 4 : nodes < 64 ? 5
+              : nodes < 256 ? 6 : 7;
+    atomicAdd(&d_trav_hist[8 * kind + bin], 1ull);
+    atomicMax(&d_trav_max[kind], nodes);
   }
 }
 
@@ -178,7 +248,7 @@ __device__ __forceinline__ void sort8(uint32_t k[8]) {
 __device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, float t_max, uint32_t* status) {
   TraceHit best{t_max, 0.0f, 0.0f, ARGENT_NO_HIT_U};
   if (pc.num_tris == 0) return best;
-  V3 inv{__fdiv_rn(1.0f, d.x), __fdiv_rn(1.0f, d.y), __fdiv_rn(1.0f, d.z)};
+  RayQ rq = make_rayq(o, d);
   uint2 stack[ARGENT_STACK_SIZE];
   int sp = 0;
   uint32_t n_nodes = 0, n_tris = 0;
@@ -214,16 +284,15 @@ __device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, f
     }
     NodeView n = load_node(pc.nodes, ref);
     ++n_nodes;
+    NodeQ nq = node_ray(n, rq);
     uint32_t k[8];
     int nh = 0;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-      k[c] = 0xFFFFFFFFu;
       float tc;
-      if (((n.present >> c) & 1u) && slab_child(n, c, o, inv, best.t, &tc)) {
-        k[c] = (__float_as_uint(tc) & ~7u) | (uint32_t)c;
-        ++nh;
-      }
+      bool h = child_q(nq, c, best.t, &tc) && ((n.present >> c) & 1u);
+      k[c] = h ? ((__float_as_uint(tc) & ~7u) | (uint32_t)c) : 0xFFFFFFFFu;
+      nh += h ? 1 : 0;
     }
     if (nh == 0) continue;
     if (sp + nh - 1 > ARGENT_STACK_SIZE) {
@@ -245,7 +314,7 @@ __device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, f
 // Any hit with t in (1e-7, t_max), bvh.rs:216-247.
 __device__ __noinline__ bool trace_any(const DevPiece& pc, V3 o, V3 d, float t_max, uint32_t* status) {
   if (pc.num_tris == 0) return false;
-  V3 inv{__fdiv_rn(1.0f, d.x), __fdiv_rn(1.0f, d.y), __fdiv_rn(1.0f, d.z)};
+  RayQ rq = make_rayq(o, d);
   uint32_t stack[ARGENT_STACK_SIZE];
   int sp = 0;
   uint32_t n_nodes = 0, n_tris = 0;
@@ -268,14 +337,14 @@ __device__ __noinline__ bool trace_any(const DevPiece& pc, V3 o, V3 d, float t_m
     }
     NodeView n = load_node(pc.nodes, ref);
     ++n_nodes;
+    NodeQ nq = node_ray(n, rq);
     uint32_t hitmask = 0;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
       float tmin;
-      if ((n.present >> c) & 1u) {
-        if (slab_child(n, c, o, inv, t_max, &tmin)) hitmask |= 1u << c;
-      }
+      if (child_q(nq, c, t_max, &tmin)) hitmask |= 1u << c;
     }
+    hitmask &= n.present;
     if (sp + __popc(hitmask) > ARGENT_STACK_SIZE) {
       atomicOr(status, ARGENT_STATUS_STACK_OVERFLOW);
       return false;

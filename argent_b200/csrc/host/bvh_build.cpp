@@ -275,6 +275,9 @@ struct Collapser {
         ee = ex;
       }
       ee = std::max(ee, -120);
+      // The device slab test multiplies scale by 1/d (capped at 2^64);
+      // scale <= 2^60 keeps that product finite.
+      if (ee > 60) throw std::runtime_error("piece extent too large for the node quantisation");
       for (;;) {
         uint8_t eb = (uint8_t)(ee + 127);
         uint8_t qh;

@@ -127,16 +127,24 @@ struct KernelProfile {
   uint64_t n[KC_COUNT] = {0, 0, 0, 0, 0, 0};
 };
 
+// Waves alternate between two lanes, each with its own stream and path
+// state, so that one wave's kernels fill the SMs that the other wave's
+// kernel tails leave idle.  Lane 0 runs on the context stream.
+#define ARGENT_LANES 2
+
 struct ArgentCtx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t lane_stream[ARGENT_LANES] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  cudaEvent_t film_ev[ARGENT_LANES] = {};
   int num_sms = 148;
   ArgentLimits limits{};
   std::string err;
   uint64_t launches = 0;
   uint32_t* d_status = nullptr;
   bool tables_ready = false;
-  WaveBuffers wave;
+  WaveBuffers wave[ARGENT_LANES];
   KernelProfile prof;
 };
 

@@ -227,11 +227,28 @@ struct WaveArgs {
 };
 
 // Queue counters of one wave: active paths per bounce, shade-queue lengths
-// per bounce and class, shadow rays per bounce.
+// per bounce and class, shadow rays per bounce.  Each queue also has a work
+// counter (CNT_WORK) from which the kernel that drains it takes batches.
 #define CNT_ACT(d) (d)
 #define CNT_CLS(d, c) ((ARGENT_MAX_DEPTH + 2) + (d) * NUM_CLS + (c))
 #define CNT_SH(d) ((ARGENT_MAX_DEPTH + 2) * (1 + NUM_CLS) + (d))
-#define CNT_TOTAL ((ARGENT_MAX_DEPTH + 2) * (2 + NUM_CLS))
+#define CNT_QUEUES ((ARGENT_MAX_DEPTH + 2) * (2 + NUM_CLS))
+#define CNT_WORK(q) (CNT_QUEUES + (q))
+#define CNT_TOTAL (2 * CNT_QUEUES)
+
+// Dynamic work distribution over a queue: a warp takes 32 consecutive
+// entries at a time.  Its first batch is fixed by its index in the grid; the
+// later ones come from the queue's work counter (zeroed with the queue
+// counters), so warps whose rays finish early take more batches.  The loop
+// condition is warp-uniform, as the ballots in the loop bodies require.
+__device__ __forceinline__ uint32_t warp_first_batch() {
+  return (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32u;
+}
+__device__ __forceinline__ uint32_t warp_next_batch(uint32_t* work) {
+  uint32_t b = 0;
+  if ((threadIdx.x & 31) == 0) b = atomicAdd(work, 32u);
+  return __shfl_sync(0xffffffffu, b, 0) + gridDim.x * blockDim.x;
+}
 
 __device__ __forceinline__ const DevSegment& find_segment(const WaveDesc& w, uint32_t slot) {
   uint32_t s = 0;
@@ -325,8 +342,9 @@ __device__ __forceinline__ void warp_append(bool pred, uint32_t value, uint32_t*
 // queued for the shading kernel of its hit's material class.
 __global__ void __launch_bounds__(128) k_intersect(WaveArgs a, int depth) {
   uint32_t count = a.counters[CNT_ACT(depth)];
-  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
-    uint32_t i = base + threadIdx.x;
+  uint32_t* work = a.counters + CNT_WORK(CNT_ACT(depth));
+  for (uint32_t base = warp_first_batch(); base < count; base = warp_next_batch(work)) {
+    uint32_t i = base + (threadIdx.x & 31);
     int cls = -1;
     uint32_t slot = 0;
     if (i < count) {
@@ -699,8 +717,9 @@ __global__ void __launch_bounds__(128, CLS == CLS_TERMINAL ? 1 : 4) k_shade(Wave
   uint32_t cap = a.cap;
   uint32_t* next_counter = a.counters + CNT_ACT(depth + 1);
   uint32_t* shadow_counter = a.counters + CNT_SH(depth);
-  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += gridDim.x * blockDim.x) {
-    uint32_t i = base + threadIdx.x;
+  uint32_t* work = a.counters + CNT_WORK(CNT_CLS(depth, CLS));
+  for (uint32_t base = warp_first_batch(); base < count; base = warp_next_batch(work)) {
+    uint32_t i = base + (threadIdx.x & 31);
     ShadeOut r;
     r.alive = false;
     r.shadow = false;
@@ -734,16 +753,20 @@ __global__ void __launch_bounds__(128, CLS == CLS_TERMINAL ? 1 : 4) k_shade(Wave
 
 __global__ void __launch_bounds__(128) k_shadow(WaveArgs a, int depth) {
   uint32_t count = a.counters[CNT_SH(depth)];
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-    float4 so = a.sh_o[i], sd = a.sh_d[i];
-    uint32_t slot = __float_as_uint(sd.w);
-    uint32_t job_id = a.meta[slot].w >> 16;
-    const DevScene* sc = a.jobs[job_id].scene;
-    bool occ = trace_any(sc->piece, V3{so.x, so.y, so.z}, V3{sd.x, sd.y, sd.z}, so.w, a.status);
-    if (!occ) {
-      float4 c = a.sh_c[i];
-      float4 l = a.L[slot];
-      a.L[slot] = make_float4(l.x + c.x, l.y + c.y, l.z + c.z, l.w + c.w);
+  uint32_t* work = a.counters + CNT_WORK(CNT_SH(depth));
+  for (uint32_t base = warp_first_batch(); base < count; base = warp_next_batch(work)) {
+    uint32_t i = base + (threadIdx.x & 31);
+    if (i < count) {
+      float4 so = a.sh_o[i], sd = a.sh_d[i];
+      uint32_t slot = __float_as_uint(sd.w);
+      uint32_t job_id = a.meta[slot].w >> 16;
+      const DevScene* sc = a.jobs[job_id].scene;
+      bool occ = trace_any(sc->piece, V3{so.x, so.y, so.z}, V3{sd.x, sd.y, sd.z}, so.w, a.status);
+      if (!occ) {
+        float4 c = a.sh_c[i];
+        float4 l = a.L[slot];
+        a.L[slot] = make_float4(l.x + c.x, l.y + c.y, l.z + c.z, l.w + c.w);
+      }
     }
   }
 }

@@ -69,6 +69,14 @@ class Context:
         k = ["closest_rays", "closest_nodes", "closest_tris", "any_rays", "any_nodes", "any_tris"]
         return dict(zip(k, [int(x) for x in out]))
 
+    def traversal_histogram(self):
+        """Rays by node visits (bins 0, 1, 2-3, 4-7, 8-15, 16-63, 64-255,
+        256+) and the largest visit count, per ray kind."""
+        out = (ctypes.c_uint64 * 18)()
+        self.check(self.lib.argent_ctx_traversal_histogram(self.h, out))
+        v = [int(x) for x in out]
+        return {"closest": v[0:8], "any": v[8:16], "closest_max": v[16], "any_max": v[17]}
+
 
 class Piece:
     """`Piece::new`: mesh upload + acceleration structure build."""
@@ -202,3 +210,80 @@ def render_batch(ctx: Context, items):
         arr[i].count = int(count)
         arr[i].seed = int(seed)
     ctx.check(ctx.lib.argent_render_batch(ctx.h, arr, len(items)))
+
+
+class Serve:
+    """Continuous batching of render requests (argent_serve_*): the GPU
+    counterpart of serve's job queue (argent/src/serve/queue.rs:599-617).
+    submit/poll/cancel may come from any thread; step and read belong to
+    the thread that owns the context."""
+
+    def __init__(self, ctx: Context, film_budget=0, max_active=0, step_path_samples=0):
+        self.ctx = ctx
+        cfg = N.ArgentServeConfig(int(film_budget), int(max_active), 0, int(step_path_samples))
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.argent_serve_create(ctx.h, ctypes.byref(cfg), ctypes.byref(h)))
+        self.h = h
+        self._scenes = {}  # ticket -> scene, kept alive while the request is
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.argent_serve_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, scene: Scene, cam, settings, width, height, spp, seed=7, priority=0, flags=N.FILM_KAHAN):
+        r = N.ArgentServeRequest()
+        r.scene = scene.h
+        r.camera = cam
+        r.settings = settings
+        r.width, r.height, r.spp, r.seed = int(width), int(height), int(spp), int(seed)
+        r.film_flags = int(flags)
+        r.priority = int(priority)
+        t = ctypes.c_uint64()
+        self.ctx.check(self.ctx.lib.argent_serve_submit(self.h, ctypes.byref(r), ctypes.byref(t)))
+        self._scenes[t.value] = (scene, width, height)
+        return t.value
+
+    def poll(self, ticket):
+        st = N.ArgentServeStatus()
+        self.ctx.check(self.ctx.lib.argent_serve_poll(self.h, ticket, ctypes.byref(st)))
+        return st
+
+    def cancel(self, ticket):
+        self.ctx.check(self.ctx.lib.argent_serve_cancel(self.h, ticket))
+
+    def step(self):
+        """One scheduling round; returns the number of requests pending."""
+        n = ctypes.c_uint32()
+        self.ctx.check(self.ctx.lib.argent_serve_step(self.h, ctypes.byref(n)))
+        return int(n.value)
+
+    def run(self):
+        """Steps until nothing is queued or active."""
+        while self.step():
+            pass
+
+    def read(self, ticket):
+        """(color, albedo, normal) of a finished request; forgets it."""
+        _, w, h = self._scenes[ticket]
+        shape = (h, w, 3)
+        c, a, n = np.zeros(shape, np.float32), np.zeros(shape, np.float32), np.zeros(shape, np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self.ctx.check(self.ctx.lib.argent_serve_read(self.h, ticket, _p(c, fp), _p(a, fp), _p(n, fp)))
+        del self._scenes[ticket]
+        return c, a, n
+
+    def release(self, ticket):
+        self.ctx.check(self.ctx.lib.argent_serve_release(self.h, ticket))
+        self._scenes.pop(ticket, None)
+
+    def stats(self):
+        s, p, b = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self.ctx.check(self.ctx.lib.argent_serve_stats(self.h, ctypes.byref(s), ctypes.byref(p), ctypes.byref(b)))
+        return {"steps": s.value, "path_samples": p.value, "film_bytes_in_use": b.value}
+
+    def now(self):
+        return float(self.ctx.lib.argent_serve_now(self.h))

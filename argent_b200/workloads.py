@@ -17,6 +17,9 @@ Workloads (seeded, procedural; no argent assets are needed):
   reel_batch     4 alloys x 36 turntable frames x 3 pieces (61k, 1.1M, 3.0M
                  triangles), 1080 x 1920, 64 spp, depth 12, noir panels plus
                  a 2048 x 1024 synthetic HDRI (env_pick 0.5), render seed 11
+  serve_trace    Poisson arrivals (seed 6) over 8 resident pieces (40k..3.0M
+                 triangles) x 7 alloys: 70 % previews 512^2 x 4 spp, 25 %
+                 listings 2000^2 x 128, 5 % finals 1080 x 1920 x 512
 """
 
 import ctypes
@@ -358,3 +361,45 @@ def reel_batch(pieces=None, alloys=REEL_ALLOYS, frames=range(REEL_FRAMES), width
                 out.append(Workload(f"reel_{label}_{alloy}_f{i:02d}_{width}x{height}_{spp}spp", m, desc, cam, width,
                                     height, spp, settings(12), 11, {"piece": label, "alloy": alloy, "frame": i}))
     return out
+
+
+# ---------------------------------------------------------------- served requests
+
+SERVE_ALLOYS = ("sterling", "gold14k", "gold18k", "rose14k", "white14k", "platinum", "bronze")
+# (nu, nv) of the signet generator: 2 * nu * nv triangles, 40k .. 3.0M
+SERVE_PIECES = ((200, 100), (250, 200), (500, 250), (500, 500), (1000, 500), (1000, 750), (2048, 512), (2048, 732))
+# class: (share, width, height, spp, priority)
+SERVE_CLASSES = {"preview": (0.70, 512, 512, 4, 0), "listing": (0.25, 2000, 2000, 128, 1),
+                 "final": (0.05, 1080, 1920, 512, 2)}
+
+
+def serve_pieces():
+    """The served workload's eight resident pieces."""
+    return [M.signet(nu=nu, nv=nv) for nu, nv in SERVE_PIECES]
+
+
+def serve_trace(rate, seconds, seed=6):
+    """Poisson arrivals at `rate` requests/s for `seconds`: a list of
+    (arrival_s, class, piece index, alloy index), drawn from one seeded
+    generator in that order per request."""
+    rng = np.random.default_rng(seed)
+    names = list(SERVE_CLASSES)
+    shares = np.array([SERVE_CLASSES[n][0] for n in names])
+    out, t = [], 0.0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t >= seconds:
+            break
+        c = names[int(rng.choice(len(names), p=shares))]
+        out.append((t, c, int(rng.integers(len(SERVE_PIECES))), int(rng.integers(len(SERVE_ALLOYS)))))
+    return out
+
+
+def serve_scene(m, alloy, turn):
+    """A served look: polished and satin slots of the alloy, noir studio,
+    the piece turned for the hero view."""
+    return _studio_scene(m, [metal(alloy, 0.05, 0.8), metal(alloy, 0.35, 0.8)], "noir", turn)
+
+
+def mean_request_path_samples():
+    return sum(sh * w * h * spp for sh, w, h, spp, _ in SERVE_CLASSES.values())

@@ -170,11 +170,12 @@ def cpu_sample(wl, seconds=12.0, threads=0, rows=None):
     return wl.width * rows * wl.spp / dt, rows, nthr, sc
 
 
-WORKLOADS = ("signet_still", "ring_still", "gems_still", "reel_batch")
+WORKLOADS = ("signet_still", "ring_still", "gems_still", "reel_batch", "serve_trace")
 DATA = {"signet_still": "seeded procedural signet, noir studio",
         "ring_still": "seeded procedural ring, noir studio",
         "gems_still": "seeded procedural 18k setting with a brilliant and 36 side stones, white studio",
-        "reel_batch": "seeded procedural signets of 61k/1.1M/3.0M triangles, seeded synthetic HDRI"}
+        "reel_batch": "seeded procedural signets of 61k/1.1M/3.0M triangles, seeded synthetic HDRI",
+        "serve_trace": "seeded procedural signets of 40k..3.0M triangles, Poisson arrivals seed 6"}
 
 
 def build_mesh(name):
@@ -211,10 +212,21 @@ def reference_wls(name):
     """The renders the reference arm samples: the still itself, or for the
     batched workload one render per piece (14k gold), whose turntable frame
     follows the step index."""
+    from argent_b200 import workloads as W
+
+    if name == "serve_trace":
+        # one render of each request class on the 1.0M-triangle piece, gold14k
+        nu, nv = W.SERVE_PIECES[4]
+        m = W.M.signet(nu=nu, nv=nv)
+        out = []
+        for cname, (_, w, h, spp, _) in W.SERVE_CLASSES.items():
+            cam, turn = W.shot(None, W.hull(m), "hero", 100.0, 0.0, w / h)
+            out.append(W.Workload(f"serve_{cname}_{w}x{h}_{spp}spp", m, W.serve_scene(m, "gold14k", turn), cam, w, h,
+                                  spp, W.settings(12), 7))
+        return out
     if name != "reel_batch":
         m = build_mesh(name)
         return [build_workload(name, m, OracleTracer(m))]
-    from argent_b200 import workloads as W
 
     pieces = {label: W.reel_piece(label) for label, _, _ in W.REEL_PIECES}
     return W.reel_batch(pieces, alloys=("gold14k",), frames=[0])
@@ -258,11 +270,15 @@ def run_reference(args, world, rank):
     value = per * len(times) / sum(times)
     wl = wls[0]
     what = (f"{len(wls)} renders (one per piece, 14k gold, turntable frame = step)" if reel else "the frame")
+    if args.workload == "serve_trace":
+        what = f"{len(wls)} renders (one per request class, 1.0M-triangle piece, 14k gold)"
     sample = (f"rows {wl.height // 2}..{wl.height // 2 + rows} of {what}, {wl.width} wide at {wl.spp} spp "
               f"({per} path-samples per step)")
     cfg = {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp,
            "triangles": int(wl.mesh.num_tris), "max_depth": int(wl.settings.max_depth),
            "parallelism": "cpu-threads"}
+    if args.workload == "serve_trace":
+        cfg["workload"] = f"serve_trace_{args.serve_rate:g}rps_{args.serve_seconds:g}s"
     if reel:
         cfg["workload"] = (f"reel_batch_{len(W.REEL_PIECES) * len(W.REEL_ALLOYS)}x{W.REEL_FRAMES}frames_"
                            f"{wl.width}x{wl.height}_{wl.spp}spp")
@@ -410,6 +426,7 @@ def run_gpu(args, world, rank, device):
     ctx.set_counting(True)
     run_plan(ctx, plan, 0, cfilms, 1)
     counts = ctx.traversal_counts()
+    hist = ctx.traversal_histogram()
     ctx.set_counting(False)
     for f in cfilms:
         f.close()
@@ -515,7 +532,118 @@ def run_gpu(args, world, rank, device):
                          "launches": dom_n, "avg_launch_ms": dom_ms / max(dom_n, 1)},
             "kernel_ms": {k: round(v[0], 3) for k, v in kt.items()},
             "traversal_per_path_sample": {k: v / px for k, v in counts.items()},
+            "traversal_nodes_per_ray_histogram": hist,
             "cpu_baseline": cpu,
+        }
+        print(json.dumps(out), flush=True)
+
+
+def run_serve(args, world, rank, device):
+    """Served requests: a thread submits the Poisson trace on the wall
+    clock while this thread steps the scheduler and reads finished films to
+    host memory.  value = path-samples served / (last completion - first
+    arrival); latency = completion - submission per request class."""
+    import torch
+
+    from argent_b200 import workloads as W
+    from argent_b200.gpu import Context, Piece, Scene, Serve
+
+    torch.cuda.set_device(device)
+    ctx = Context(device)
+    meshes = W.serve_pieces()
+    pieces = [Piece(ctx, m) for m in meshes]
+    cams, scenes = {}, {}
+    for i, m in enumerate(meshes):
+        pts = W.hull(m)
+        for cname, (_, w, h, _, _) in W.SERVE_CLASSES.items():
+            cams[(i, cname)], turn = W.shot(None, pts, "hero", 100.0, 0.0, w / h)
+        for j, alloy in enumerate(W.SERVE_ALLOYS):
+            scenes[(i, j)] = Scene(ctx, pieces[i], W.serve_scene(m, alloy, turn))
+    ps = W.settings(12)
+    rate = args.serve_rate
+    trace = W.serve_trace(rate, args.serve_seconds)
+    srv = Serve(ctx, film_budget=32 << 30, max_active=64, step_path_samples=1 << 24)
+
+    def submit(cname, i, j):
+        _, w, h, spp, prio = W.SERVE_CLASSES[cname]
+        return srv.submit(scenes[(i, j)], cams[(i, cname)], ps, w, h, spp, 7, prio)
+
+    # Warm-up: previews rendered to completion before the trace.
+    for k in range(args.warmup):
+        t = submit("preview", k % len(meshes), k % len(W.SERVE_ALLOYS))
+        srv.run()
+        srv.read(t)
+
+    launches0 = ctx.kernel_launches
+    steps0 = srv.stats()
+    tickets = {}
+    done = threading.Event()
+    t_origin = srv.now()
+
+    def driver():
+        for (ta, cname, i, j) in trace:
+            dt = t_origin + ta - srv.now()
+            if dt > 0:
+                time.sleep(dt)
+            tickets[submit(cname, i, j)] = cname
+        done.set()
+
+    clocks = Clocks(smi_index(device))
+    clocks.start()
+    th = threading.Thread(target=driver)
+    th.start()
+    lat = {c: [] for c in W.SERVE_CLASSES}
+    finished = set()
+    d2h = 0
+    t_last = t_origin
+    while True:
+        pending = srv.step()
+        for t, cname in list(tickets.items()):
+            if t in finished:
+                continue
+            st = srv.poll(t)
+            if st.state == 2:  # done
+                lat[cname].append(st.t_done - st.t_submit)
+                t_last = max(t_last, st.t_done)
+                c, a, n = srv.read(t)
+                d2h += c.nbytes + a.nbytes + n.nbytes
+                finished.add(t)
+        if done.is_set() and pending == 0 and len(finished) == len(tickets):
+            break
+        if pending == 0:
+            time.sleep(0.001)
+    th.join()
+    ck = clocks.stop()
+    st = srv.stats()
+    served = st["path_samples"] - steps0["path_samples"]
+    wall = t_last - t_origin
+    value = served / wall
+    offered = rate * W.mean_request_path_samples()
+    launches = ctx.kernel_launches - launches0
+
+    def pct(v, q):
+        return float(np.percentile(v, q)) if v else None
+
+    if rank == 0:
+        out = {
+            "metric": "path-samples/s", "value": value, "unit": "path-samples/s", "n_gpus": world,
+            "steps": int(st["steps"] - steps0["steps"]), "warmup": args.warmup,
+            "ms_per_step": 1000.0 * wall / max(1, st["steps"] - steps0["steps"]),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": f"synthetic ({DATA['serve_trace']})",
+            "config": {"workload": f"serve_trace_{rate:g}rps_{args.serve_seconds:g}s", "requests": len(trace),
+                       "classes": {k: list(v[1:]) for k, v in W.SERVE_CLASSES.items()},
+                       "pieces_triangles": [int(m.num_tris) for m in meshes], "alloys": list(W.SERVE_ALLOYS),
+                       "offered_path_samples_per_s": offered, "step_path_samples": 1 << 24,
+                       "parallelism": f"replicas{world}",
+                       "timing": "wall clock of the serve loop (latency is a wall-clock quantity); each step "
+                                 "synchronises its batch"},
+            "latency_s": {c: {"n": len(v), "p50": pct(v, 50), "p99": pct(v, 99), "max": max(v) if v else None}
+                          for c, v in lat.items()},
+            "clocks": ck,
+            "e2e": {"value": value, "unit": "path-samples/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": d2h / max(1, len(finished)), "note": "per request: films read to host"},
+            "gpu_launches": int(launches),
         }
         print(json.dumps(out), flush=True)
 
@@ -535,6 +663,8 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--spp", type=int, default=0, help="override spp (short profiling runs)")
+    ap.add_argument("--serve-rate", type=float, default=1.0, help="serve_trace: requests per second")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="serve_trace: trace length")
     args = ap.parse_args()
     if args.impl == "reference":
         # CPU only: rank 0 measures, the other ranks have nothing to do.
@@ -545,6 +675,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload == "serve_trace":
+            run_serve(args, world, rank, local)
         else:
             run_gpu(args, world, rank, local)
     finally:

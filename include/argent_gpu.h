@@ -338,6 +338,89 @@ int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n
 uint64_t argent_ctx_kernel_launches(const ArgentCtx* ctx);
 
 /* ------------------------------------------------------------------ */
+/* Serving: continuous batching of render requests.                   */
+/* ------------------------------------------------------------------ */
+
+/*
+ * Replaces serve's job loop for stills (argent/src/serve/queue.rs:599-617:
+ * one job at a time, render_pass in chunks sized for ~1.5 s, seed 7, a
+ * cancel check between chunks) and its progressive live passes
+ * (serve/live.rs:747, 767).  Here all requests in flight advance together:
+ * each argent_serve_step is one argent_render_batch in which the active
+ * requests, lowest priority value first and then in submission order, take
+ * whole samples of their frame up to step_path_samples (the first at least
+ * one).  Chunks continue each film's sample indices, so a finished film
+ * holds what one argent_render_pass of `spp` samples with the same seed
+ * gives (up to the order of the FP32 sums).
+ *
+ * Admission: a queued request becomes active, in the same order, while
+ * fewer than max_active are active and its film fits in film_budget
+ * together with the films in use and pooled (pooled films of other sizes
+ * are freed first).  Films are pooled by (width, height, flags).
+ *
+ * Threads: submit, poll, cancel, release and stats may be called from any
+ * thread.  step and read use the context and must be called from the one
+ * thread that owns it.  A request's scene must outlive the request.
+ */
+typedef struct ArgentServe ArgentServe;
+
+typedef struct ArgentServeConfig {
+  uint64_t film_budget;       /* device bytes for films in use and pooled; 0 = 8 GiB */
+  uint32_t max_active;        /* requests rendered together; 0 = 64 */
+  uint32_t reserved;
+  uint64_t step_path_samples; /* path-samples per step; 0 = 2^24 */
+} ArgentServeConfig;
+
+typedef struct ArgentServeRequest {
+  ArgentScene* scene;
+  ArgentCamera camera;
+  ArgentPathSettings settings;
+  uint32_t width, height;
+  uint32_t spp;        /* samples per pixel in total */
+  uint32_t seed;       /* render seed (serve uses 7 for stills, queue.rs:613) */
+  uint32_t film_flags; /* ARGENT_FILM_*; 0 = Kahan */
+  int32_t priority;    /* lower values are served first */
+} ArgentServeRequest;
+
+enum {
+  ARGENT_REQ_QUEUED = 0,
+  ARGENT_REQ_ACTIVE = 1,
+  ARGENT_REQ_DONE = 2,
+  ARGENT_REQ_CANCELLED = 3,
+  ARGENT_REQ_FAILED = 4
+};
+
+typedef struct ArgentServeStatus {
+  int32_t state;    /* ARGENT_REQ_* */
+  uint32_t samples; /* samples accumulated so far */
+  uint32_t spp;
+  uint32_t reserved;
+  double t_submit, t_start, t_done; /* seconds on the serve's steady clock; -1 = not yet */
+} ArgentServeStatus;
+
+int argent_serve_create(ArgentCtx* ctx, const ArgentServeConfig* cfg, ArgentServe** out);
+/* Frees every film the serve holds; the context stays. */
+void argent_serve_destroy(ArgentServe* serve);
+/* Queues a request.  ARGENT_E_BUSY if its film alone exceeds film_budget. */
+int argent_serve_submit(ArgentServe* serve, const ArgentServeRequest* req, uint64_t* ticket);
+int argent_serve_poll(ArgentServe* serve, uint64_t ticket, ArgentServeStatus* status);
+/* Marks a queued or active request; it is cancelled at the next step. */
+int argent_serve_cancel(ArgentServe* serve, uint64_t ticket);
+/* One scheduling round: cancellations, admission, one batch (waits for it),
+ * completions.  *pending (may be NULL) = requests still queued or active.
+ * A failed batch marks its requests ARGENT_REQ_FAILED and returns the code. */
+int argent_serve_step(ArgentServe* serve, uint32_t* pending);
+/* Averages of a finished request's film (as argent_film_read; any pointer
+ * may be NULL), then forgets the request and pools its film. */
+int argent_serve_read(ArgentServe* serve, uint64_t ticket, float* color, float* albedo, float* normal);
+/* Forgets a finished, cancelled or failed request without reading it. */
+int argent_serve_release(ArgentServe* serve, uint64_t ticket);
+/* Steps that ran a batch, path-samples rendered, film bytes in use. */
+int argent_serve_stats(ArgentServe* serve, uint64_t* steps, uint64_t* path_samples, uint64_t* film_bytes_in_use);
+/* Seconds on the serve's steady clock (the clock of ArgentServeStatus). */
+double argent_serve_now(ArgentServe* serve);
+
+/* ------------------------------------------------------------------ */
 /* Measurement (no counterpart in argent, whose only timing is wall   */
 /* clock around render_pass, argent/src/jobs.rs:501-504).             */
 /* ------------------------------------------------------------------ */
@@ -363,6 +446,11 @@ int argent_ctx_set_counting(ArgentCtx* ctx, int on);
 /* out[6] = closest-hit rays, nodes, triangles; any-hit rays, nodes,
  * triangles, counted since the last argent_ctx_set_counting. */
 int argent_ctx_traversal_counts(ArgentCtx* ctx, uint64_t* out);
+/* out[18]: rays by node visits in bins 0, 1, 2-3, 4-7, 8-15, 16-63, 64-255,
+ * 256+ (closest-hit out[0..7], any-hit out[8..15]), then the largest node
+ * count of a closest-hit ray and of an any-hit ray, since the last
+ * argent_ctx_set_counting. */
+int argent_ctx_traversal_histogram(ArgentCtx* ctx, uint64_t* out);
 
 #ifdef __cplusplus
 }

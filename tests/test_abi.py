@@ -63,3 +63,47 @@ def test_error_path_without_device():
     rc = lib.argent_ctx_create(0, None, ctypes.byref(h))
     assert rc == N.E_CUDA
     assert b"device" in lib.argent_last_error(None)
+
+
+def test_serve_structs_match_c(tmp_path):
+    """The serve structs' ctypes mirrors have the compiler's layout."""
+    import subprocess
+
+    from argent_b200 import _native as N
+
+    src = tmp_path / "layout.c"
+    src.write_text('''#include <stddef.h>
+#include <stdio.h>
+#include "argent_gpu.h"
+int main(void) {
+  printf("%zu %zu %zu\\n", sizeof(ArgentServeConfig), offsetof(ArgentServeConfig, step_path_samples), sizeof(ArgentServeRequest));
+  printf("%zu %zu %zu %zu\\n", offsetof(ArgentServeRequest, camera), offsetof(ArgentServeRequest, settings), offsetof(ArgentServeRequest, width), offsetof(ArgentServeRequest, priority));
+  printf("%zu %zu %zu\\n", sizeof(ArgentServeStatus), offsetof(ArgentServeStatus, t_submit), offsetof(ArgentServeStatus, t_done));
+  printf("%zu %zu %zu\\n", sizeof(ArgentBatchItem), offsetof(ArgentBatchItem, film), offsetof(ArgentBatchItem, count));
+  return 0;
+}
+''')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    C, R, S, B = N.ArgentServeConfig, N.ArgentServeRequest, N.ArgentServeStatus, N.ArgentBatchItem
+    want = [ctypes.sizeof(C), C.step_path_samples.offset, ctypes.sizeof(R),
+            R.camera.offset, R.settings.offset, R.width.offset, R.priority.offset,
+            ctypes.sizeof(S), S.t_submit.offset, S.t_done.offset,
+            ctypes.sizeof(B), B.film.offset, B.count.offset]
+    assert got == want
+
+
+def test_serve_rejects_null_arguments():
+    """Serve entry points return ARGENT_E_INVALID for NULL handles (no device needed)."""
+    from argent_b200 import _native as N
+
+    lib = N.gpu()
+    h = ctypes.c_void_p()
+    assert lib.argent_serve_create(None, None, ctypes.byref(h)) == N.E_INVALID
+    t = ctypes.c_uint64()
+    assert lib.argent_serve_submit(None, None, ctypes.byref(t)) == N.E_INVALID
+    assert lib.argent_serve_step(None, None) == N.E_INVALID
+    assert lib.argent_serve_poll(None, 1, None) == N.E_INVALID
+    assert lib.argent_serve_read(None, 1, None, None, None) == N.E_INVALID
+    lib.argent_serve_destroy(None)
