@@ -120,6 +120,12 @@ class ArgentServeStatus(ctypes.Structure):
 REQ_QUEUED, REQ_ACTIVE, REQ_DONE, REQ_CANCELLED, REQ_FAILED = range(5)
 
 
+class ArgentPatinaSettings(ctypes.Structure):
+    _fields_ = [("ao_samples", ctypes.c_uint32), ("ao_distance", ctypes.c_float),
+                ("curvature_radius", ctypes.c_float), ("concavity_weight", ctypes.c_float),
+                ("smooth_iterations", ctypes.c_uint32)]
+
+
 class ArgentMesh(ctypes.Structure):
     _fields_ = [("nv", ctypes.c_uint32), ("nt", ctypes.c_uint32), ("positions", c_float_p), ("normals", c_float_p),
                 ("tris", c_u32_p), ("tri_material", c_u16_p)]
@@ -169,6 +175,19 @@ GPU_FUNCS = {
     "argent_ctx_set_counting": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "argent_ctx_traversal_counts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
     "argent_ctx_traversal_histogram": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
+    "argent_denoise_atrous": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, c_float_p, c_float_p,
+                                             c_float_p, c_float_p]),
+    "argent_film_denoise": (ctypes.c_int, [ctypes.c_void_p, c_float_p]),
+    "argent_piece_ambient_occlusion": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, c_float_p, c_float_p,
+                                                      ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, c_float_p]),
+    "argent_piece_patina_mask": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, c_float_p, c_float_p,
+                                                ctypes.c_uint32, c_u32_p, ctypes.c_uint32,
+                                                ctypes.POINTER(ArgentPatinaSettings), c_float_p]),
+    "argent_mesh_smooth_normals": (ctypes.c_int, [c_float_p, ctypes.c_uint32, c_u32_p, ctypes.c_uint32, c_float_p]),
+    "argent_mesh_concavity": (ctypes.c_int, [c_float_p, ctypes.c_uint32, c_float_p, c_u32_p, ctypes.c_uint32,
+                                             ctypes.c_float, c_float_p]),
+    "argent_mesh_smooth": (ctypes.c_int, [c_float_p, ctypes.c_uint32, c_u32_p, ctypes.c_uint32, c_float_p,
+                                          ctypes.c_uint32, ctypes.c_float]),
     "argent_serve_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ArgentServeConfig),
                                            ctypes.POINTER(ctypes.c_void_p)]),
     "argent_serve_destroy": (None, [ctypes.c_void_p]),

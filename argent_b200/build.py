@@ -28,6 +28,7 @@ GPU_SOURCES = [
     os.path.join(CSRC, "host", "bvh_build.cpp"),
     os.path.join(CSRC, "host", "scene_prep.cpp"),
     os.path.join(CSRC, "host", "serve.cpp"),
+    os.path.join(CSRC, "host", "cavity.cpp"),
 ]
 HOST_SOURCES = [
     os.path.join(CSRC, "host", "synth.cpp"),

@@ -18,8 +18,10 @@
 #include "device/traverse.cuh"
 #include "host/bvh_build.h"
 #include "host/scene_prep.h"
+#include "host/cavity.h"
 #include "internal.cuh"
 #include "render_impl.cuh"
+#include "denoise.cuh"
 
 using namespace dev;
 
@@ -75,6 +77,53 @@ __global__ void k_trace_any(DevPiece pc, const ArgentRay* __restrict__ rays, uin
     float4 a = __ldg(rp), b = __ldg(rp + 1);
     occ[i] = trace_any(pc, V3{a.x, a.y, a.z}, V3{b.x, b.y, b.z}, a.w, status) ? 1 : 0;
   }
+}
+
+// ------------------------------------------------------------------ cavity ambient occlusion
+
+// cavity.rs:96-135, one thread per (vertex, sample): the ray from the
+// vertex nudged eps along its normal, direction from a cosine-weighted
+// stratified hemisphere rotated by a vertex hash, tested for any hit within
+// `distance` (the Occluder of scene.rs:40-44).  Consecutive threads are
+// samples of one vertex, so a warp's rays share an origin.  glam's
+// normalize_or_zero and any_orthonormal_pair (Duff et al. 2017, sign =
+// signum(z)) are restated in glam's scalar operation order.
+__global__ void __launch_bounds__(128) k_cavity_ao(DevPiece pc, const float* __restrict__ normals, uint32_t nv,
+                                                   uint32_t n, float distance, float eps, uint32_t* counts,
+                                                   uint32_t* status) {
+  uint64_t total = (uint64_t)nv * n;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t v = (uint32_t)(i / n), k = (uint32_t)(i % n);
+    float nx = normals[3 * (size_t)v], ny = normals[3 * (size_t)v + 1], nz = normals[3 * (size_t)v + 2];
+    float rcp = __fdiv_rn(1.0f, __fsqrt_rn((nx * nx + ny * ny) + nz * nz));
+    if (!(isfinite(rcp) && rcp > 0.0f)) continue;
+    nx *= rcp;
+    ny *= rcp;
+    nz *= rcp;
+    float sign = signbit(nz) ? -1.0f : 1.0f;
+    float a = __fdiv_rn(-1.0f, sign + nz);
+    float bb = nx * ny * a;
+    float tx = 1.0f + sign * nx * nx * a, ty = sign * bb, tz = -sign * nx;
+    float bx = bb, by = sign + ny * ny * a, bz = -ny;
+    float4 p = __ldg(pc.pos + v);
+    V3 o{p.x + nx * eps, p.y + ny * eps, p.z + nz * eps};
+    uint32_t h = hash32(v ^ 0x5bd1e995u);
+    float rot = (float)(h >> 8) * (1.0f / 16777216.0f);
+    float jit = (float)(hash32(h) >> 8) * (1.0f / 16777216.0f);
+    float u1 = fminf(__fdiv_rn((float)k + jit, (float)n), 0.999999f);
+    float x = (float)k * 0.618034f + rot;
+    float u2 = x - truncf(x);
+    float r = __fsqrt_rn(u1);
+    float phi = 6.28318530717958647692f * u2;
+    float c = r * cosf(phi), sn = r * sinf(phi), w = __fsqrt_rn(1.0f - u1);
+    V3 d{(tx * c + bx * sn) + nx * w, (ty * c + by * sn) + ny * w, (tz * c + bz * sn) + nz * w};
+    if (trace_any(pc, o, d, distance, status)) atomicAdd(counts + v, 1u);
+  }
+}
+
+__global__ void k_cavity_ao_finish(const uint32_t* counts, uint32_t nv, uint32_t n, float* out) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+    out[v] = __fdiv_rn((float)counts[v], (float)n);
 }
 
 // ------------------------------------------------------------------ context
@@ -205,6 +254,7 @@ void argent_ctx_destroy(ArgentCtx* ctx) {
   for (cudaEvent_t e : ctx->prof.pool) cudaEventDestroy(e);
   for (int l = 0; l < ARGENT_LANES; ++l) ctx->wave[l].release();
   if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->resolve) cudaFree(ctx->resolve);
   for (int l = 1; l < ARGENT_LANES; ++l)
     if (ctx->lane_stream[l]) cudaStreamDestroy(ctx->lane_stream[l]);
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
@@ -395,6 +445,204 @@ int argent_trace_anyhit(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* ray
   if (rc != ARGENT_OK) return rc;
   if (e != cudaSuccess) return set_error(ctx, ARGENT_E_CUDA, std::string("trace: ") + cudaGetErrorString(e));
   return ctx_check_status(ctx);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ à-trous denoise
+
+namespace {
+
+// argent-post's atrous (denoise.rs:653-712) on device buffers: d_color
+// (and the optional guides) in, d_out out; w*h pixels, 3 floats each.
+int run_atrous(ArgentCtx* ctx, uint32_t w, uint32_t h, const float* d_color, const float* d_albedo,
+               const float* d_normal, float* d_out) {
+  size_t np = (size_t)w * h;
+  cudaStream_t st = ctx->stream;
+  float* base = nullptr;
+  // sig, sig2, demod, g_albedo, g_normal (3 np each); l, l2, var, var2, vb, tmp, tmp2 (np each)
+  size_t total = 15 * np + 7 * np;
+  ARGENT_CK(ctx, cudaMallocAsync((void**)&base, total * sizeof(float), st));
+  float *sig = base, *sig2 = sig + 3 * np, *demod = sig2 + 3 * np, *ga = demod + 3 * np, *gn = ga + 3 * np;
+  float *l = gn + 3 * np, *l2 = l + np, *var = l2 + np, *var2 = var + np, *vb = var2 + np, *tmp = vb + np,
+        *tmp2 = tmp + np;
+  int grid = (int)std::min<size_t>((np + 255) / 256, (size_t)ctx->num_sms * 8);
+  grid = std::max(grid, 1);
+  auto blur = [&](const float* src, float* dst, std::initializer_list<float> k) {
+    dn::Taps t{};
+    t.n = 0;
+    for (float v : k) t.k[t.n++] = v;
+    dn::k_dn_blur<<<grid, 256, 0, st>>>(src, tmp2, w, h, t, 0);
+    dn::k_dn_blur<<<grid, 256, 0, st>>>(tmp2, dst, w, h, t, 1);
+    ctx->launches += 2;
+  };
+  dn::k_dn_prep<<<grid, 256, 0, st>>>(d_color, d_albedo, d_normal, (uint32_t)np, sig, l, demod, ga, gn);
+  ctx->launches++;
+  // noise_variance (denoise.rs:582-586)
+  blur(l, tmp, {1.0f, 1.0f, 1.0f});
+  dn::k_dn_resid<<<grid, 256, 0, st>>>(l, tmp, (uint32_t)np, vb);
+  ctx->launches++;
+  blur(vb, var, {1.0f, 1.0f, 1.0f, 1.0f, 1.0f});
+  for (int pass = 0; pass < DN_PASSES; ++pass) {
+    blur(var, vb, {0.25f, 0.5f, 0.25f});
+    dn::k_dn_atrous<<<grid, 256, 0, st>>>(sig, l, var, vb, d_albedo ? ga : nullptr, d_normal ? gn : nullptr, w, h,
+                                          1 << pass, sig2, var2, l2);
+    ctx->launches++;
+    std::swap(sig, sig2);
+    std::swap(var, var2);
+    std::swap(l, l2);
+  }
+  if (d_albedo) {
+    dn::k_dn_remod<<<grid, 256, 0, st>>>(sig, demod, (uint32_t)np);
+    ctx->launches++;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_out, sig, 3 * np * sizeof(float), cudaMemcpyDeviceToDevice, st);
+  cudaFreeAsync(base, st);
+  if (e != cudaSuccess) return set_error(ctx, ARGENT_E_CUDA, std::string("denoise: ") + cudaGetErrorString(e));
+  return ARGENT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int argent_denoise_atrous(ArgentCtx* ctx, uint32_t width, uint32_t height, const float* color, const float* albedo,
+                          const float* normal, float* out) {
+  if (!ctx || (width && height && (!color || !out))) return set_error(ctx, ARGENT_E_INVALID, "NULL argument");
+  if (normal && !albedo) normal = nullptr;  // a lone normal is ignored, as with OIDN (denoise.rs:16-17)
+  size_t np = (size_t)width * height;
+  if (np == 0) return ARGENT_OK;
+  if (np > (1ull << 31)) return set_error(ctx, ARGENT_E_INVALID, "image too large");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  float* d = nullptr;
+  ARGENT_CK(ctx, cudaMallocAsync((void**)&d, 12 * np * sizeof(float), ctx->stream));
+  float *dc = d, *da = albedo ? d + 3 * np : nullptr, *dn_ = normal ? d + 6 * np : nullptr, *dout = d + 9 * np;
+  cudaError_t e = cudaMemcpyAsync(dc, color, 3 * np * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess && da) e = cudaMemcpyAsync(da, albedo, 3 * np * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess && dn_) e = cudaMemcpyAsync(dn_, normal, 3 * np * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+  int rc = e == cudaSuccess ? run_atrous(ctx, width, height, dc, da, dn_, dout) : ARGENT_E_CUDA;
+  if (rc == ARGENT_OK) e = cudaMemcpyAsync(out, dout, 3 * np * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaFreeAsync(d, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (rc != ARGENT_OK) return rc;
+  if (e != cudaSuccess) return set_error(ctx, ARGENT_E_CUDA, std::string("denoise: ") + cudaGetErrorString(e));
+  return ctx_check_status(ctx);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ cavity mask
+
+extern "C" {
+
+int argent_mesh_smooth_normals(const float* positions, uint32_t nv, const uint32_t* tris, uint32_t nt, float* out) {
+  if ((nv && (!positions || !out)) || (nt && !tris)) return set_error(nullptr, ARGENT_E_INVALID, "NULL argument");
+  for (uint64_t i = 0; i < 3ull * nt; ++i)
+    if (tris[i] >= nv) return set_error(nullptr, ARGENT_E_INVALID, "triangle index out of range");
+  argent::smooth_vertex_normals(positions, nv, tris, nt, out);
+  return ARGENT_OK;
+}
+
+int argent_mesh_concavity(const float* positions, uint32_t nv, const float* normals, const uint32_t* tris, uint32_t nt,
+                          float radius, float* out) {
+  if ((nv && (!positions || !normals || !out)) || (nt && !tris))
+    return set_error(nullptr, ARGENT_E_INVALID, "NULL argument");
+  for (uint64_t i = 0; i < 3ull * nt; ++i)
+    if (tris[i] >= nv) return set_error(nullptr, ARGENT_E_INVALID, "triangle index out of range");
+  argent::concavity(positions, nv, tris, nt, normals, radius, out);
+  return ARGENT_OK;
+}
+
+int argent_mesh_smooth(const float* positions, uint32_t nv, const uint32_t* tris, uint32_t nt, float* values,
+                       uint32_t iterations, float lambda) {
+  if ((nv && (!positions || !values)) || (nt && !tris)) return set_error(nullptr, ARGENT_E_INVALID, "NULL argument");
+  for (uint64_t i = 0; i < 3ull * nt; ++i)
+    if (tris[i] >= nv) return set_error(nullptr, ARGENT_E_INVALID, "triangle index out of range");
+  argent::smooth_values(positions, nv, tris, nt, values, iterations, lambda);
+  return ARGENT_OK;
+}
+
+int argent_piece_ambient_occlusion(ArgentCtx* ctx, ArgentPiece* piece, const float* positions, const float* normals,
+                                   uint32_t nv, uint32_t samples, float distance, float* ao) {
+  if (!ctx || !piece || (nv && (!positions || !normals || !ao))) return set_error(ctx, ARGENT_E_INVALID, "NULL argument");
+  if (nv != piece->nv) return set_error(ctx, ARGENT_E_INVALID, "vertex count differs from the uploaded piece");
+  if (nv == 0) return ARGENT_OK;
+  if (piece->nt == 0 || samples == 0 || !(distance > 0.0f)) {
+    std::fill(ao, ao + nv, 0.0f);
+    return ARGENT_OK;
+  }
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  // cavity.rs:87-90: eps = max(2e-4 * |hi - lo|, 1e-3) over the vertices.
+  float lo[3] = {positions[0], positions[1], positions[2]}, hi[3] = {positions[0], positions[1], positions[2]};
+  for (uint32_t v = 1; v < nv; ++v)
+    for (int k = 0; k < 3; ++k) {
+      float x = positions[3 * (size_t)v + k];
+      lo[k] = x < lo[k] ? x : lo[k];
+      hi[k] = x > hi[k] ? x : hi[k];
+    }
+  float ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
+  float diag = std::sqrt((ex * ex + ey * ey) + ez * ez);
+  float eps = std::max(2e-4f * diag, 1e-3f);
+  float* d_n = nullptr;
+  uint32_t* d_cnt = nullptr;
+  float* d_ao = nullptr;
+  ARGENT_CK(ctx, cudaMallocAsync((void**)&d_n, 3ull * nv * sizeof(float), ctx->stream));
+  ARGENT_CK(ctx, cudaMallocAsync((void**)&d_cnt, (size_t)nv * sizeof(uint32_t), ctx->stream));
+  ARGENT_CK(ctx, cudaMallocAsync((void**)&d_ao, (size_t)nv * sizeof(float), ctx->stream));
+  ARGENT_CK(ctx, cudaMemcpyAsync(d_n, normals, 3ull * nv * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+  ARGENT_CK(ctx, cudaMemsetAsync(d_cnt, 0, (size_t)nv * sizeof(uint32_t), ctx->stream));
+  uint64_t total = (uint64_t)nv * samples;
+  int grid = grid_for(ctx, (const void*)k_cavity_ao, 128, total);
+  {
+    ProfScope ps(ctx, KC_TRACE);
+    k_cavity_ao<<<grid, 128, 0, ctx->stream>>>(piece->dev, d_n, nv, samples, distance, eps, d_cnt, ctx->d_status);
+  }
+  int g2 = (int)std::min<uint64_t>((nv + 255) / 256, (uint64_t)ctx->num_sms * 8);
+  k_cavity_ao_finish<<<std::max(g2, 1), 256, 0, ctx->stream>>>(d_cnt, nv, samples, d_ao);
+  ctx->launches += 2;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ao, d_ao, (size_t)nv * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaFreeAsync(d_n, ctx->stream);
+  cudaFreeAsync(d_cnt, ctx->stream);
+  cudaFreeAsync(d_ao, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return set_error(ctx, ARGENT_E_CUDA, std::string("ambient occlusion: ") + cudaGetErrorString(e));
+  return ctx_check_status(ctx);
+}
+
+int argent_piece_patina_mask(ArgentCtx* ctx, ArgentPiece* piece, const float* positions, const float* normals,
+                             uint32_t nv, const uint32_t* tris, uint32_t nt, const ArgentPatinaSettings* settings,
+                             float* mask) {
+  if (!ctx || !piece || !settings || (nv && (!positions || !mask)) || (nt && !tris))
+    return set_error(ctx, ARGENT_E_INVALID, "NULL argument");
+  if (nv != piece->nv || nt != piece->nt)
+    return set_error(ctx, ARGENT_E_INVALID, "mesh differs from the uploaded piece");
+  for (uint64_t i = 0; i < 3ull * nt; ++i)
+    if (tris[i] >= nv) return set_error(ctx, ARGENT_E_INVALID, "triangle index out of range");
+  if (nv == 0) return ARGENT_OK;
+  if (nt == 0) {
+    std::fill(mask, mask + nv, 0.0f);
+    return ARGENT_OK;
+  }
+  std::vector<float> nrm(3 * (size_t)nv);
+  if (normals)
+    std::memcpy(nrm.data(), normals, nrm.size() * sizeof(float));
+  else
+    argent::smooth_vertex_normals(positions, nv, tris, nt, nrm.data());
+  std::vector<float> ao(nv, 0.0f), cav(nv, 0.0f);
+  if (settings->ao_samples > 0 && settings->ao_distance > 0.0f) {
+    int rc = argent_piece_ambient_occlusion(ctx, piece, positions, nrm.data(), nv, settings->ao_samples,
+                                            settings->ao_distance, ao.data());
+    if (rc != ARGENT_OK) return rc;
+  }
+  float w = std::min(std::max(settings->concavity_weight, 0.0f), 1.0f);
+  if (w > 0.0f && settings->curvature_radius > 0.0f)
+    argent::concavity(positions, nv, tris, nt, nrm.data(), settings->curvature_radius, cav.data());
+  argent::patina_blend(positions, nv, tris, nt, ao.data(), cav.data(), settings->concavity_weight,
+                       settings->smooth_iterations, mask);
+  return ARGENT_OK;
 }
 
 }  // extern "C"
@@ -869,44 +1117,126 @@ int argent_film_read_xyz(ArgentFilm* f, float* out) {
 }
 
 // render.rs:36-62: averages; color is the camera matrix applied to XYZ.
+}  // extern "C"
+
+namespace {
+
+struct Mat3 {
+  float m[9];
+};
+
+// Film::color / albedo / normal (render.rs:40-62) per pixel: camera RGB of
+// the XYZ sums (((m0 x + m1 y) + m2 z) * k per row), albedo * k, and the
+// normal sum scaled by k and normalised (zero when shorter than 1e-6), each
+// rounded as the host loops round them (the library has no FMA contraction).
+__global__ void __launch_bounds__(256) k_film_resolve(const float* xyz, const double* xyz64, const float* alb,
+                                                      const float* nrm, Mat3 mt, float k, uint32_t np, float* color,
+                                                      float* albedo, float* normal) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+    size_t o = 3 * (size_t)i;
+    if (color) {
+      float x, y, z;
+      if (xyz64) {
+        x = (float)xyz64[o];
+        y = (float)xyz64[o + 1];
+        z = (float)xyz64[o + 2];
+      } else {
+        x = xyz[o];
+        y = xyz[o + 1];
+        z = xyz[o + 2];
+      }
+      const float* m = mt.m;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) color[o + c] = (m[3 * c] * x + m[3 * c + 1] * y + m[3 * c + 2] * z) * k;
+    }
+    if (albedo) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) albedo[o + c] = alb[o + c] * k;
+    }
+    if (normal) {
+      float v[3] = {nrm[o] * k, nrm[o + 1] * k, nrm[o + 2] * k};
+      float l = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) normal[o + c] = l > 1e-6f ? v[c] / l : 0.0f;
+    }
+  }
+}
+
+// Device staging for film reads, grown on demand and kept by the context.
+int ensure_resolve(ArgentCtx* ctx, size_t floats) {
+  if (ctx->resolve_floats >= floats) return ARGENT_OK;
+  if (ctx->resolve) cudaFree(ctx->resolve);
+  ctx->resolve = nullptr;
+  ctx->resolve_floats = 0;
+  if (cudaMalloc(&ctx->resolve, floats * sizeof(float)) != cudaSuccess)
+    return set_error(ctx, ARGENT_E_OOM, "film read staging: out of device memory");
+  ctx->resolve_floats = floats;
+  return ARGENT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int argent_film_read(ArgentFilm* f, float* color, float* albedo, float* normal) {
   if (!f) return set_error(nullptr, ARGENT_E_INVALID, "film is NULL");
   ArgentCtx* ctx = f->ctx;
   ARGENT_CK(ctx, cudaSetDevice(ctx->device));
   size_t np = (size_t)f->w * f->h;
+  if (!color && !albedo && !normal) return ARGENT_OK;
   float k = 1.0f / (float)std::max<uint32_t>(f->samples, 1);
-  if (color) {
-    std::vector<double> xyz;
-    int rc = film_fetch_xyz(f, xyz);
-    if (rc != ARGENT_OK) return rc;
-    float m[9];
-    if (f->has_matrix)
-      std::memcpy(m, f->cam_m, sizeof(m));
-    else
-      argent::camera_matrix(false, nullptr, m);
-    for (size_t i = 0; i < np; ++i) {
-      float x = (float)xyz[3 * i], y = (float)xyz[3 * i + 1], z = (float)xyz[3 * i + 2];
-      for (int c = 0; c < 3; ++c) color[3 * i + c] = (m[3 * c] * x + m[3 * c + 1] * y + m[3 * c + 2] * z) * k;
-    }
-  }
-  if (albedo) {
-    ARGENT_CK(ctx, cudaMemcpyAsync(albedo, f->albedo, 3 * np * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
-  }
-  std::vector<float> nrm;
-  if (normal) {
-    nrm.resize(3 * np);
-    ARGENT_CK(ctx, cudaMemcpyAsync(nrm.data(), f->normal, 3 * np * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
-  }
-  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  Mat3 mt;
+  if (f->has_matrix)
+    std::memcpy(mt.m, f->cam_m, sizeof(mt.m));
+  else
+    argent::camera_matrix(false, nullptr, mt.m);
+  int rc = ensure_resolve(ctx, 9 * np);
+  if (rc != ARGENT_OK) return rc;
+  float* d_color = color ? ctx->resolve : nullptr;
+  float* d_albedo = albedo ? ctx->resolve + 3 * np : nullptr;
+  float* d_normal = normal ? ctx->resolve + 6 * np : nullptr;
+  int grid = (int)std::min<size_t>((np + 255) / 256, (size_t)ctx->num_sms * 8);
+  k_film_resolve<<<std::max(grid, 1), 256, 0, ctx->stream>>>(f->xyz, f->xyz64, f->albedo, f->normal, mt, k,
+                                                              (uint32_t)np, d_color, d_albedo, d_normal);
+  ctx->launches++;
+  ARGENT_CK(ctx, cudaGetLastError());
+  if (color)
+    ARGENT_CK(ctx, cudaMemcpyAsync(color, d_color, 3 * np * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
   if (albedo)
-    for (size_t i = 0; i < 3 * np; ++i) albedo[i] *= k;
-  if (normal) {
-    for (size_t i = 0; i < np; ++i) {
-      float v[3] = {nrm[3 * i] * k, nrm[3 * i + 1] * k, nrm[3 * i + 2] * k};
-      float l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-      for (int c = 0; c < 3; ++c) normal[3 * i + c] = l > 1e-6f ? v[c] / l : 0.0f;
-    }
-  }
+    ARGENT_CK(ctx, cudaMemcpyAsync(albedo, d_albedo, 3 * np * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  if (normal)
+    ARGENT_CK(ctx, cudaMemcpyAsync(normal, d_normal, 3 * np * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  return ctx_check_status(ctx);
+}
+
+int argent_film_denoise(ArgentFilm* f, float* out) {
+  if (!f || !out) return set_error(f ? f->ctx : nullptr, ARGENT_E_INVALID, "NULL argument");
+  ArgentCtx* ctx = f->ctx;
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  size_t np = (size_t)f->w * f->h;
+  float k = 1.0f / (float)std::max<uint32_t>(f->samples, 1);
+  Mat3 mt;
+  if (f->has_matrix)
+    std::memcpy(mt.m, f->cam_m, sizeof(mt.m));
+  else
+    argent::camera_matrix(false, nullptr, mt.m);
+  int rc = ensure_resolve(ctx, 9 * np);
+  if (rc != ARGENT_OK) return rc;
+  float *dc = ctx->resolve, *da = ctx->resolve + 3 * np, *dnrm = ctx->resolve + 6 * np;
+  int grid = (int)std::min<size_t>((np + 255) / 256, (size_t)ctx->num_sms * 8);
+  k_film_resolve<<<std::max(grid, 1), 256, 0, ctx->stream>>>(f->xyz, f->xyz64, f->albedo, f->normal, mt, k,
+                                                              (uint32_t)np, dc, da, dnrm);
+  ctx->launches++;
+  float* dout = nullptr;
+  ARGENT_CK(ctx, cudaMallocAsync((void**)&dout, 3 * np * sizeof(float), ctx->stream));
+  rc = run_atrous(ctx, f->w, f->h, dc, da, dnrm, dout);
+  cudaError_t e = cudaSuccess;
+  if (rc == ARGENT_OK) e = cudaMemcpyAsync(out, dout, 3 * np * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaFreeAsync(dout, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (rc != ARGENT_OK) return rc;
+  if (e != cudaSuccess) return set_error(ctx, ARGENT_E_CUDA, std::string("film denoise: ") + cudaGetErrorString(e));
   return ctx_check_status(ctx);
 }
 

@@ -72,9 +72,24 @@ struct NodeView {
   uint32_t qlx0, qlx1, qly0, qly1, qlz0, qlz1, qhx0, qhx1, qhy0, qhy1, qhz0, qhz1;
 };
 
+// Read-only 16-byte load of BVH node data with the L2 "evict last"
+// priority: every ray walks the upper levels and the node array is a small
+// share of what passes through L2 (path state streams through it once per
+// kernel), so nodes are kept in preference to the streaming data.
+__device__ __forceinline__ uint4 ld_node16(const uint4* ptr) {
+  uint4 r;
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  asm("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+      : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+      : "l"(ptr), "l"(pol));
+  return r;
+}
+
 __device__ __forceinline__ NodeView load_node(const uint4* nodes, uint32_t idx) {
   const uint4* p = nodes + 5 * (size_t)idx;
-  uint4 w0 = __ldg(p), w1 = __ldg(p + 1), w2 = __ldg(p + 2), w3 = __ldg(p + 3), w4 = __ldg(p + 4);
+  uint4 w0 = ld_node16(p), w1 = ld_node16(p + 1), w2 = ld_node16(p + 2), w3 = ld_node16(p + 3),
+        w4 = ld_node16(p + 4);
   NodeView n;
   n.ox = __uint_as_float(w0.x);
   n.oy = __uint_as_float(w0.y);
@@ -174,6 +189,28 @@ struct NodeQ {
   AxisQ x, y, z;
 };
 
+// The whole box of a node, planes 0 and 255 on every axis (it holds every
+// child box), with the slack of axis_q.  Reads only the node's first 16
+// bytes.  A ray that misses the root's box misses the piece.
+__device__ __forceinline__ bool node_box_hit(const uint4* nodes, uint32_t idx, const RayQ& r, float t_max) {
+  uint4 w0 = ld_node16(nodes + 5 * (size_t)idx);
+  float o[3] = {__uint_as_float(w0.x), __uint_as_float(w0.y), __uint_as_float(w0.z)};
+  float ro[3] = {r.o.x, r.o.y, r.o.z};
+  float iv[3] = {r.ix, r.iy, r.iz};
+  float tmin = 0.0f, tmax = t_max;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float scale = __uint_as_float(((w0.w >> (8 * k)) & 0xffu) << 23);
+    float dd = __fsub_rn(o[k], ro[k]);
+    float b = __fmul_rn(dd, iv[k]);
+    float e = __fmul_rn(__fmul_rn(__fadd_rn(fabsf(dd), __fmul_rn(256.0f, scale)), fabsf(iv[k])), 3.814697265625e-06f);
+    float t1 = __fmaf_rn(255.0f, __fmul_rn(scale, iv[k]), b);
+    tmin = fmaxf(tmin, __fsub_rn(fminf(b, t1), e));
+    tmax = fminf(tmax, __fadd_rn(fmaxf(b, t1), e));
+  }
+  return tmin <= tmax;
+}
+
 __device__ __forceinline__ NodeQ node_ray(const NodeView& n, const RayQ& r) {
   NodeQ q;
   q.x = axis_q(n.ox, n.sx, r.o.x, r.ix, r.nx, n.qlx0, n.qlx1, n.qhx0, n.qhx1);
@@ -245,118 +282,186 @@ __device__ __forceinline__ void sort8(uint32_t k[8]) {
 // The visit order changes how much is pruned, never the result: a triangle
 // whose hit is the final best has box entry <= that distance <= the running
 // best at every point, so its box is always entered.
-__device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, float t_max, uint32_t* status) {
-  TraceHit best{t_max, 0.0f, 0.0f, ARGENT_NO_HIT_U};
-  if (pc.num_tris == 0) return best;
-  RayQ rq = make_rayq(o, d);
-  uint2 stack[ARGENT_STACK_SIZE];
-  int sp = 0;
-  uint32_t n_nodes = 0, n_tris = 0;
-  uint32_t ref = 0u;
-  bool have = true;
-  for (;;) {
-    if (!have) {
-      if (sp == 0) break;
-      --sp;
-      ref = stack[sp].x;
-      if (__uint_as_float(stack[sp].y) > best.t) continue;
-    }
-    have = false;
-    if (ref & ARGENT_LEAF_BIT) {
-      uint32_t start = ref & 0x07FFFFFFu;
-      uint32_t cnt = ((ref >> 27) & 15u) + 1u;
-      n_tris += cnt;
-      for (uint32_t i = 0; i < cnt; ++i) {
-        float t, u, v;
-        uint32_t prim;
-        // Accept t == best.t too, so equal-t ties resolve by index.
-        float lim = best.t;
-        if (mt_hit(pc.tris + 3 * (size_t)(start + i), o, d, t_max, &t, &u, &v, &prim)) {
-          if (t < lim || (t == lim && prim < best.prim)) {
-            best.t = t;
-            best.u = u;
-            best.v = v;
-            best.prim = prim;
-          }
-        }
-      }
-      continue;
-    }
-    NodeView n = load_node(pc.nodes, ref);
-    ++n_nodes;
-    NodeQ nq = node_ray(n, rq);
-    uint32_t k[8];
-    int nh = 0;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      float tc;
-      bool h = child_q(nq, c, best.t, &tc) && ((n.present >> c) & 1u);
-      k[c] = h ? ((__float_as_uint(tc) & ~7u) | (uint32_t)c) : 0xFFFFFFFFu;
-      nh += h ? 1 : 0;
-    }
-    if (nh == 0) continue;
-    if (sp + nh - 1 > ARGENT_STACK_SIZE) {
-      atomicOr(status, ARGENT_STATUS_STACK_OVERFLOW);
-      break;
-    }
-    sort8(k);
-#pragma unroll
-    for (int j = 7; j >= 1; --j) {
-      if (j < nh) stack[sp++] = make_uint2(child_ref(n, (int)(k[j] & 7u)), k[j] & ~7u);
-    }
-    ref = child_ref(n, (int)(k[0] & 7u));
-    have = true;
-  }
-  count_visits(0, n_nodes, n_tris);
-  return best;
+//
+// The traversal is resumable: closest_begin sets it up and each
+// closest_step visits one node or one leaf, so a kernel can interleave the
+// steps of rays that start at different times (persistent lanes that take a
+// new ray as soon as theirs finishes).  The stack lives with the caller.
+struct ClosestTrav {
+  V3 o, d;
+  RayQ rq;
+  float t_max;
+  TraceHit best;
+  uint32_t ref;
+  int sp;
+  bool have;
+  uint32_t n_nodes, n_tris;
+};
+
+// Returns false when the traversal is already over (empty piece, or a ray
+// that misses the piece's box); s.best is then a miss.
+__device__ __forceinline__ bool closest_begin(const DevPiece& pc, ClosestTrav& s, V3 o, V3 d, float t_max) {
+  s.o = o;
+  s.d = d;
+  s.t_max = t_max;
+  s.best = TraceHit{t_max, 0.0f, 0.0f, ARGENT_NO_HIT_U};
+  s.ref = 0u;
+  s.sp = 0;
+  s.have = false;
+  s.n_nodes = 0;
+  s.n_tris = 0;
+  if (pc.num_tris == 0) return false;
+  s.rq = make_rayq(o, d);
+  if (!node_box_hit(pc.nodes, 0u, s.rq, t_max)) return false;
+  s.have = true;
+  return true;
 }
 
-// Any hit with t in (1e-7, t_max), bvh.rs:216-247.
-__device__ __noinline__ bool trace_any(const DevPiece& pc, V3 o, V3 d, float t_max, uint32_t* status) {
-  if (pc.num_tris == 0) return false;
-  RayQ rq = make_rayq(o, d);
-  uint32_t stack[ARGENT_STACK_SIZE];
-  int sp = 0;
-  uint32_t n_nodes = 0, n_tris = 0;
-  stack[sp++] = 0u;
-  while (sp > 0) {
-    uint32_t ref = stack[--sp];
-    if (ref & ARGENT_LEAF_BIT) {
-      uint32_t start = ref & 0x07FFFFFFu;
-      uint32_t cnt = ((ref >> 27) & 15u) + 1u;
-      for (uint32_t i = 0; i < cnt; ++i) {
-        float t, u, v;
-        uint32_t prim;
-        ++n_tris;
-        if (mt_hit(pc.tris + 3 * (size_t)(start + i), o, d, t_max, &t, &u, &v, &prim)) {
-          count_visits(3, n_nodes, n_tris);
-          return true;
+// Visits one node or one leaf; true when the traversal has finished.
+__device__ __forceinline__ bool closest_step(const DevPiece& pc, ClosestTrav& s, uint2* stack, uint32_t* status) {
+  if (!s.have) {
+    for (;;) {
+      if (s.sp == 0) return true;
+      --s.sp;
+      if (__uint_as_float(stack[s.sp].y) <= s.best.t) break;
+    }
+    s.ref = stack[s.sp].x;
+  }
+  s.have = false;
+  uint32_t ref = s.ref;
+  if (ref & ARGENT_LEAF_BIT) {
+    uint32_t start = ref & 0x07FFFFFFu;
+    uint32_t cnt = ((ref >> 27) & 15u) + 1u;
+    s.n_tris += cnt;
+    for (uint32_t i = 0; i < cnt; ++i) {
+      float t, u, v;
+      uint32_t prim;
+      // Accept t == best.t too, so equal-t ties resolve by index.
+      float lim = s.best.t;
+      if (mt_hit(pc.tris + 3 * (size_t)(start + i), s.o, s.d, s.t_max, &t, &u, &v, &prim)) {
+        if (t < lim || (t == lim && prim < s.best.prim)) {
+          s.best.t = t;
+          s.best.u = u;
+          s.best.v = v;
+          s.best.prim = prim;
         }
       }
-      continue;
     }
-    NodeView n = load_node(pc.nodes, ref);
-    ++n_nodes;
-    NodeQ nq = node_ray(n, rq);
-    uint32_t hitmask = 0;
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      float tmin;
-      if (child_q(nq, c, t_max, &tmin)) hitmask |= 1u << c;
-    }
-    hitmask &= n.present;
-    if (sp + __popc(hitmask) > ARGENT_STACK_SIZE) {
-      atomicOr(status, ARGENT_STATUS_STACK_OVERFLOW);
-      return false;
-    }
-    while (hitmask) {
-      int c = __ffs(hitmask) - 1;
-      hitmask &= hitmask - 1u;
-      stack[sp++] = child_ref(n, c);
-    }
+    return s.sp == 0;
   }
-  count_visits(3, n_nodes, n_tris);
+  NodeView n = load_node(pc.nodes, ref);
+  ++s.n_nodes;
+  NodeQ nq = node_ray(n, s.rq);
+  uint32_t k[8];
+  int nh = 0;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    float tc;
+    bool h = child_q(nq, c, s.best.t, &tc) && ((n.present >> c) & 1u);
+    k[c] = h ? ((__float_as_uint(tc) & ~7u) | (uint32_t)c) : 0xFFFFFFFFu;
+    nh += h ? 1 : 0;
+  }
+  if (nh == 0) return s.sp == 0;
+  if (s.sp + nh - 1 > ARGENT_STACK_SIZE) {
+    atomicOr(status, ARGENT_STATUS_STACK_OVERFLOW);
+    s.sp = 0;
+    return true;
+  }
+  sort8(k);
+#pragma unroll
+  for (int j = 7; j >= 1; --j) {
+    if (j < nh) stack[s.sp++] = make_uint2(child_ref(n, (int)(k[j] & 7u)), k[j] & ~7u);
+  }
+  s.ref = child_ref(n, (int)(k[0] & 7u));
+  s.have = true;
   return false;
+}
+
+__device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, float t_max, uint32_t* status) {
+  ClosestTrav s;
+  uint2 stack[ARGENT_STACK_SIZE];
+  if (closest_begin(pc, s, o, d, t_max))
+    while (!closest_step(pc, s, stack, status)) {
+    }
+  count_visits(0, s.n_nodes, s.n_tris);
+  return s.best;
+}
+
+// Any hit with t in (1e-7, t_max), bvh.rs:216-247, resumable like the
+// closest-hit traversal.
+struct AnyTrav {
+  V3 o, d;
+  RayQ rq;
+  float t_max;
+  int sp;
+  uint32_t n_nodes, n_tris;
+};
+
+#define ARGENT_ANY_RUNNING 0
+#define ARGENT_ANY_HIT 1
+#define ARGENT_ANY_CLEAR 2
+
+// Returns ARGENT_ANY_RUNNING, or ARGENT_ANY_CLEAR when the ray misses the
+// piece outright.
+__device__ __forceinline__ int any_begin(const DevPiece& pc, AnyTrav& s, uint32_t* stack, V3 o, V3 d, float t_max) {
+  s.o = o;
+  s.d = d;
+  s.t_max = t_max;
+  s.sp = 0;
+  s.n_nodes = 0;
+  s.n_tris = 0;
+  if (pc.num_tris == 0) return ARGENT_ANY_CLEAR;
+  s.rq = make_rayq(o, d);
+  if (!node_box_hit(pc.nodes, 0u, s.rq, t_max)) return ARGENT_ANY_CLEAR;
+  stack[s.sp++] = 0u;
+  return ARGENT_ANY_RUNNING;
+}
+
+// Visits one node or one leaf.
+__device__ __forceinline__ int any_step(const DevPiece& pc, AnyTrav& s, uint32_t* stack, uint32_t* status) {
+  if (s.sp == 0) return ARGENT_ANY_CLEAR;
+  uint32_t ref = stack[--s.sp];
+  if (ref & ARGENT_LEAF_BIT) {
+    uint32_t start = ref & 0x07FFFFFFu;
+    uint32_t cnt = ((ref >> 27) & 15u) + 1u;
+    for (uint32_t i = 0; i < cnt; ++i) {
+      float t, u, v;
+      uint32_t prim;
+      ++s.n_tris;
+      if (mt_hit(pc.tris + 3 * (size_t)(start + i), s.o, s.d, s.t_max, &t, &u, &v, &prim)) return ARGENT_ANY_HIT;
+    }
+    return s.sp == 0 ? ARGENT_ANY_CLEAR : ARGENT_ANY_RUNNING;
+  }
+  NodeView n = load_node(pc.nodes, ref);
+  ++s.n_nodes;
+  NodeQ nq = node_ray(n, s.rq);
+  uint32_t hitmask = 0;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    float tmin;
+    if (child_q(nq, c, s.t_max, &tmin)) hitmask |= 1u << c;
+  }
+  hitmask &= n.present;
+  if (s.sp + __popc(hitmask) > ARGENT_STACK_SIZE) {
+    atomicOr(status, ARGENT_STATUS_STACK_OVERFLOW);
+    s.sp = 0;
+    return ARGENT_ANY_CLEAR;
+  }
+  while (hitmask) {
+    int c = __ffs(hitmask) - 1;
+    hitmask &= hitmask - 1u;
+    stack[s.sp++] = child_ref(n, c);
+  }
+  return s.sp == 0 ? ARGENT_ANY_CLEAR : ARGENT_ANY_RUNNING;
+}
+
+__device__ __noinline__ bool trace_any(const DevPiece& pc, V3 o, V3 d, float t_max, uint32_t* status) {
+  AnyTrav s;
+  uint32_t stack[ARGENT_STACK_SIZE];
+  int r = any_begin(pc, s, stack, o, d, t_max);
+  while (r == ARGENT_ANY_RUNNING) r = any_step(pc, s, stack, status);
+  count_visits(3, s.n_nodes, s.n_tris);
+  return r == ARGENT_ANY_HIT;
 }
 
 }  // namespace dev

@@ -146,6 +146,8 @@ struct ArgentCtx {
   bool tables_ready = false;
   WaveBuffers wave[ARGENT_LANES];
   KernelProfile prof;
+  float* resolve = nullptr;  // film-read staging (grown on demand)
+  size_t resolve_floats = 0;
 };
 
 struct ArgentPiece {

@@ -338,34 +338,75 @@ __device__ __forceinline__ void warp_append(bool pred, uint32_t value, uint32_t*
   }
 }
 
-// scene.rs:169-218: closest hit of every active path, then the path is
-// queued for the shading kernel of its hit's material class.
-__global__ void __launch_bounds__(128) k_intersect(WaveArgs a, int depth) {
-  uint32_t count = a.counters[CNT_ACT(depth)];
+// Persistent-lane work fetch, shared by k_intersect and k_shadow: a warp
+// keeps each lane on one queue entry and, when at least ARGENT_REFILL lanes
+// are idle (or all are), hands them the next entries in one atomic.  The
+// warp's first 32 entries are fixed by its index in the grid, as in
+// warp_first_batch.  Returns the queue index given to this lane (or ~0u)
+// and clears *more once the queue has run out; the decisions are
+// warp-uniform.
+#define ARGENT_REFILL 8
+__device__ __forceinline__ uint32_t lane_refill(bool idle, bool* first, bool* more, uint32_t count, uint32_t* work) {
+  const unsigned lane = threadIdx.x & 31;
+  unsigned need = __ballot_sync(0xffffffffu, idle);
+  if (!*more || need == 0 || (!*first && __popc(need) < ARGENT_REFILL && need != 0xffffffffu)) return ~0u;
+  uint32_t b;
+  if (*first) {
+    b = warp_first_batch();
+    *first = false;
+  } else {
+    uint32_t t = 0;
+    if (lane == 0) t = atomicAdd(work, (uint32_t)__popc(need));
+    b = __shfl_sync(0xffffffffu, t, 0) + gridDim.x * blockDim.x;
+  }
+  if (b + (uint32_t)__popc(need) >= count) *more = false;
+  if (!idle) return ~0u;
+  uint32_t j = b + (uint32_t)__popc(need & ((1u << lane) - 1u));
+  return j < count ? j : ~0u;
+}
+
+// scene.rs:169-218: closest hit of every active path (piece BVH in object
+// space, then panels, then floor), then the path is queued for the shading
+// kernel of its hit's material class.  Persistent lanes step their BVH
+// traversals one node or leaf at a time and take a new path as soon as
+// theirs is done.
+__global__ void __launch_bounds__(128, 8) k_intersect(WaveArgs a, int depth) {
+  const uint32_t count = a.counters[CNT_ACT(depth)];
   uint32_t* work = a.counters + CNT_WORK(CNT_ACT(depth));
-  for (uint32_t base = warp_first_batch(); base < count; base = warp_next_batch(work)) {
-    uint32_t i = base + (threadIdx.x & 31);
+  uint2 stack[ARGENT_STACK_SIZE];
+  ClosestTrav s;
+  const DevScene* sc = nullptr;
+  uint32_t slot = 0;
+  bool active = false, running = false, first = true, more = true;
+  for (;;) {
+    uint32_t j = lane_refill(!active, &first, &more, count, work);
+    if (j != ~0u) {
+      slot = a.q_in[j];
+      sc = a.jobs[a.meta[slot].w >> 16].scene;
+      float4 of = a.o[slot], df = a.d[slot];
+      V3 oo{of.x, of.y, of.z}, od{df.x, df.y, df.z};
+      if (sc->has_turn) {
+        oo = rot_y_sc(oo, sc->to_obj_s, sc->to_obj_c);
+        od = rot_y_sc(od, sc->to_obj_s, sc->to_obj_c);
+      }
+      running = closest_begin(sc->piece, s, oo, od, INFINITY);
+      active = true;
+    }
+    if (__ballot_sync(0xffffffffu, active) == 0 && !more) break;
+    if (active && running) running = !closest_step(sc->piece, s, stack, a.status);
+    bool fin = active && !running;
     int cls = -1;
-    uint32_t slot = 0;
-    if (i < count) {
-      slot = a.q_in[i];
-      uint32_t job_id = a.meta[slot].w >> 16;
-      const DevScene* sc = a.jobs[job_id].scene;
+    if (fin) {
+      count_visits(0, s.n_nodes, s.n_tris);
       float4 of = a.o[slot], df = a.d[slot];
       V3 o{of.x, of.y, of.z}, d{df.x, df.y, df.z};
       float t_max = INFINITY;
       float4 rec = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(HIT_MISS));
-      V3 oo = o, od = d;
-      if (sc->has_turn) {
-        oo = rot_y_sc(o, sc->to_obj_s, sc->to_obj_c);
-        od = rot_y_sc(d, sc->to_obj_s, sc->to_obj_c);
-      }
-      TraceHit h = trace_closest(sc->piece, oo, od, INFINITY, a.status);
       cls = CLS_TERMINAL;
-      if (h.prim != ARGENT_NO_HIT_U) {
-        t_max = h.t;
-        rec = make_float4(h.t, h.u, h.v, __uint_as_float(h.prim));
-        cls = sc->mat_class[__ldg(&sc->piece.tri_idx[h.prim].w)];
+      if (s.best.prim != ARGENT_NO_HIT_U) {
+        t_max = s.best.t;
+        rec = make_float4(s.best.t, s.best.u, s.best.v, __uint_as_float(s.best.prim));
+        cls = sc->mat_class[__ldg(&sc->piece.tri_idx[s.best.prim].w)];
       }
       for (int p = 0; p < sc->num_panels; ++p) {
         const DevPanel& pn = sc->panels[p];
@@ -385,10 +426,13 @@ __global__ void __launch_bounds__(128) k_intersect(WaveArgs a, int depth) {
         }
       }
       a.hit[slot] = rec;
+      active = false;
     }
+    if (__ballot_sync(0xffffffffu, fin)) {
 #pragma unroll
-    for (int c = 0; c < NUM_CLS; ++c)
-      warp_append(cls == c, slot, a.counters + CNT_CLS(depth, c), a.qc + (size_t)c * a.cap, a.cap, a.status);
+      for (int c = 0; c < NUM_CLS; ++c)
+        warp_append(cls == c, slot, a.counters + CNT_CLS(depth, c), a.qc + (size_t)c * a.cap, a.cap, a.status);
+    }
   }
 }
 
@@ -751,22 +795,40 @@ __global__ void __launch_bounds__(128, CLS == CLS_TERMINAL ? 1 : 4) k_shade(Wave
   }
 }
 
-__global__ void __launch_bounds__(128) k_shadow(WaveArgs a, int depth) {
-  uint32_t count = a.counters[CNT_SH(depth)];
+// scene.rs:123-140 (piece part): any hit of the piece for each shadow ray;
+// unoccluded rays add their contribution to L.  Persistent lanes, so a
+// lane whose ray ends early takes a new one instead of idling until the
+// slowest ray of its warp ends.
+__global__ void __launch_bounds__(128, 8) k_shadow(WaveArgs a, int depth) {
+  const uint32_t count = a.counters[CNT_SH(depth)];
   uint32_t* work = a.counters + CNT_WORK(CNT_SH(depth));
-  for (uint32_t base = warp_first_batch(); base < count; base = warp_next_batch(work)) {
-    uint32_t i = base + (threadIdx.x & 31);
-    if (i < count) {
-      float4 so = a.sh_o[i], sd = a.sh_d[i];
+  uint32_t stack[ARGENT_STACK_SIZE];
+  AnyTrav s;
+  const DevScene* sc = nullptr;
+  uint32_t idx = 0;
+  int state = ARGENT_ANY_CLEAR;
+  bool active = false, first = true, more = true;
+  for (;;) {
+    uint32_t j = lane_refill(!active, &first, &more, count, work);
+    if (j != ~0u) {
+      idx = j;
+      float4 so = __ldcs(a.sh_o + j), sd = __ldcs(a.sh_d + j);
       uint32_t slot = __float_as_uint(sd.w);
-      uint32_t job_id = a.meta[slot].w >> 16;
-      const DevScene* sc = a.jobs[job_id].scene;
-      bool occ = trace_any(sc->piece, V3{so.x, so.y, so.z}, V3{sd.x, sd.y, sd.z}, so.w, a.status);
-      if (!occ) {
-        float4 c = a.sh_c[i];
+      sc = a.jobs[a.meta[slot].w >> 16].scene;
+      state = any_begin(sc->piece, s, stack, V3{so.x, so.y, so.z}, V3{sd.x, sd.y, sd.z}, so.w);
+      active = true;
+    }
+    if (__ballot_sync(0xffffffffu, active) == 0 && !more) break;
+    if (active && state == ARGENT_ANY_RUNNING) state = any_step(sc->piece, s, stack, a.status);
+    if (active && state != ARGENT_ANY_RUNNING) {
+      count_visits(3, s.n_nodes, s.n_tris);
+      if (state == ARGENT_ANY_CLEAR) {
+        uint32_t slot = __float_as_uint(__ldcs(a.sh_d + idx).w);
+        float4 c = __ldcs(a.sh_c + idx);
         float4 l = a.L[slot];
         a.L[slot] = make_float4(l.x + c.x, l.y + c.y, l.z + c.z, l.w + c.w);
       }
+      active = false;
     }
   }
 }

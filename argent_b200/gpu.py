@@ -109,6 +109,29 @@ class Piece:
     def device_bytes(self):
         return int(self.ctx.lib.argent_piece_device_bytes(self.h))
 
+    def ambient_occlusion(self, normals, samples=48, distance=1.2):
+        """cavity::ambient_occlusion (argent-mesh cavity.rs:96-135) on the
+        device, for the mesh this piece was uploaded from."""
+        m = self.mesh
+        fp = ctypes.POINTER(ctypes.c_float)
+        n = np.ascontiguousarray(normals, np.float32)
+        out = np.zeros(len(m.positions), np.float32)
+        self.ctx.check(self.ctx.lib.argent_piece_ambient_occlusion(
+            self.ctx.h, self.h, _p(m.positions, fp), _p(n, fp), len(m.positions), samples, distance, _p(out, fp)))
+        return out
+
+    def patina_mask(self, settings=None):
+        """cavity::patina_mask (cavity.rs:52-78) of the uploaded mesh; pass
+        the result as Mesh.cavity to upload a piece with its mask."""
+        m = self.mesh
+        s = settings if settings is not None else N.ArgentPatinaSettings(48, 1.2, 0.4, 0.35, 3)
+        fp = ctypes.POINTER(ctypes.c_float)
+        out = np.zeros(len(m.positions), np.float32)
+        self.ctx.check(self.ctx.lib.argent_piece_patina_mask(
+            self.ctx.h, self.h, _p(m.positions, fp), _p(m.normals, fp), len(m.positions), _p(m.tris, N.c_u32_p),
+            len(m.tris), ctypes.byref(s), _p(out, fp)))
+        return out
+
     def trace_closest(self, rays: np.ndarray) -> np.ndarray:
         """rays: (n, 8) float32 [ox oy oz tmax dx dy dz pad] -> hits (n, 4)
         float32 [t u v prim-bits]."""
@@ -186,6 +209,13 @@ class Film:
         fp = ctypes.POINTER(ctypes.c_float)
         self.ctx.check(self.ctx.lib.argent_film_read(self.h, _p(c, fp), None, None))
         return c
+
+    def denoised(self):
+        """The colour denoised on the device with the film's albedo and
+        normal guides (argent-post's à-trous backend)."""
+        out = np.zeros((self.height, self.width, 3), np.float32)
+        self.ctx.check(self.ctx.lib.argent_film_denoise(self.h, _p(out, ctypes.POINTER(ctypes.c_float))))
+        return out
 
     def xyz(self):
         x = np.zeros((self.height, self.width, 3), np.float32)
@@ -287,3 +317,16 @@ class Serve:
 
     def now(self):
         return float(self.ctx.lib.argent_serve_now(self.h))
+
+
+def denoise_atrous(ctx: Context, color, albedo=None, normal=None):
+    """argent-post's `denoise(.., DenoiseBackend::Atrous)` on the device:
+    (h, w, 3) float32 images in, the denoised colour out."""
+    fp = ctypes.POINTER(ctypes.c_float)
+    c = np.ascontiguousarray(color, np.float32)
+    a = None if albedo is None else np.ascontiguousarray(albedo, np.float32)
+    n = None if normal is None else np.ascontiguousarray(normal, np.float32)
+    out = np.zeros_like(c)
+    h, w = c.shape[0], c.shape[1]
+    ctx.check(ctx.lib.argent_denoise_atrous(ctx.h, w, h, _p(c, fp), _p(a, fp), _p(n, fp), _p(out, fp)))
+    return out

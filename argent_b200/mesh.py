@@ -81,3 +81,41 @@ def gem_ring(shank_nu=768, shank_nv=440, center_mm=2.0, stone_mm=0.75, seed=4) -
     if rc != N.OK:
         raise N.ArgentError(rc, "argent_synth_gem_ring failed")
     return _take(m)
+
+
+# ---------------------------------------------------------------- argent-mesh helpers (host)
+
+def smooth_normals(m: Mesh) -> np.ndarray:
+    """normals::smooth_vertex_normals (argent-mesh normals.rs:226-242)."""
+    out = np.zeros_like(m.positions)
+    fp = ctypes.POINTER(ctypes.c_float)
+    N.check(N.gpu().argent_mesh_smooth_normals(m.positions.ctypes.data_as(fp), len(m.positions),
+                                               m.tris.ctypes.data_as(N.c_u32_p), len(m.tris), out.ctypes.data_as(fp)))
+    return out
+
+
+def concavity(m: Mesh, normals, radius) -> np.ndarray:
+    """cavity::concavity (argent-mesh cavity.rs:137-236)."""
+    n = np.ascontiguousarray(normals, np.float32)
+    out = np.zeros(len(m.positions), np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    N.check(N.gpu().argent_mesh_concavity(m.positions.ctypes.data_as(fp), len(m.positions), n.ctypes.data_as(fp),
+                                          m.tris.ctypes.data_as(N.c_u32_p), len(m.tris), radius,
+                                          out.ctypes.data_as(fp)))
+    return out
+
+
+def smooth(m: Mesh, values, iterations, lam=0.5) -> np.ndarray:
+    """cavity::smooth (argent-mesh cavity.rs:241-299)."""
+    v = np.array(values, np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    N.check(N.gpu().argent_mesh_smooth(m.positions.ctypes.data_as(fp), len(m.positions),
+                                       m.tris.ctypes.data_as(N.c_u32_p), len(m.tris), v.ctypes.data_as(fp),
+                                       iterations, lam))
+    return v
+
+
+def patina_settings(radius):
+    """Prepared::build's PatinaSettings (core/src/shot.rs:137-141)."""
+    return N.ArgentPatinaSettings(48, float(min(max(radius * 0.09, 0.4), 2.5)),
+                                  float(min(max(radius * 0.03, 0.15), 1.0)), 0.35, 3)

@@ -128,8 +128,9 @@ def peaks():
 
 
 def ncu_traffic():
-    """dram read+write bytes per launch of the dominant kernel, from the
-    committed ncu summary (profiles/ncu_traffic.json), or None."""
+    """DRAM read+write bytes per ray of the traversal kernel and its issue
+    activity, from one ncu capture summarised in profiles/ncu_traffic.json
+    (the capture's command is in that file), or None."""
     try:
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
             return json.load(f)
@@ -474,14 +475,23 @@ def run_gpu(args, world, rank, device):
     # hit attributes (index 16 B + 3 positions + 3 normals 96 B), spectral tables (~64 B)
     per_sample["shade"] = rays_c * (152 + 112 + 112 + 64)
     per_sample["raygen"] = 176.0
+    # The same traversal in argent's layout (128 B Node4, 48 B Tri); argent's
+    # 4-wide tree visits more nodes, so this understates its bytes.
+    per_sample_ref = {
+        "intersect": (counts["closest_nodes"] * 128 + counts["closest_tris"] * 48) / px + rays_c * (32 + 16 + 16 + 4),
+        "shadow": (counts["any_nodes"] * 128 + counts["any_tris"] * 48) / px + rays_a * (48 + 16 + 16)}
     per_sample["film"] = 64.0 + 12.0 * 3 / max(plan.config()["spp"], 1)
     alg_bytes_total = per_sample[dom] * path_samples_timed
     achieved = alg_bytes_total / (dom_ms / 1000.0) / 1e9  # GB/s
     peak, peak_kind = peaks()
-    traffic = None
+    # DRAM traffic per average launch: bytes per ray from the committed ncu
+    # capture (profiles/ncu_traffic.json) times this run's rays per launch.
+    traffic, issue = None, None
     tr = ncu_traffic()
-    if tr and tr.get("kernel") == dom and tr.get("workload") == plan.name:
-        traffic = tr.get("dram_bytes_per_launch")
+    if tr and tr.get("kernel") == f"k_{dom}" and tr.get("workload") == plan.name and dom in ("intersect", "shadow"):
+        rays = rays_c if dom == "intersect" else rays_a
+        traffic = tr["dram_bytes_per_ray"] * rays * path_samples_timed / max(dom_n, 1)
+        issue = tr.get("issue_active_pct")
 
     # End-to-end through the C ABI with host buffers.
     e2e_value = None
@@ -529,6 +539,8 @@ def run_gpu(args, world, rank, device):
                          "frac": achieved / peak, "traffic": traffic, "kernel": f"k_{dom}",
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "alg_bytes_per_path_sample": per_sample[dom],
+                         "alg_bytes_per_path_sample_argent_layout": per_sample_ref.get(dom),
+                         "issue_active_pct": issue,
                          "launches": dom_n, "avg_launch_ms": dom_ms / max(dom_n, 1)},
             "kernel_ms": {k: round(v[0], 3) for k, v in kt.items()},
             "traversal_per_path_sample": {k: v / px for k, v in counts.items()},

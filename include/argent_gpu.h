@@ -338,6 +338,70 @@ int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n
 uint64_t argent_ctx_kernel_launches(const ArgentCtx* ctx);
 
 /* ------------------------------------------------------------------ */
+/* Denoise (argent-post denoise.rs, the built-in à-trous backend).    */
+/* ------------------------------------------------------------------ */
+
+/*
+ * argent's à-trous denoiser (argent-post/src/denoise.rs:535-712: 5 passes
+ * of the 5x5 B3 kernel with holes 1..16, luminance edge stopping against a
+ * per-pixel noise estimate, normal weight max(0, n.n')^128, albedo weight
+ * exp(-|da|^2 / 0.01), albedo demodulation) on the device.  color, albedo,
+ * normal and out are width*height*3 floats in host memory; albedo and
+ * normal may be NULL (a normal without an albedo is ignored, as with argent's
+ * OIDN path).  Replaces `denoise(.., DenoiseBackend::Atrous)`.
+ */
+int argent_denoise_atrous(ArgentCtx* ctx, uint32_t width, uint32_t height, const float* color, const float* albedo,
+                          const float* normal, float* out);
+/* The film's colour denoised with its albedo and normal guides, without the
+ * averages leaving the device (the `render_image` hand-off, shot.rs:424-444);
+ * out receives width*height*3 floats of camera RGB. */
+int argent_film_denoise(ArgentFilm* film, float* out);
+
+/* ------------------------------------------------------------------ */
+/* Cavity mask (argent-mesh cavity.rs), the patina input of `Piece`.  */
+/* ------------------------------------------------------------------ */
+
+/* `PatinaSettings` (argent-mesh/src/cavity.rs:24-42).  argent's defaults:
+ * 48 samples, ao_distance 1.2 mm, curvature_radius 0.4 mm, concavity_weight
+ * 0.35, 3 smoothing passes; `Prepared::build` scales the two distances by
+ * the piece radius (core/src/shot.rs:137-141). */
+typedef struct ArgentPatinaSettings {
+  uint32_t ao_samples;
+  float ao_distance;
+  float curvature_radius;
+  float concavity_weight;
+  uint32_t smooth_iterations;
+} ArgentPatinaSettings;
+
+/*
+ * Fraction of `samples` cosine-weighted hemisphere rays per vertex blocked
+ * within `distance` (cavity::ambient_occlusion, cavity.rs:96-135), traced on
+ * the device against the uploaded piece.  positions/normals are the nv
+ * vertices the piece was uploaded with (normals already chosen: the mesh's,
+ * or argent_mesh_smooth_normals); ao receives nv floats.
+ */
+int argent_piece_ambient_occlusion(ArgentCtx* ctx, ArgentPiece* piece, const float* positions, const float* normals,
+                                   uint32_t nv, uint32_t samples, float distance, float* ao);
+/*
+ * cavity::patina_mask (cavity.rs:52-78): device AO, host concavity and
+ * Laplacian smoothing, then the contrast blend; mask receives nv values in
+ * [0, 1] for `argent_piece_upload`'s cavity argument.  normals may be NULL
+ * (smooth vertex normals, cavity.rs:80-86).  The mesh must be the one the
+ * piece was uploaded from.
+ */
+int argent_piece_patina_mask(ArgentCtx* ctx, ArgentPiece* piece, const float* positions, const float* normals,
+                             uint32_t nv, const uint32_t* tris, uint32_t nt, const ArgentPatinaSettings* settings,
+                             float* mask);
+/* Host helpers with argent-mesh's public semantics (no device needed):
+ * normals::smooth_vertex_normals (normals.rs:226-242), cavity::concavity
+ * (cavity.rs:137-236) and cavity::smooth (cavity.rs:241-299). */
+int argent_mesh_smooth_normals(const float* positions, uint32_t nv, const uint32_t* tris, uint32_t nt, float* out);
+int argent_mesh_concavity(const float* positions, uint32_t nv, const float* normals, const uint32_t* tris, uint32_t nt,
+                          float radius, float* out);
+int argent_mesh_smooth(const float* positions, uint32_t nv, const uint32_t* tris, uint32_t nt, float* values,
+                       uint32_t iterations, float lambda);
+
+/* ------------------------------------------------------------------ */
 /* Serving: continuous batching of render requests.                   */
 /* ------------------------------------------------------------------ */
 

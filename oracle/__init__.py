@@ -66,6 +66,12 @@ def lib():
             "oracle_sampler_random": (None, [u32, u32, u32, fp]),
             "oracle_sobol_4d": (None, [u32, u32, u32, fp]),
             "oracle_sobol_raw": (None, [u32, ctypes.c_int, ctypes.POINTER(u32)]),
+            "oracle_smooth_vertex_normals": (None, [vp, u32, vp, u32, vp]),
+            "oracle_ambient_occlusion": (None, [vp, u32, vp, vp, u32, u32, f, vp]),
+            "oracle_concavity": (None, [vp, u32, vp, vp, u32, f, vp]),
+            "oracle_smooth": (None, [vp, u32, vp, u32, vp, u32, f]),
+            "oracle_patina_mask": (None, [vp, u32, vp, vp, u32, u32, f, f, f, u32, vp]),
+            "oracle_atrous": (None, [u32, u32, vp, vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -154,3 +160,63 @@ class Scene:
         lib().oracle_render_pass(self.h, ctypes.byref(cam), ctypes.byref(settings), w, h, first, count, seed, y0, y1,
                                  _ptr(color), _ptr(albedo), _ptr(normal), _ptr(xyz), threads)
         return color, albedo, normal, xyz
+
+
+# ---------------------------------------------------------------- cavity mask (argent-mesh cavity.rs)
+
+def _mesh_arrays(mesh):
+    p = np.ascontiguousarray(mesh.positions, np.float32)
+    t = np.ascontiguousarray(mesh.tris, np.uint32)
+    return p, t
+
+
+def smooth_vertex_normals(mesh):
+    p, t = _mesh_arrays(mesh)
+    out = np.zeros_like(p)
+    lib().oracle_smooth_vertex_normals(_ptr(p), len(p), _ptr(t), len(t), _ptr(out))
+    return out
+
+
+def ambient_occlusion(mesh, normals, samples=48, distance=1.2):
+    p, t = _mesh_arrays(mesh)
+    n = np.ascontiguousarray(normals, np.float32)
+    out = np.zeros(len(p), np.float32)
+    lib().oracle_ambient_occlusion(_ptr(p), len(p), _ptr(n), _ptr(t), len(t), samples, distance, _ptr(out))
+    return out
+
+
+def concavity(mesh, normals, radius):
+    p, t = _mesh_arrays(mesh)
+    n = np.ascontiguousarray(normals, np.float32)
+    out = np.zeros(len(p), np.float32)
+    lib().oracle_concavity(_ptr(p), len(p), _ptr(n), _ptr(t), len(t), radius, _ptr(out))
+    return out
+
+
+def smooth(mesh, values, iterations, lam=0.5):
+    p, t = _mesh_arrays(mesh)
+    v = np.array(values, np.float32)
+    lib().oracle_smooth(_ptr(p), len(p), _ptr(t), len(t), _ptr(v), iterations, lam)
+    return v
+
+
+def patina_mask(mesh, normals=None, ao_samples=48, ao_distance=1.2, curvature_radius=0.4, concavity_weight=0.35,
+                smooth_iterations=3):
+    """cavity.rs:52-78 with PatinaSettings' defaults (cavity.rs:38-42)."""
+    p, t = _mesh_arrays(mesh)
+    n = None if normals is None else np.ascontiguousarray(normals, np.float32)
+    out = np.zeros(len(p), np.float32)
+    lib().oracle_patina_mask(_ptr(p), len(p), _ptr(n), _ptr(t), len(t), ao_samples, ao_distance, curvature_radius,
+                             concavity_weight, smooth_iterations, _ptr(out))
+    return out
+
+
+def atrous(color, albedo=None, normal=None):
+    """argent-post's built-in à-trous denoiser (denoise.rs:653-712) on
+    (h, w, 3) float32 images."""
+    c = np.ascontiguousarray(color, np.float32)
+    a = None if albedo is None else np.ascontiguousarray(albedo, np.float32)
+    n = None if normal is None else np.ascontiguousarray(normal, np.float32)
+    out = np.zeros_like(c)
+    lib().oracle_atrous(c.shape[1], c.shape[0], _ptr(c), _ptr(a), _ptr(n), _ptr(out))
+    return out

@@ -48,6 +48,21 @@ void oracle_trace_sample(const oracle_scene* sc, const ArgentCamera* cam, const 
                          uint32_t h, uint32_t x, uint32_t y, uint32_t si, uint32_t seed, float* xyz_out);
 void oracle_camera_matrix(int has_white, const float* white, float* out9);
 
+/* Cavity mask (argent-mesh cavity.rs; AO on argent's BVH) */
+void oracle_smooth_vertex_normals(const float* pos, uint32_t nv, const uint32_t* tris, uint32_t nt, float* out);
+void oracle_ambient_occlusion(const float* pos, uint32_t nv, const float* normals, const uint32_t* tris, uint32_t nt,
+                              uint32_t samples, float distance, float* out);
+void oracle_concavity(const float* pos, uint32_t nv, const float* normals, const uint32_t* tris, uint32_t nt,
+                      float radius, float* out);
+void oracle_smooth(const float* pos, uint32_t nv, const uint32_t* tris, uint32_t nt, float* values,
+                   uint32_t iterations, float lambda);
+void oracle_patina_mask(const float* pos, uint32_t nv, const float* normals, const uint32_t* tris, uint32_t nt,
+                        uint32_t ao_samples, float ao_distance, float curvature_radius, float concavity_weight,
+                        uint32_t smooth_iterations, float* out);
+
+/* À-trous denoiser (argent-post denoise.rs:535-712); albedo/normal may be NULL */
+void oracle_atrous(uint32_t w, uint32_t h, const float* color, const float* albedo, const float* normal, float* out);
+
 /* Primitives, for argent's unit-test known answers */
 float oracle_fresnel_dielectric(float c, float eta);
 float oracle_fresnel_conductor(float c, float eta, float k);
