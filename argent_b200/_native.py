@@ -92,7 +92,8 @@ class ArgentHit(ctypes.Structure):
 
 
 class ArgentLimits(ctypes.Structure):
-    _fields_ = [("wave_paths", ctypes.c_uint64), ("memory_budget", ctypes.c_uint64)]
+    _fields_ = [("wave_paths", ctypes.c_uint64), ("memory_budget", ctypes.c_uint64), ("lanes", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 class ArgentBatchItem(ctypes.Structure):
@@ -120,10 +121,24 @@ class ArgentServeStatus(ctypes.Structure):
 REQ_QUEUED, REQ_ACTIVE, REQ_DONE, REQ_CANCELLED, REQ_FAILED = range(5)
 
 
+class ArgentGrade(ctypes.Structure):
+    _fields_ = [("exposure_ev", ctypes.c_float), ("tonemap", ctypes.c_int32), ("look", ctypes.c_int32),
+                ("saturation", ctypes.c_float)]
+
+
+TM_AGX, TM_ACES, TM_KHRONOS, TM_REINHARD, TM_CLAMP = range(5)
+AGX_BASE, AGX_PUNCHY, AGX_GOLDEN = range(3)
+
+
 class ArgentPatinaSettings(ctypes.Structure):
     _fields_ = [("ao_samples", ctypes.c_uint32), ("ao_distance", ctypes.c_float),
                 ("curvature_radius", ctypes.c_float), ("concavity_weight", ctypes.c_float),
                 ("smooth_iterations", ctypes.c_uint32)]
+
+
+class ArgentTuneResult(ctypes.Structure):
+    _fields_ = [("lanes", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("wave_paths", ctypes.c_uint64),
+                ("path_samples_per_s", ctypes.c_double)]
 
 
 class ArgentMesh(ctypes.Structure):
@@ -141,6 +156,9 @@ GPU_FUNCS = {
     "argent_ctx_kernel_launches": (ctypes.c_uint64, [ctypes.c_void_p]),
     "argent_piece_upload": (ctypes.c_int, [ctypes.c_void_p, c_float_p, ctypes.c_uint32, c_float_p, c_u32_p,
                                            ctypes.c_uint32, c_u16_p, c_float_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "argent_piece_upload_device_bvh": (ctypes.c_int, [ctypes.c_void_p, c_float_p, ctypes.c_uint32, c_float_p,
+                                                      c_u32_p, ctypes.c_uint32, c_u16_p, c_float_p,
+                                                      ctypes.POINTER(ctypes.c_void_p)]),
     "argent_piece_destroy": (None, [ctypes.c_void_p]),
     "argent_piece_bounds": (ctypes.c_int, [ctypes.c_void_p, c_float_p, c_float_p]),
     "argent_piece_device_bytes": (ctypes.c_uint64, [ctypes.c_void_p]),
@@ -167,6 +185,12 @@ GPU_FUNCS = {
     "argent_trace_anyhit_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                   ctypes.c_uint64, ctypes.c_void_p]),
     "argent_render_batch": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ArgentBatchItem), ctypes.c_uint32]),
+    "argent_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ArgentCamera),
+                                       ctypes.POINTER(ArgentPathSettings), ctypes.c_uint32, ctypes.c_uint32,
+                                       ctypes.c_uint32, ctypes.POINTER(ArgentTuneResult), ctypes.c_uint32,
+                                       ctypes.POINTER(ctypes.c_uint32)]),
+    "argent_ctx_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
+                                         ctypes.POINTER(ctypes.c_uint64)]),
     "argent_trace_closest_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_uint64, ctypes.c_void_p]),
     "argent_ctx_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -178,6 +202,10 @@ GPU_FUNCS = {
     "argent_denoise_atrous": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, c_float_p, c_float_p,
                                              c_float_p, c_float_p]),
     "argent_film_denoise": (ctypes.c_int, [ctypes.c_void_p, c_float_p]),
+    "argent_develop": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, c_float_p,
+                                      ctypes.POINTER(ArgentGrade), ctypes.c_void_p]),
+    "argent_film_develop": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ArgentGrade), ctypes.c_int,
+                                           ctypes.c_void_p]),
     "argent_piece_ambient_occlusion": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, c_float_p, c_float_p,
                                                       ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, c_float_p]),
     "argent_piece_patina_mask": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, c_float_p, c_float_p,

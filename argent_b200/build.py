@@ -29,6 +29,7 @@ GPU_SOURCES = [
     os.path.join(CSRC, "host", "scene_prep.cpp"),
     os.path.join(CSRC, "host", "serve.cpp"),
     os.path.join(CSRC, "host", "cavity.cpp"),
+    os.path.join(CSRC, "host", "develop.cpp"),
 ]
 HOST_SOURCES = [
     os.path.join(CSRC, "host", "synth.cpp"),

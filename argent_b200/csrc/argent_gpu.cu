@@ -1,6 +1,7 @@
 // argent_gpu.cu — the C ABI of include/argent_gpu.h: context, piece, scene,
 // film, render_pass, batch and traversal entry points.  Kernels live in the
 // device/*.cuh headers included here.
+#include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -22,6 +23,9 @@
 #include "internal.cuh"
 #include "render_impl.cuh"
 #include "denoise.cuh"
+#include "develop.cuh"
+#include "device_build.cuh"
+#include "host/develop.h"
 
 using namespace dev;
 
@@ -219,15 +223,20 @@ int argent_ctx_create(int device, const ArgentLimits* limits, ArgentCtx** out) {
   ArgentCtx* ctx = new ArgentCtx();
   ctx->device = device;
   if (limits) ctx->limits = *limits;
-  if (ctx->limits.wave_paths == 0) ctx->limits.wave_paths = 1ull << 21;
+  if (ctx->limits.wave_paths == 0) ctx->limits.wave_paths = 1ull << 23;
+  if (ctx->limits.wave_paths > (1ull << 30) || ctx->limits.lanes > ARGENT_LANES) {
+    delete ctx;
+    return set_error(nullptr, ARGENT_E_INVALID, "wave_paths above 2^30 or more than 16 lanes");
+  }
+  ctx->lanes = ctx->limits.lanes ? (int)ctx->limits.lanes : 8;
   cudaError_t r = cudaSetDevice(device);
   if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   ctx->lane_stream[0] = ctx->stream;
-  for (int l = 1; l < ARGENT_LANES && r == cudaSuccess; ++l)
+  for (int l = 1; l < ctx->lanes && r == cudaSuccess; ++l)
     r = cudaStreamCreateWithFlags(&ctx->lane_stream[l], cudaStreamNonBlocking);
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming);
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming);
-  for (int l = 0; l < ARGENT_LANES && r == cudaSuccess; ++l)
+  for (int l = 0; l < ctx->lanes && r == cudaSuccess; ++l)
     r = cudaEventCreateWithFlags(&ctx->film_ev[l], cudaEventDisableTiming);
   if (r == cudaSuccess) r = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (r == cudaSuccess) r = cudaMalloc(&ctx->d_status, sizeof(uint32_t) * 4);
@@ -344,6 +353,213 @@ int argent_piece_upload(ArgentCtx* ctx, const float* positions, uint32_t nv, con
   }
   p->dev.nodes = (const uint4*)dn;
   p->dev.tris = (const float4*)dt;
+  p->dev.pos = (const float4*)dp;
+  p->dev.nrm = (const float4*)dnr;
+  p->dev.tri_idx = (const uint4*)di;
+  p->dev.cavity = (const float*)dc;
+  p->dev.num_tris = nt;
+  *out = p;
+  return ARGENT_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Stream-ordered temporaries of one device build, freed together.
+struct BuildTemps {
+  cudaStream_t st;
+  std::vector<void*> ptrs;
+  cudaError_t err = cudaSuccess;
+  template <class T>
+  T* get(size_t count) {
+    void* p = nullptr;
+    if (err == cudaSuccess) err = cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), st);
+    if (err == cudaSuccess) ptrs.push_back(p);
+    return (T*)p;
+  }
+  ~BuildTemps() {
+    for (void* p : ptrs) cudaFreeAsync(p, st);
+  }
+};
+
+// Builds the 8-wide BVH of the piece's uploaded triangles on the device
+// (device_build.cuh) and stores nodes, triangle records, depth and bounds
+// in `p`.  `tidx` holds the piece's triangles (x, y, z = vertex indices).
+std::string device_bvh(ArgentCtx* ctx, ArgentPiece* p, const float4* pos, const uint4* tidx, uint32_t nt) {
+  cudaStream_t st = ctx->stream;
+  const size_t n = nt, nb = 2 * n - 1;
+  BuildTemps tmp{st};
+  const uint32_t tpb = 256;
+  const uint32_t nblk = (uint32_t)std::min<size_t>((n + tpb - 1) / tpb, (size_t)148 * 8);
+  float* tlo = tmp.get<float>(3 * n);
+  float* thi = tmp.get<float>(3 * n);
+  float* cen = tmp.get<float>(3 * n);
+  float* blo = tmp.get<float>(3 * (size_t)nblk);
+  float* bhi = tmp.get<float>(3 * (size_t)nblk);
+  uint64_t* k0 = tmp.get<uint64_t>(n);
+  uint64_t* k1 = tmp.get<uint64_t>(n);
+  uint32_t* v0 = tmp.get<uint32_t>(n);
+  uint32_t* v1 = tmp.get<uint32_t>(n);
+  db::Bin bn;
+  bn.lo = tmp.get<float>(3 * nb);
+  bn.hi = tmp.get<float>(3 * nb);
+  bn.first = tmp.get<uint32_t>(nb);
+  bn.last = tmp.get<uint32_t>(nb);
+  bn.left = tmp.get<int32_t>(nb);
+  bn.right = tmp.get<int32_t>(nb);
+  bn.parent = tmp.get<int32_t>(nb);
+  bn.flag = tmp.get<uint32_t>(nb);
+  int2* qa = tmp.get<int2>(n);
+  int2* qb = tmp.get<int2>(n);
+  uint32_t* ctr = tmp.get<uint32_t>(4);  // n_out, node_count, tri_count, err
+  const size_t max_nodes = std::max<size_t>(1, n - 1);
+  uint4* nodes = tmp.get<uint4>(5 * max_nodes);
+  if (tmp.err != cudaSuccess) return std::string("device BVH temporaries: ") + cudaGetErrorString(tmp.err);
+
+  void* dt = nullptr;
+  cudaError_t e = cudaMalloc(&dt, n * sizeof(argent::TriRecord));
+  if (e != cudaSuccess) return std::string("device BVH triangles: ") + cudaGetErrorString(e);
+  p->allocs.push_back(dt);
+  p->bytes += n * sizeof(argent::TriRecord);
+
+  db::k_tri_boxes<<<nblk, tpb, 0, st>>>(pos, tidx, nt, tlo, thi, cen, blo, bhi);
+  const uint32_t grid = nblk;
+  db::k_morton<<<grid, tpb, 0, st>>>(cen, nt, blo, bhi, nblk, k0, v0);
+  size_t sort_bytes = 0;
+  e = cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, k0, k1, v0, v1, (int)n, 0, 63, st);
+  void* sort_tmp = tmp.get<uint8_t>(sort_bytes);
+  if (e == cudaSuccess) e = tmp.err;
+  if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, k0, k1, v0, v1, (int)n, 0, 63, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bn.flag, 0, nb * sizeof(uint32_t), st);
+  if (e != cudaSuccess) return std::string("device BVH sort: ") + cudaGetErrorString(e);
+  ctx->launches += 4;
+  if (n > 1) {
+    db::k_radix_tree<<<grid, tpb, 0, st>>>(k1, nt, bn);
+    ++ctx->launches;
+  }
+  db::k_boxes_up<<<grid, tpb, 0, st>>>(tlo, thi, v1, nt, bn);
+  ++ctx->launches;
+
+  const uint32_t init[4] = {0, 1, 0, 0};
+  const int2 root = make_int2(0, 0);  // wide node 0 <- binary root (internal 0, or leaf 0 when n = 1)
+  e = cudaMemcpyAsync(ctr, init, sizeof(init), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, st);
+  uint32_t n_in = 1, depth = 0;
+  db::Collapse c{};
+  c.n_out = ctr;
+  c.node_count = ctr + 1;
+  c.tri_count = ctr + 2;
+  c.err = ctr + 3;
+  c.nodes = nodes;
+  c.tris = (float4*)dt;
+  c.pos = pos;
+  c.tri = tidx;
+  c.vals = v1;
+  while (e == cudaSuccess && n_in > 0) {
+    if (++depth > 64) return "device BVH collapse did not finish in 64 levels";
+    c.in = qa;
+    c.n_in = n_in;
+    c.out = qb;
+    e = cudaMemsetAsync(ctr, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) break;
+    uint32_t g = (uint32_t)std::min<size_t>((n_in + 127) / 128, (size_t)148 * 16);
+    db::k_collapse<<<g, 128, 0, st>>>(c, bn, nt);
+    ++ctx->launches;
+    e = cudaMemcpyAsync(&n_in, ctr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    std::swap(qa, qb);
+  }
+  uint32_t got[4] = {0, 0, 0, 0};
+  float box[6];
+  if (e == cudaSuccess) e = cudaMemcpyAsync(got, ctr, sizeof(got), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(box, bn.lo, 3 * sizeof(float), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(box + 3, bn.hi, 3 * sizeof(float), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return std::string("device BVH build: ") + cudaGetErrorString(e);
+  if (got[3] & DB_ERR_EXTENT) return "piece extent too large for the node quantisation";
+  if (got[3]) return "device BVH quantisation failed";
+  if (got[2] != nt || got[1] == 0 || got[1] > max_nodes)
+    return "device BVH build lost triangles or nodes";
+  if ((uint64_t)depth * 7 + 1 > ARGENT_STACK_SIZE) return "BVH too deep for the traversal stack";
+
+  void* dn = nullptr;
+  const size_t node_bytes = (size_t)got[1] * sizeof(argent::WideNode);
+  e = cudaMalloc(&dn, node_bytes);
+  if (e != cudaSuccess) return std::string("device BVH nodes: ") + cudaGetErrorString(e);
+  p->allocs.push_back(dn);
+  p->bytes += node_bytes;
+  e = cudaMemcpyAsync(dn, nodes, node_bytes, cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return std::string("device BVH nodes: ") + cudaGetErrorString(e);
+  p->dev.nodes = (const uint4*)dn;
+  p->dev.tris = (const float4*)dt;
+  p->depth = depth;
+  for (int a = 0; a < 3; ++a) {
+    p->lo[a] = box[a];
+    p->hi[a] = box[3 + a];
+  }
+  return "";
+}
+
+}  // namespace
+
+extern "C" {
+
+int argent_piece_upload_device_bvh(ArgentCtx* ctx, const float* positions, uint32_t nv, const float* normals,
+                                   const uint32_t* tris, uint32_t nt, const uint16_t* tri_material,
+                                   const float* cavity, ArgentPiece** out) {
+  if (!ctx || !out) return set_error(ctx, ARGENT_E_INVALID, "argent_piece_upload_device_bvh: NULL argument");
+  *out = nullptr;
+  if ((nv && !positions) || (nt && !tris)) return set_error(ctx, ARGENT_E_INVALID, "piece arrays are NULL");
+  // An empty piece has nothing to build: the host path makes the same empty piece.
+  if (nt == 0) return argent_piece_upload(ctx, positions, nv, normals, tris, nt, tri_material, cavity, out);
+  if (nt >= (1u << 27)) return set_error(ctx, ARGENT_E_INVALID, "device BVH build takes fewer than 2^27 triangles");
+  for (uint64_t i = 0; i < 3ull * nt; ++i)
+    if (tris[i] >= nv) return set_error(ctx, ARGENT_E_INVALID, "triangle index out of range");
+  for (uint64_t i = 0; i < 3ull * nv; ++i)
+    if (!std::isfinite(positions[i])) return set_error(ctx, ARGENT_E_INVALID, "non-finite vertex position");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  ArgentPiece* p = new ArgentPiece();
+  p->ctx = ctx;
+  p->nv = nv;
+  p->nt = nt;
+  std::vector<float4> pos4(nv), nrm4;
+  for (uint32_t i = 0; i < nv; ++i) pos4[i] = make_float4(positions[3 * i], positions[3 * i + 1], positions[3 * i + 2], 0);
+  if (normals) {
+    nrm4.resize(nv);
+    for (uint32_t i = 0; i < nv; ++i) nrm4[i] = make_float4(normals[3 * i], normals[3 * i + 1], normals[3 * i + 2], 0);
+  }
+  std::vector<uint4> tidx(nt);
+  for (uint32_t i = 0; i < nt; ++i)
+    tidx[i] = make_uint4(tris[3 * i], tris[3 * i + 1], tris[3 * i + 2], tri_material ? tri_material[i] : 0u);
+  for (uint32_t i = 0; tri_material && i < nt; ++i) p->max_material = std::max<uint32_t>(p->max_material, tri_material[i]);
+  auto up = [&](const void* src, size_t bytes, void** dst) -> cudaError_t {
+    *dst = nullptr;
+    if (bytes == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(dst, bytes);
+    if (e != cudaSuccess) return e;
+    p->allocs.push_back(*dst);
+    p->bytes += bytes;
+    return cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  };
+  void *dp = nullptr, *dnr = nullptr, *di = nullptr, *dc = nullptr;
+  cudaError_t e = up(pos4.data(), pos4.size() * sizeof(float4), &dp);
+  if (e == cudaSuccess && normals) e = up(nrm4.data(), nrm4.size() * sizeof(float4), &dnr);
+  if (e == cudaSuccess) e = up(tidx.data(), tidx.size() * sizeof(uint4), &di);
+  if (e == cudaSuccess && cavity) e = up(cavity, (size_t)nv * sizeof(float), &dc);
+  if (e != cudaSuccess) {
+    cudaStreamSynchronize(ctx->stream);
+    std::string m = std::string("piece upload: ") + cudaGetErrorString(e);
+    argent_piece_destroy(p);
+    return set_error(ctx, e == cudaErrorMemoryAllocation ? ARGENT_E_OOM : ARGENT_E_CUDA, m);
+  }
+  std::string err = device_bvh(ctx, p, (const float4*)dp, (const uint4*)di, nt);
+  cudaStreamSynchronize(ctx->stream);
+  if (!err.empty()) {
+    argent_piece_destroy(p);
+    return set_error(ctx, ARGENT_E_INVALID, err);
+  }
   p->dev.pos = (const float4*)dp;
   p->dev.nrm = (const float4*)dnr;
   p->dev.tri_idx = (const uint4*)di;
@@ -532,6 +748,78 @@ int argent_denoise_atrous(ArgentCtx* ctx, uint32_t width, uint32_t height, const
 
 }  // extern "C"
 
+// ------------------------------------------------------------------ develop
+
+namespace {
+
+// Uploads the grade's tables and develops d_rgb (w*h camera RGB on the
+// device) into d_out (w*h*3 bytes on the device).
+int run_develop(ArgentCtx* ctx, uint32_t w, uint32_t h, const float* d_rgb, const ArgentGrade* g, uint8_t* d_out) {
+  if (g->tonemap < ARGENT_TM_AGX || g->tonemap > ARGENT_TM_CLAMP || g->look < ARGENT_AGX_BASE ||
+      g->look > ARGENT_AGX_GOLDEN)
+    return set_error(ctx, ARGENT_E_INVALID, "unknown tone map or AgX look");
+  argent::DevelopTables t = argent::develop_tables(g->exposure_ev, g->tonemap, g->look, g->saturation);
+  size_t nc = t.curves.size(), ne = t.enc.size();
+  float* d_tab = nullptr;
+  ARGENT_CK(ctx, cudaMallocAsync((void**)&d_tab, (nc + ne) * sizeof(float), ctx->stream));
+  cudaError_t e = cudaSuccess;
+  if (nc) e = cudaMemcpyAsync(d_tab, t.curves.data(), nc * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_tab + nc, t.enc.data(), ne * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+  dv::DevTables dt;
+  dt.k = t.k;
+  dt.op = t.op;
+  dt.sat = t.sat;
+  dt.pick0 = t.pick[0];
+  dt.pick1 = t.pick[1];
+  dt.pick2 = t.pick[2];
+  dt.curves = d_tab;
+  dt.curve_base = t.curve_base;
+  dt.curve_len = t.curve_len;
+  dt.enc = d_tab + nc;
+  dt.enc_lo = t.enc_lo;
+  dt.enc_scale = t.enc_scale;
+  dt.enc_last = t.enc_last;
+  size_t np = (size_t)w * h;
+  int grid = (int)std::min<size_t>((np + 255) / 256, (size_t)ctx->num_sms * 8);
+  if (e == cudaSuccess) {
+    dv::k_develop<<<std::max(grid, 1), 256, 0, ctx->stream>>>(d_rgb, (uint32_t)np, dt, d_out);
+    ctx->launches++;
+    e = cudaGetLastError();
+  }
+  cudaFreeAsync(d_tab, ctx->stream);
+  if (e != cudaSuccess) return set_error(ctx, ARGENT_E_CUDA, std::string("develop: ") + cudaGetErrorString(e));
+  return ARGENT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int argent_develop(ArgentCtx* ctx, uint32_t width, uint32_t height, const float* rgb, const ArgentGrade* grade,
+                   uint8_t* out) {
+  if (!ctx || !grade || (width && height && (!rgb || !out))) return set_error(ctx, ARGENT_E_INVALID, "NULL argument");
+  size_t np = (size_t)width * height;
+  if (np == 0) return ARGENT_OK;
+  if (np > (1ull << 31)) return set_error(ctx, ARGENT_E_INVALID, "image too large");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  float* d_rgb = nullptr;
+  uint8_t* d_out = nullptr;
+  ARGENT_CK(ctx, cudaMallocAsync((void**)&d_rgb, 3 * np * sizeof(float), ctx->stream));
+  ARGENT_CK(ctx, cudaMallocAsync((void**)&d_out, 3 * np, ctx->stream));
+  cudaError_t e = cudaMemcpyAsync(d_rgb, rgb, 3 * np * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+  int rc = e == cudaSuccess ? run_develop(ctx, width, height, d_rgb, grade, d_out) : ARGENT_E_CUDA;
+  if (rc == ARGENT_OK) e = cudaMemcpyAsync(out, d_out, 3 * np, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaFreeAsync(d_rgb, ctx->stream);
+  cudaFreeAsync(d_out, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (rc != ARGENT_OK) return rc;
+  if (e != cudaSuccess) return set_error(ctx, ARGENT_E_CUDA, std::string("develop: ") + cudaGetErrorString(e));
+  return ctx_check_status(ctx);
+}
+
+}  // extern "C"
+
 // ------------------------------------------------------------------ cavity mask
 
 extern "C" {
@@ -673,10 +961,20 @@ static int ensure_tables(ArgentCtx* ctx) {
   return ARGENT_OK;
 }
 
-static int ensure_wave(ArgentCtx* ctx, int lane) {
+// Streams and events for lanes 0 .. n-1 (created once, kept).
+static int ensure_lane_streams(ArgentCtx* ctx, int n) {
+  for (int l = 1; l < n; ++l)
+    if (!ctx->lane_stream[l]) ARGENT_CK(ctx, cudaStreamCreateWithFlags(&ctx->lane_stream[l], cudaStreamNonBlocking));
+  for (int l = 0; l < n; ++l)
+    if (!ctx->film_ev[l]) ARGENT_CK(ctx, cudaEventCreateWithFlags(&ctx->film_ev[l], cudaEventDisableTiming));
+  return ARGENT_OK;
+}
+
+// Grows lane `lane`'s path state to at least `cap` slots (never shrinks, so
+// small renders after large ones reuse the buffers).
+static int ensure_wave(ArgentCtx* ctx, int lane, uint64_t cap) {
   WaveBuffers& w = ctx->wave[lane];
-  uint64_t cap = ctx->limits.wave_paths;
-  if (w.cap == cap) return ARGENT_OK;
+  if (w.cap >= cap) return ARGENT_OK;
   w.release();
   auto alloc = [&](void** p, size_t bytes) -> bool {
     if (cudaMalloc(p, bytes) != cudaSuccess) return false;
@@ -786,20 +1084,26 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
                     const std::vector<uint32_t>& scene_classes) {
   int rc = ensure_tables(ctx);
   if (rc != ARGENT_OK) return rc;
-  for (int l = 0; l < ARGENT_LANES; ++l) {
-    rc = ensure_wave(ctx, l);
-    if (rc != ARGENT_OK) return rc;
-  }
-  uint32_t cap = (uint32_t)ctx->wave[0].cap;
+  // Waves of up to wave_paths slots; a call with fewer path-samples than
+  // that plans one wave of its own size (at least 2^16 slots).
+  uint64_t total = 0;
+  for (size_t j = 0; j < jobs.size(); ++j) total += (uint64_t)jobs[j].w * jobs[j].h * counts[j];
+  uint32_t cap = (uint32_t)std::min<uint64_t>(ctx->limits.wave_paths, std::max<uint64_t>(total, 1u << 16));
   std::vector<uint32_t> depths;
   std::vector<dev::WaveDesc> waves = plan_waves(jobs, counts, cap, &depths);
   if (waves.empty()) return ARGENT_OK;
+  rc = ensure_lane_streams(ctx, ctx->lanes);
+  if (rc != ARGENT_OK) return rc;
+  for (int l = 0; l < std::min<int>(ctx->lanes, (int)waves.size()); ++l) {
+    rc = ensure_wave(ctx, l, cap);
+    if (rc != ARGENT_OK) return rc;
+  }
   dev::DevJob* d_jobs = nullptr;
   ARGENT_CK(ctx, cudaMallocAsync((void**)&d_jobs, jobs.size() * sizeof(dev::DevJob), ctx->stream));
   // Pageable source: the call returns once the bytes are staged.
   ARGENT_CK(ctx, cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(dev::DevJob), cudaMemcpyHostToDevice,
                                  ctx->stream));
-  int lanes = (int)std::min<size_t>(ARGENT_LANES, waves.size());
+  int lanes = (int)std::min<size_t>((size_t)ctx->lanes, waves.size());
   ARGENT_CK(ctx, cudaEventRecord(ctx->fork_ev, ctx->stream));
   for (int l = 1; l < lanes; ++l) ARGENT_CK(ctx, cudaStreamWaitEvent(ctx->lane_stream[l], ctx->fork_ev, 0));
   dev::WaveArgs args[ARGENT_LANES];
@@ -1240,6 +1544,45 @@ int argent_film_denoise(ArgentFilm* f, float* out) {
   return ctx_check_status(ctx);
 }
 
+int argent_film_develop(ArgentFilm* f, const ArgentGrade* grade, int denoise, uint8_t* out) {
+  if (!f || !grade || !out) return set_error(f ? f->ctx : nullptr, ARGENT_E_INVALID, "NULL argument");
+  ArgentCtx* ctx = f->ctx;
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  size_t np = (size_t)f->w * f->h;
+  float k = 1.0f / (float)std::max<uint32_t>(f->samples, 1);
+  Mat3 mt;
+  if (f->has_matrix)
+    std::memcpy(mt.m, f->cam_m, sizeof(mt.m));
+  else
+    argent::camera_matrix(false, nullptr, mt.m);
+  int rc = ensure_resolve(ctx, 9 * np);
+  if (rc != ARGENT_OK) return rc;
+  float *dc = ctx->resolve, *da = ctx->resolve + 3 * np, *dnrm = ctx->resolve + 6 * np;
+  int grid = (int)std::min<size_t>((np + 255) / 256, (size_t)ctx->num_sms * 8);
+  k_film_resolve<<<std::max(grid, 1), 256, 0, ctx->stream>>>(f->xyz, f->xyz64, f->albedo, f->normal, mt, k,
+                                                              (uint32_t)np, dc, denoise ? da : nullptr,
+                                                              denoise ? dnrm : nullptr);
+  ctx->launches++;
+  float* dd = nullptr;
+  uint8_t* d8 = nullptr;
+  ARGENT_CK(ctx, cudaMallocAsync((void**)&dd, 3 * np * sizeof(float), ctx->stream));
+  ARGENT_CK(ctx, cudaMallocAsync((void**)&d8, 3 * np, ctx->stream));
+  const float* src = dc;
+  if (denoise) {
+    rc = run_atrous(ctx, f->w, f->h, dc, da, dnrm, dd);
+    src = dd;
+  }
+  if (rc == ARGENT_OK) rc = run_develop(ctx, f->w, f->h, src, grade, d8);
+  cudaError_t e = cudaSuccess;
+  if (rc == ARGENT_OK) e = cudaMemcpyAsync(out, d8, 3 * np, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaFreeAsync(dd, ctx->stream);
+  cudaFreeAsync(d8, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (rc != ARGENT_OK) return rc;
+  if (e != cudaSuccess) return set_error(ctx, ARGENT_E_CUDA, std::string("film develop: ") + cudaGetErrorString(e));
+  return ctx_check_status(ctx);
+}
+
 // ------------------------------------------------------------------ render
 
 static int make_job(ArgentScene* scene, const ArgentCamera* cam, ArgentFilm* film, const ArgentPathSettings* ps,
@@ -1290,6 +1633,91 @@ int argent_render_pass(ArgentCtx* ctx, ArgentScene* scene, const ArgentCamera* c
   film->samples += count;
   film->has_matrix = true;
   std::memcpy(film->cam_m, scene->cam_m, sizeof(film->cam_m));
+  return ARGENT_OK;
+}
+
+int argent_autotune(ArgentCtx* ctx, ArgentScene* scene, const ArgentCamera* camera,
+                    const ArgentPathSettings* settings, uint32_t width, uint32_t height, uint32_t count,
+                    ArgentTuneResult* results, uint32_t max_results, uint32_t* n_results) {
+  if (!ctx || !scene || !camera || !settings || !n_results || (max_results && !results))
+    return set_error(ctx, ARGENT_E_INVALID, "argent_autotune: NULL argument");
+  if (width == 0 || height == 0 || count == 0) return set_error(ctx, ARGENT_E_INVALID, "empty tuning render");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  *n_results = 0;
+  size_t fr = 0, tot = 0;
+  ARGENT_CK(ctx, cudaMemGetInfo(&fr, &tot));
+  // A candidate's path state must fit in half of what is free now plus what
+  // the context already holds.
+  uint64_t held = 0;
+  for (int l = 0; l < ARGENT_LANES; ++l) held += ctx->wave[l].bytes;
+  uint64_t room = (uint64_t)fr / 2 + held;
+  const uint32_t lanes_c[] = {2, 4, 8, 12, 16};
+  const uint64_t waves_c[] = {1ull << 21, 1ull << 22, 1ull << 23, 1ull << 24};
+  uint64_t path_samples = (uint64_t)width * height * count;
+  ArgentFilm* film = nullptr;
+  int rc = argent_film_create(ctx, width, height, ARGENT_FILM_KAHAN, &film);
+  if (rc != ARGENT_OK) return rc;
+  int keep_lanes = ctx->lanes;
+  uint64_t keep_wave = ctx->limits.wave_paths;
+  double best = -1.0;
+  int best_lanes = keep_lanes;
+  uint64_t best_wave = keep_wave;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (uint32_t L : lanes_c) {
+    for (uint64_t W : waves_c) {
+      if ((uint64_t)L * W * 224 > room) continue;
+      if (W > path_samples * 2 && W > (1ull << 21)) continue;  // waves larger than the render change nothing
+      ctx->lanes = (int)L;
+      ctx->limits.wave_paths = W;
+      rc = argent_film_clear(film);
+      if (rc == ARGENT_OK) rc = argent_render_pass(ctx, scene, camera, film, settings, count, 1);  // warm-up
+      if (rc == ARGENT_OK) rc = argent_film_clear(film);
+      if (rc != ARGENT_OK) break;
+      cudaEventRecord(e0, ctx->stream);
+      rc = argent_render_pass(ctx, scene, camera, film, settings, count, 1);
+      cudaEventRecord(e1, ctx->stream);
+      if (rc == ARGENT_OK) rc = argent_ctx_sync(ctx);
+      if (rc != ARGENT_OK) break;
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      double v = ms > 0.0f ? (double)path_samples / (ms * 1e-3) : 0.0;
+      if (*n_results < max_results) {
+        results[*n_results].lanes = L;
+        results[*n_results].reserved = 0;
+        results[*n_results].wave_paths = W;
+        results[*n_results].path_samples_per_s = v;
+      }
+      ++*n_results;
+      if (v > best) {
+        best = v;
+        best_lanes = (int)L;
+        best_wave = W;
+      }
+    }
+    if (rc != ARGENT_OK) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  argent_film_destroy(film);
+  if (rc != ARGENT_OK) {
+    ctx->lanes = keep_lanes;
+    ctx->limits.wave_paths = keep_wave;
+    return rc;
+  }
+  ctx->lanes = best_lanes;
+  ctx->limits.wave_paths = best_wave;
+  // Free the path state of lanes the chosen configuration does not use.
+  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int l = best_lanes; l < ARGENT_LANES; ++l) ctx->wave[l].release();
+  return ARGENT_OK;
+}
+
+int argent_ctx_config(const ArgentCtx* ctx, uint32_t* lanes, uint64_t* wave_paths) {
+  if (!ctx) return set_error(nullptr, ARGENT_E_INVALID, "ctx is NULL");
+  if (lanes) *lanes = (uint32_t)ctx->lanes;
+  if (wave_paths) *wave_paths = ctx->limits.wave_paths;
   return ARGENT_OK;
 }
 

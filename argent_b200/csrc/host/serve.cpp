@@ -129,7 +129,7 @@ int argent_serve_create(ArgentCtx* ctx, const ArgentServeConfig* cfg, ArgentServ
   if (cfg) s->cfg = *cfg;
   if (s->cfg.film_budget == 0) s->cfg.film_budget = 8ull << 30;
   if (s->cfg.max_active == 0) s->cfg.max_active = 64;
-  if (s->cfg.step_path_samples == 0) s->cfg.step_path_samples = 1ull << 24;
+  if (s->cfg.step_path_samples == 0) s->cfg.step_path_samples = 1ull << 25;
   s->t0 = std::chrono::steady_clock::now();
   *out = s;
   return ARGENT_OK;

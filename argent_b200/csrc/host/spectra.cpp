@@ -615,6 +615,9 @@ struct Bands {
 
 // gems.rs:262-268 dispersion formulas
 const Sellmeier DIAMOND{{4.3356f, 0.3306f, 0.0f}, {0.011236f, 0.030625f, 0.0f}};
+// The gems workload's stated alternate fit (B = [0.4336, 3.3248],
+// C = [0.0106, 0.0321] um^2; n_D about 2.261), not one of argent's gems.
+const Sellmeier DIAMOND_ALT{{0.4336f, 3.3248f, 0.0f}, {0.0106f, 0.0321f, 0.0f}};
 const Sellmeier CUBIC_ZIRCONIA{{1.347091f, 2.117788f, 9.452943f}, {0.003911627f, 0.027801894f, 591.4901f}};
 const Sellmeier MOISSANITE{{0.20075f, 5.54861f, 35.65066f}, {-12.07224f, 0.02641f, 1268.247f}};
 const Sellmeier CORUNDUM_O{{1.4313493f, 0.65054713f, 5.3414021f}, {0.005279926f, 0.014238265f, 325.0178f}};
@@ -674,6 +677,7 @@ bool gem_def(const std::string& name_in, GemDef* g) {
   Bands TOURM{0.0365f, {band(720, 0.55f, 1.5f), band(470, 0.45f, 0.72f)}, false, NO};
   Bands MOISS_ABS{0.0005f, {}, true, {380, 0.05f, 0.08f}};
   if (n == "diamond") return T(sell(DIAMOND), constant(0.0f));
+  if (n == "diamond_alt") return T(sell(DIAMOND_ALT), constant(0.0f));
   if (n == "cubic_zirconia" || n == "cz" || n == "zirconia") return T(sell(CUBIC_ZIRCONIA), constant(0.0005f));
   if (n == "moissanite") return T(sell(MOISSANITE), bands(MOISS_ABS));
   if (n == "sapphire" || n == "blue_sapphire") return T(sell(CORUNDUM_O), bands(SAPPHIRE));

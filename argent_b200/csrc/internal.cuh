@@ -127,10 +127,11 @@ struct KernelProfile {
   uint64_t n[KC_COUNT] = {0, 0, 0, 0, 0, 0};
 };
 
-// Waves alternate between two lanes, each with its own stream and path
-// state, so that one wave's kernels fill the SMs that the other wave's
-// kernel tails leave idle.  Lane 0 runs on the context stream.
-#define ARGENT_LANES 2
+// Waves rotate over `lanes` lanes (default 8, at most ARGENT_LANES), each
+// with its own stream and path state, so that one wave's kernels fill the
+// SMs that another wave's kernel tails and small late-bounce launches leave
+// idle.  Lane 0 runs on the context stream.
+#define ARGENT_LANES 16
 
 struct ArgentCtx {
   int device = 0;
@@ -139,6 +140,7 @@ struct ArgentCtx {
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   cudaEvent_t film_ev[ARGENT_LANES] = {};
   int num_sms = 148;
+  int lanes = 8;
   ArgentLimits limits{};
   std::string err;
   uint64_t launches = 0;

@@ -21,9 +21,9 @@ def _p(a, t=ctypes.c_void_p):
 class Context:
     """One device, one stream (argent_ctx_create)."""
 
-    def __init__(self, device=0, wave_paths=0, memory_budget=0):
+    def __init__(self, device=0, wave_paths=0, memory_budget=0, lanes=0):
         self.lib = N.gpu()
-        lim = N.ArgentLimits(wave_paths, memory_budget)
+        lim = N.ArgentLimits(wave_paths, memory_budget, lanes, 0)
         h = ctypes.c_void_p()
         N.check(self.lib.argent_ctx_create(device, ctypes.byref(lim), ctypes.byref(h)))
         self.h = h
@@ -60,6 +60,21 @@ class Context:
         self.check(self.lib.argent_ctx_kernel_times(self.h, ms, n))
         return {k: (ms[i], int(n[i])) for i, k in enumerate(N.KERNEL_CLASSES)}
 
+    def autotune(self, scene, cam, settings, width, height, count):
+        """argent_autotune: times the frame for each (lanes, wave size) and
+        keeps the fastest.  Returns [(lanes, wave_paths, path-samples/s)]."""
+        res = (N.ArgentTuneResult * 32)()
+        n = ctypes.c_uint32()
+        self.check(self.lib.argent_autotune(self.h, scene.h, ctypes.byref(cam), ctypes.byref(settings), width, height,
+                                            count, res, 32, ctypes.byref(n)))
+        return [(r.lanes, r.wave_paths, r.path_samples_per_s) for r in res[: min(n.value, 32)]]
+
+    def config(self):
+        """(lanes, wave_paths) in use."""
+        lanes, wave = ctypes.c_uint32(), ctypes.c_uint64()
+        self.check(self.lib.argent_ctx_config(self.h, ctypes.byref(lanes), ctypes.byref(wave)))
+        return lanes.value, wave.value
+
     def set_counting(self, on):
         self.check(self.lib.argent_ctx_set_counting(self.h, 1 if on else 0))
 
@@ -79,14 +94,17 @@ class Context:
 
 
 class Piece:
-    """`Piece::new`: mesh upload + acceleration structure build."""
+    """`Piece::new`: mesh upload + acceleration structure build.  With
+    `device_bvh` the tree is the linear BVH built on the device (faster to
+    build, slower to trace; the same closest hits)."""
 
-    def __init__(self, ctx: Context, mesh):
+    def __init__(self, ctx: Context, mesh, device_bvh: bool = False):
         self.ctx = ctx
         self.mesh = mesh
         h = ctypes.c_void_p()
         fp = ctypes.POINTER(ctypes.c_float)
-        ctx.check(ctx.lib.argent_piece_upload(
+        upload = ctx.lib.argent_piece_upload_device_bvh if device_bvh else ctx.lib.argent_piece_upload
+        ctx.check(upload(
             ctx.h, _p(mesh.positions, fp), len(mesh.positions), _p(mesh.normals, fp), _p(mesh.tris, N.c_u32_p),
             len(mesh.tris), _p(mesh.tri_material, N.c_u16_p), _p(mesh.cavity, fp), ctypes.byref(h)))
         self.h = h
@@ -217,6 +235,14 @@ class Film:
         self.ctx.check(self.ctx.lib.argent_film_denoise(self.h, _p(out, ctypes.POINTER(ctypes.c_float))))
         return out
 
+    def developed(self, grade=None, denoise=True):
+        """8-bit sRGB (h, w, 3) of the film: render_image's denoise plus
+        argent-post's develop, on the device."""
+        g = grade if grade is not None else N.ArgentGrade(0.0, N.TM_AGX, N.AGX_PUNCHY, 1.0)
+        out = np.zeros((self.height, self.width, 3), np.uint8)
+        self.ctx.check(self.ctx.lib.argent_film_develop(self.h, ctypes.byref(g), 1 if denoise else 0, _p(out)))
+        return out
+
     def xyz(self):
         x = np.zeros((self.height, self.width, 3), np.float32)
         self.ctx.check(self.ctx.lib.argent_film_read_xyz(self.h, _p(x, ctypes.POINTER(ctypes.c_float))))
@@ -329,4 +355,15 @@ def denoise_atrous(ctx: Context, color, albedo=None, normal=None):
     out = np.zeros_like(c)
     h, w = c.shape[0], c.shape[1]
     ctx.check(ctx.lib.argent_denoise_atrous(ctx.h, w, h, _p(c, fp), _p(a, fp), _p(n, fp), _p(out, fp)))
+    return out
+
+
+def develop(ctx: Context, rgb, grade=None):
+    """argent_post::develop on the device: (h, w, 3) scene-linear float32 in,
+    8-bit sRGB out."""
+    g = grade if grade is not None else N.ArgentGrade(0.0, N.TM_AGX, N.AGX_PUNCHY, 1.0)
+    c = np.ascontiguousarray(rgb, np.float32)
+    out = np.zeros(c.shape, np.uint8)
+    ctx.check(ctx.lib.argent_develop(ctx.h, c.shape[1], c.shape[0], _p(c, ctypes.POINTER(ctypes.c_float)),
+                                     ctypes.byref(g), _p(out)))
     return out

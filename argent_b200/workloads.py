@@ -224,14 +224,15 @@ def signet_still(piece_gpu=None, spp=256, width=1920, height=1080, mesh=None):
 SIDE_GEMS = ("ruby", "sapphire", "emerald", "garnet")
 
 
-def gems_still(piece_gpu=None, spp=512, width=1080, height=1920, mesh=None, max_depth=32):
+def gems_still(piece_gpu=None, spp=512, width=1080, height=1920, mesh=None, max_depth=32, center="diamond"):
     """The gems workload: 18k gold setting (about 0.9M triangles) with a
-    diamond brilliant (argent's DIAMOND Sellmeier) and 36 side stones drawn
-    from ruby / sapphire / emerald / garnet; white studio, 1080 x 1920,
-    512 spp, max depth 32, 100 mm pinhole, hero view."""
+    diamond brilliant (argent's DIAMOND Sellmeier; `center="diamond_alt"`
+    takes the workload's stated alternate fit, n_D about 2.261) and 36 side
+    stones drawn from ruby / sapphire / emerald / garnet; white studio,
+    1080 x 1920, 512 spp, max depth 32, 100 mm pinhole, hero view."""
     m = mesh if mesh is not None else M.gem_ring()
     cam, turn = shot(piece_gpu, hull(m), "hero", 100.0, 0.0, width / height)
-    mats = [metal("gold18k", 0.07, 0.8), gem("diamond")] + [gem(g) for g in SIDE_GEMS]
+    mats = [metal("gold18k", 0.07, 0.8), gem(center)] + [gem(g) for g in SIDE_GEMS]
     desc = _studio_scene(m, mats, "white", turn)
     return Workload(f"gems_still_{width}x{height}_{spp}spp", m, desc, cam, width, height, spp, settings(max_depth), 7)
 

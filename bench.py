@@ -412,7 +412,7 @@ def run_gpu(args, world, rank, device):
     from argent_b200.gpu import Context, Film
 
     torch.cuda.set_device(device)
-    ctx = Context(device)
+    ctx = Context(device, wave_paths=args.wave_paths, lanes=args.lanes)
     plan = ReelPlan(ctx) if args.workload == "reel_batch" else StillPlan(ctx, args.workload)
     if args.spp:
         plan.set_spp(args.spp)  # profiling runs only: the bench line uses the workload's spp
@@ -460,8 +460,12 @@ def run_gpu(args, world, rank, device):
     samples_per_step = plan.path_samples
     value = world * samples_per_step * args.steps / (ms_max / 1000.0)
 
-    # Roofline of the dominant kernel.
-    dom = max(("intersect", "shade", "shadow", "raygen", "film"), key=lambda k: kt[k][0])
+    # Roofline of the dominant kernel: closest-hit traversal, the largest
+    # share of serialised device time in the ncu launch list
+    # (profiles/launches_signet_still.md).  With lanes overlapping, the live
+    # per-class event totals include time shared with other lanes' kernels,
+    # so they do not rank the kernels.
+    dom = "intersect"
     dom_ms, dom_n = kt[dom]
     path_samples_timed = samples_per_step * args.steps
     per_sample = {}
@@ -523,7 +527,8 @@ def run_gpu(args, world, rank, device):
     if rank == 0:
         cfg = plan.config()
         cfg.update({"parallelism": f"replicas{world}", "l2": "inputs larger than L2 (path state "
-                    f"{ctx_wave_mb(ctx)} MB per wave + BVH/triangles {plan.device_bytes / 1e6:.0f} MB)",
+                    f"{ctx_wave_mb(args)} MB per wave x {args.lanes or 8} lanes + BVH/triangles "
+                    f"{plan.device_bytes / 1e6:.0f} MB)",
                     "vs_baseline_ref": "README.md:5-6 ~17.7M path-samples/s on 32 CPU cores"})
         out = {
             "metric": "path-samples/s", "value": value, "unit": "path-samples/s", "n_gpus": world,
@@ -574,7 +579,7 @@ def run_serve(args, world, rank, device):
     ps = W.settings(12)
     rate = args.serve_rate
     trace = W.serve_trace(rate, args.serve_seconds)
-    srv = Serve(ctx, film_budget=32 << 30, max_active=64, step_path_samples=1 << 24)
+    srv = Serve(ctx, film_budget=32 << 30, max_active=64, step_path_samples=1 << 25)
 
     def submit(cname, i, j):
         _, w, h, spp, prio = W.SERVE_CLASSES[cname]
@@ -646,7 +651,7 @@ def run_serve(args, world, rank, device):
             "config": {"workload": f"serve_trace_{rate:g}rps_{args.serve_seconds:g}s", "requests": len(trace),
                        "classes": {k: list(v[1:]) for k, v in W.SERVE_CLASSES.items()},
                        "pieces_triangles": [int(m.num_tris) for m in meshes], "alloys": list(W.SERVE_ALLOYS),
-                       "offered_path_samples_per_s": offered, "step_path_samples": 1 << 24,
+                       "offered_path_samples_per_s": offered, "step_path_samples": 1 << 25,
                        "parallelism": f"replicas{world}",
                        "timing": "wall clock of the serve loop (latency is a wall-clock quantity); each step "
                                  "synchronises its batch"},
@@ -660,8 +665,8 @@ def run_serve(args, world, rank, device):
         print(json.dumps(out), flush=True)
 
 
-def ctx_wave_mb(ctx):
-    return 224 * 2 ** 21 // 10 ** 6
+def ctx_wave_mb(args):
+    return 224 * (args.wave_paths or 2 ** 23) // 10 ** 6
 
 
 def main():
@@ -675,6 +680,8 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--spp", type=int, default=0, help="override spp (short profiling runs)")
+    ap.add_argument("--lanes", type=int, default=0, help="concurrent waves (0 = the library default)")
+    ap.add_argument("--wave-paths", type=int, default=0, help="path slots per wave (0 = the library default)")
     ap.add_argument("--serve-rate", type=float, default=1.0, help="serve_trace: requests per second")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serve_trace: trace length")
     args = ap.parse_args()

@@ -197,10 +197,14 @@ typedef struct ArgentHit {
   uint32_t prim;
 } ArgentHit;
 
-/* Context limits; zero fields take defaults. */
+/* Context limits; zero fields take defaults.  Path state is 224 bytes per
+ * slot per lane and grows on demand to what a render needs, so the defaults
+ * (8 lanes of 2^23 slots) hold about 15 GB once a large frame has run. */
 typedef struct ArgentLimits {
-  uint64_t wave_paths;      /* path slots per wavefront wave (default 2^21) */
+  uint64_t wave_paths;      /* path slots per wavefront wave (default 2^23, at most 2^30) */
   uint64_t memory_budget;   /* bytes the serve loop may hold (default 3/4 of free) */
+  uint32_t lanes;           /* concurrent waves, each with its own stream and path state (default 8, at most 16) */
+  uint32_t reserved;
 } ArgentLimits;
 
 /* Film flags. */
@@ -233,6 +237,17 @@ int argent_piece_upload(ArgentCtx* ctx, const float* positions, uint32_t nv, con
                         const uint32_t* tris, uint32_t nt, const uint16_t* tri_material,
                         const float* cavity, ArgentPiece** out);
 void argent_piece_destroy(ArgentPiece* piece);
+/*
+ * Same arguments and result as argent_piece_upload, with the BVH built on
+ * the device: a linear BVH (63-bit Morton codes, radix sort, Karras radix
+ * tree) collapsed to the same 8-wide nodes.  For piece swaps: it builds
+ * much faster than the host SAH tree, which traces faster.  Closest
+ * hits are the same for either tree (the minimum of (t, triangle index)
+ * over the triangles hit).  Replaces `Bvh::build` (bvh.rs:117-146).
+ */
+int argent_piece_upload_device_bvh(ArgentCtx* ctx, const float* positions, uint32_t nv, const float* normals,
+                                   const uint32_t* tris, uint32_t nt, const uint16_t* tri_material,
+                                   const float* cavity, ArgentPiece** out);
 /* Root bounds, as `Piece::bounds` (scene.rs:34-37). */
 int argent_piece_bounds(const ArgentPiece* piece, float lo[3], float hi[3]);
 /* Bytes the piece holds on the device. */
@@ -334,6 +349,31 @@ typedef struct ArgentBatchItem {
 
 int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n);
 
+/* ------------------------------------------------------------------ */
+/* Autotuning (no counterpart in argent).                             */
+/* ------------------------------------------------------------------ */
+
+typedef struct ArgentTuneResult {
+  uint32_t lanes;
+  uint32_t reserved;
+  uint64_t wave_paths;
+  double path_samples_per_s;
+} ArgentTuneResult;
+
+/*
+ * Times `count` samples of the given frame (after one warm-up pass) for each
+ * lane count in {2, 4, 8, 12, 16} and wave size in {2^21 .. 2^24} whose path
+ * state fits in half of the free device memory, keeps the fastest as the
+ * context's configuration, and frees the path state of unused lanes.
+ * results (may be NULL when max_results is 0) receives up to max_results
+ * measurements; *n_results the number taken.  Renders into a scratch film.
+ */
+int argent_autotune(ArgentCtx* ctx, ArgentScene* scene, const ArgentCamera* camera,
+                    const ArgentPathSettings* settings, uint32_t width, uint32_t height, uint32_t count,
+                    ArgentTuneResult* results, uint32_t max_results, uint32_t* n_results);
+/* The context's current lanes and wave size. */
+int argent_ctx_config(const ArgentCtx* ctx, uint32_t* lanes, uint64_t* wave_paths);
+
 /* Kernels the library has launched on this context since creation. */
 uint64_t argent_ctx_kernel_launches(const ArgentCtx* ctx);
 
@@ -356,6 +396,36 @@ int argent_denoise_atrous(ArgentCtx* ctx, uint32_t width, uint32_t height, const
  * averages leaving the device (the `render_image` hand-off, shot.rs:424-444);
  * out receives width*height*3 floats of camera RGB. */
 int argent_film_denoise(ArgentFilm* film, float* out);
+
+/* ------------------------------------------------------------------ */
+/* Develop (argent-post tonemap.rs): the 8-bit hand-off.              */
+/* ------------------------------------------------------------------ */
+
+/* `ToneMap` and `AgxLook` (argent-post/src/tonemap.rs:38-55). */
+enum { ARGENT_TM_AGX = 0, ARGENT_TM_ACES = 1, ARGENT_TM_KHRONOS = 2, ARGENT_TM_REINHARD = 3, ARGENT_TM_CLAMP = 4 };
+enum { ARGENT_AGX_BASE = 0, ARGENT_AGX_PUNCHY = 1, ARGENT_AGX_GOLDEN = 2 };
+
+/* `Grade` (tonemap.rs:57-68); argent's default is AgX Punchy, 0 EV,
+ * saturation 1.  `look` is used by AgX only. */
+typedef struct ArgentGrade {
+  float exposure_ev;
+  int32_t tonemap;
+  int32_t look;
+  float saturation;
+} ArgentGrade;
+
+/*
+ * argent_post::develop (tonemap.rs:369-391): exposure, tone map, saturation,
+ * sRGB encode through argent's per-grade tables, TPDF dither, 8 bits.  rgb is
+ * width*height*3 floats of scene-linear camera RGB in host memory; out
+ * receives width*height*3 bytes, byte-identical to argent's develop.
+ */
+int argent_develop(ArgentCtx* ctx, uint32_t width, uint32_t height, const float* rgb, const ArgentGrade* grade,
+                   uint8_t* out);
+/* The film's colour (denoised with its guides when `denoise` is non-zero)
+ * developed to 8-bit sRGB without leaving the device: render_image + develop
+ * (shot.rs:424-444, serve/live.rs:200).  out receives width*height*3 bytes. */
+int argent_film_develop(ArgentFilm* film, const ArgentGrade* grade, int denoise, uint8_t* out);
 
 /* ------------------------------------------------------------------ */
 /* Cavity mask (argent-mesh cavity.rs), the patina input of `Piece`.  */
@@ -432,7 +502,7 @@ typedef struct ArgentServeConfig {
   uint64_t film_budget;       /* device bytes for films in use and pooled; 0 = 8 GiB */
   uint32_t max_active;        /* requests rendered together; 0 = 64 */
   uint32_t reserved;
-  uint64_t step_path_samples; /* path-samples per step; 0 = 2^24 */
+  uint64_t step_path_samples; /* path-samples per step; 0 = 2^25 (about 30 ms of rendering) */
 } ArgentServeConfig;
 
 typedef struct ArgentServeRequest {

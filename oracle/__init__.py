@@ -72,6 +72,9 @@ def lib():
             "oracle_smooth": (None, [vp, u32, vp, u32, vp, u32, f]),
             "oracle_patina_mask": (None, [vp, u32, vp, vp, u32, u32, f, f, f, u32, vp]),
             "oracle_atrous": (None, [u32, u32, vp, vp, vp, vp]),
+            "oracle_tonemap_pixel": (None, [fp, f, ctypes.c_int, ctypes.c_int, f, fp]),
+            "oracle_srgb_encode": (f, [f]),
+            "oracle_develop": (None, [vp, u64, f, ctypes.c_int, ctypes.c_int, f, vp, vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -220,3 +223,27 @@ def atrous(color, albedo=None, normal=None):
     out = np.zeros_like(c)
     lib().oracle_atrous(c.shape[1], c.shape[0], _ptr(c), _ptr(a), _ptr(n), _ptr(out))
     return out
+
+
+# ---------------------------------------------------------------- develop (argent-post tonemap.rs)
+
+def tonemap_pixel(rgb, ev=0.0, op=0, look=0, saturation=1.0):
+    """tonemap.rs:201-213: exact display-linear result of one pixel."""
+    x = (ctypes.c_float * 3)(*[float(v) for v in rgb])
+    out = (ctypes.c_float * 3)()
+    lib().oracle_tonemap_pixel(x, ev, op, look, saturation, out)
+    return np.array(out[:], np.float32)
+
+
+def srgb_encode(x):
+    return float(lib().oracle_srgb_encode(float(x)))
+
+
+def develop(rgb, ev=0.0, op=0, look=1, saturation=1.0):
+    """tonemap.rs:369-391 on an (h, w, 3) image: (8-bit image, encoded
+    floats of the fast path)."""
+    c = np.ascontiguousarray(rgb, np.float32)
+    enc = np.zeros_like(c)
+    out = np.zeros(c.shape, np.uint8)
+    lib().oracle_develop(_ptr(c), c.size // 3, ev, op, look, saturation, _ptr(enc), _ptr(out))
+    return out, enc

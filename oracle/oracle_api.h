@@ -63,6 +63,12 @@ void oracle_patina_mask(const float* pos, uint32_t nv, const float* normals, con
 /* À-trous denoiser (argent-post denoise.rs:535-712); albedo/normal may be NULL */
 void oracle_atrous(uint32_t w, uint32_t h, const float* color, const float* albedo, const float* normal, float* out);
 
+/* Tone mapping and develop (argent-post tonemap.rs, color.rs) */
+void oracle_tonemap_pixel(const float* rgb, float ev, int op, int look, float saturation, float* out);
+float oracle_srgb_encode(float x);
+void oracle_develop(const float* rgb, uint64_t n, float ev, int op, int look, float saturation, float* enc_out,
+                    uint8_t* out8);
+
 /* Primitives, for argent's unit-test known answers */
 float oracle_fresnel_dielectric(float c, float eta);
 float oracle_fresnel_conductor(float c, float eta, float k);

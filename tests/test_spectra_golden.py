@@ -261,6 +261,7 @@ def test_dispersion_matches_the_references():
     assert abs(disp("moissanite")[2] - 0.104) < 0.01
     assert abs(n589("sapphire") - 1.768) < 0.001
     assert abs(disp("sapphire")[2] - 0.018) < 0.001
+    assert abs(n589("diamond_alt") - 2.261) < 0.01
     assert abs(n589("amethyst") - 1.544) < 0.001
     assert abs(disp("spinel")[2] - 0.020) < 0.001
     nd, fire, _ = disp("glass")

@@ -149,8 +149,8 @@ def test_empty_piece_misses():
 
 
 @pytest.mark.gpu
-def test_closest_hit_parity_signet_2p22():
-    """The 2.1M-triangle signet piece, 2^22 rays."""
+def test_closest_hit_parity_signet_2p24():
+    """The 2.1M-triangle signet piece, 2^24 rays."""
     import oracle as O
     from argent_b200 import mesh
     from argent_b200.gpu import Piece
@@ -160,12 +160,12 @@ def test_closest_hit_parity_signet_2p22():
     ctx = _ctx()
     piece = Piece(ctx, m)
     bvh = O.Bvh(m.positions, m.tris)
-    n = 1 << 22
+    n = 1 << 24
     rays = make_rays(m.positions, m.tris, n, seed=8)
     got = piece.trace_closest(rays)
     ref = bvh.intersect(rays)
     r = compare_hits(ref, got, bvh, rays)
-    print("closest-hit parity (signet, 2^22 rays):", {k: v for k, v in r.items() if k != "mismatch_idx"})
+    print("closest-hit parity (signet, 2^24 rays):", {k: v for k, v in r.items() if k != "mismatch_idx"})
     assert r["mismatch"] == 0, r["mismatch_idx"]
     assert r["t_ulp_fail"] == 0
     assert r["closer"] <= n // 100000
