@@ -25,6 +25,11 @@
 namespace dev {
 
 // Hit record encoding (w component of the hit float4).
+// Minimum resident blocks of 128 threads per SM for the traversal kernels
+// (the register budget ptxas gets: 8 blocks = 64 registers per thread).
+#ifndef ARGENT_TRAV_BLOCKS
+#define ARGENT_TRAV_BLOCKS 8
+#endif
 #define HIT_MISS 0xFFFFFFFFu
 #define HIT_FLOOR 0xFFFFFFFEu
 #define HIT_PANEL 0xF0000000u
@@ -370,7 +375,7 @@ __device__ __forceinline__ uint32_t lane_refill(bool idle, bool* first, bool* mo
 // kernel of its hit's material class.  Persistent lanes step their BVH
 // traversals one node or leaf at a time and take a new path as soon as
 // theirs is done.
-__global__ void __launch_bounds__(128, 8) k_intersect(WaveArgs a, int depth) {
+__global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_intersect(WaveArgs a, int depth) {
   const uint32_t count = a.counters[CNT_ACT(depth)];
   uint32_t* work = a.counters + CNT_WORK(CNT_ACT(depth));
   uint2 stack[ARGENT_STACK_SIZE];
@@ -799,7 +804,7 @@ __global__ void __launch_bounds__(128, CLS == CLS_TERMINAL ? 1 : 4) k_shade(Wave
 // unoccluded rays add their contribution to L.  Persistent lanes, so a
 // lane whose ray ends early takes a new one instead of idling until the
 // slowest ray of its warp ends.
-__global__ void __launch_bounds__(128, 8) k_shadow(WaveArgs a, int depth) {
+__global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_shadow(WaveArgs a, int depth) {
   const uint32_t count = a.counters[CNT_SH(depth)];
   uint32_t* work = a.counters + CNT_WORK(CNT_SH(depth));
   uint32_t stack[ARGENT_STACK_SIZE];

@@ -7,6 +7,8 @@ with argent's traversal (restated in the oracle) under the same buckets as
 the host tree's parity tests.
 """
 
+import time
+
 import numpy as np
 import pytest
 
@@ -54,8 +56,13 @@ def test_signet_parity_and_bounds():
 
     m = mesh.signet()
     ctx = _ctx()
+    Piece(ctx, m, device_bvh=True).close()  # warm the allocator and the kernels
+    t0 = time.perf_counter()
     dev = Piece(ctx, m, device_bvh=True)
+    t1 = time.perf_counter()
     host = Piece(ctx, m)
+    t2 = time.perf_counter()
+    print(f"signet upload + BVH build: device {1e3 * (t1 - t0):.1f} ms, host {1e3 * (t2 - t1):.1f} ms")
     for a, b in zip(dev.bounds(), host.bounds()):
         assert np.array_equal(a, b)
     n = 1 << 21
