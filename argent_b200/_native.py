@@ -198,6 +198,7 @@ GPU_FUNCS = {
                                                ctypes.POINTER(ctypes.c_uint64)]),
     "argent_ctx_set_counting": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "argent_ctx_traversal_counts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
+    "argent_ctx_bounce_counts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
     "argent_ctx_traversal_histogram": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
     "argent_denoise_atrous": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, c_float_p, c_float_p,
                                              c_float_p, c_float_p]),

@@ -1081,7 +1081,7 @@ static void fill_args(dev::WaveArgs& a, const WaveBuffers& wb) {
 // chained by events, so films accumulate in wave order exactly as on one
 // stream.  The lanes fork from and join back into the context stream.
 static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const std::vector<uint32_t>& counts,
-                    const std::vector<uint32_t>& scene_classes) {
+                    const std::vector<const ArgentScene*>& job_scenes) {
   int rc = ensure_tables(ctx);
   if (rc != ARGENT_OK) return rc;
   // Waves of up to wave_paths slots; a call with fewer path-samples than
@@ -1114,9 +1114,11 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
     fill_args(args[l], ctx->wave[l]);
   }
   int g_ray = grid_for(ctx, (const void*)dev::k_raygen, 256, cap);
-  int g_int = grid_for(ctx, (const void*)dev::k_intersect, 128, cap);
+  int g_int[2] = {grid_for(ctx, (const void*)dev::k_intersect<false>, 128, cap),
+                   grid_for(ctx, (const void*)dev::k_intersect<true>, 128, cap)};
   int g_sh = grid_for(ctx, (const void*)dev::k_shade<CLS_METAL>, 128, cap);
-  int g_any = grid_for(ctx, (const void*)dev::k_shadow, 128, cap);
+  int g_any[2] = {grid_for(ctx, (const void*)dev::k_shadow<false>, 128, cap),
+                  grid_for(ctx, (const void*)dev::k_shadow<true>, 128, cap)};
   int g_film = grid_for(ctx, (const void*)dev::k_film, 256, cap);
   for (size_t wi = 0; wi < waves.size(); ++wi) {
     const dev::WaveDesc& w = waves[wi];
@@ -1125,7 +1127,18 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
     dev::WaveArgs& a = args[lane];
     const WaveBuffers& wb = ctx->wave[lane];
     uint32_t classes = 1u << CLS_TERMINAL;
-    for (uint32_t sgi = 0; sgi < w.num_segments; ++sgi) classes |= scene_classes[w.seg[sgi].job];
+    const ArgentScene* one = job_scenes[w.seg[0].job];
+    for (uint32_t sgi = 0; sgi < w.num_segments; ++sgi) {
+      const ArgentScene* sc = job_scenes[w.seg[sgi].job];
+      classes |= sc->host.class_mask;
+      if (sc != one) one = nullptr;
+    }
+    const int uni = one ? 1 : 0;
+    a.uscene = one ? one->d_scene : nullptr;
+    a.upiece = one ? one->host.piece : dev::DevPiece{};
+    a.u_has_turn = one ? one->host.has_turn : 0;
+    a.u_to_obj_s = one ? one->host.to_obj_s : 0.0f;
+    a.u_to_obj_c = one ? one->host.to_obj_c : 1.0f;
     a.q_in = wb.q0;
     a.q_out = wb.q1;
     {
@@ -1138,7 +1151,10 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
       a.q_out = (depth & 1) ? wb.q0 : wb.q1;
       {
         ProfScope ps(ctx, KC_INTERSECT, st);
-        dev::k_intersect<<<g_int, 128, 0, st>>>(a, (int)depth);
+        if (uni)
+          dev::k_intersect<true><<<g_int[1], 128, 0, st>>>(a, (int)depth);
+        else
+          dev::k_intersect<false><<<g_int[0], 128, 0, st>>>(a, (int)depth);
       }
       {
         ProfScope ps(ctx, KC_SHADE, st);
@@ -1151,9 +1167,17 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
       }
       {
         ProfScope ps(ctx, KC_SHADOW, st);
-        dev::k_shadow<<<g_any, 128, 0, st>>>(a, (int)depth);
+        if (uni)
+          dev::k_shadow<true><<<g_any[1], 128, 0, st>>>(a, (int)depth);
+        else
+          dev::k_shadow<false><<<g_any[0], 128, 0, st>>>(a, (int)depth);
       }
       ctx->launches += 3;
+    }
+    if (ctx->counting) {
+      dev::k_count_bounces<<<1, ARGENT_MAX_DEPTH, 0, st>>>(wb.counters, (int)std::min<uint32_t>(depths[wi],
+                                                                                            ARGENT_MAX_DEPTH));
+      ctx->launches++;
     }
     // Films accumulate in wave order: wait for the previous wave's film pass.
     if (wi > 0 && lanes > 1) ARGENT_CK(ctx, cudaStreamWaitEvent(st, ctx->film_ev[(lane + lanes - 1) % lanes], 0));
@@ -1183,6 +1207,8 @@ void argent_scene_destroy(ArgentScene* s) {
   cudaSetDevice(s->ctx->device);
   cudaStreamSynchronize(s->ctx->stream);
   for (void* a : s->allocs) cudaFree(a);
+  if (s->staged) cudaFreeHost(s->staged);
+  if (s->staged_ev) cudaEventDestroy(s->staged_ev);
   delete s;
 }
 
@@ -1323,10 +1349,19 @@ int argent_scene_set_turntable(ArgentScene* s, float deg) {
   if (!s) return set_error(nullptr, ARGENT_E_INVALID, "scene is NULL");
   ArgentCtx* ctx = s->ctx;
   ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  // Stream-ordered, without waiting for the renders already queued (they
+  // keep their angle): the descriptor goes through a pinned staging copy,
+  // rewritten only once its previous copy has run.
+  if (!s->staged) {
+    ARGENT_CK(ctx, cudaMallocHost((void**)&s->staged, sizeof(dev::DevScene)));
+    ARGENT_CK(ctx, cudaEventCreateWithFlags(&s->staged_ev, cudaEventDisableTiming));
+  } else {
+    ARGENT_CK(ctx, cudaEventSynchronize(s->staged_ev));
+  }
   set_turn(s->host, deg);
-  // Stream-ordered: renders already queued keep their angle.
-  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
-  ARGENT_CK(ctx, cudaMemcpy(s->d_scene, &s->host, sizeof(dev::DevScene), cudaMemcpyHostToDevice));
+  *s->staged = s->host;
+  ARGENT_CK(ctx, cudaMemcpyAsync(s->d_scene, s->staged, sizeof(dev::DevScene), cudaMemcpyHostToDevice, ctx->stream));
+  ARGENT_CK(ctx, cudaEventRecord(s->staged_ev, ctx->stream));
   return ARGENT_OK;
 }
 
@@ -1627,8 +1662,8 @@ int argent_render_pass(ArgentCtx* ctx, ArgentScene* scene, const ArgentCamera* c
   int rc = make_job(scene, camera, film, settings, seed, &jobs[0]);
   if (rc != ARGENT_OK) return rc;
   std::vector<uint32_t> counts{count};
-  std::vector<uint32_t> classes{scene->host.class_mask};
-  rc = run_jobs(ctx, jobs, counts, classes);
+  std::vector<const ArgentScene*> scenes{scene};
+  rc = run_jobs(ctx, jobs, counts, scenes);
   if (rc != ARGENT_OK) return rc;
   film->samples += count;
   film->has_matrix = true;
@@ -1726,7 +1761,7 @@ int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n
   ARGENT_CK(ctx, cudaSetDevice(ctx->device));
   std::vector<dev::DevJob> jobs(n);
   std::vector<uint32_t> counts(n);
-  std::vector<uint32_t> classes(n);
+  std::vector<const ArgentScene*> scenes(n);
   // Items that share a film run one after another: the second starts where
   // the first leaves film.samples.
   std::vector<uint32_t> pending(n, 0);
@@ -1744,9 +1779,9 @@ int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n
         return set_error(ctx, ARGENT_E_INVALID, "batch items share a film under different white balances");
     jobs[i].first = base;
     counts[i] = it.count;
-    classes[i] = it.scene->host.class_mask;
+    scenes[i] = it.scene;
   }
-  int rc = run_jobs(ctx, jobs, counts, classes);
+  int rc = run_jobs(ctx, jobs, counts, scenes);
   if (rc != ARGENT_OK) return rc;
   for (uint32_t i = 0; i < n; ++i) {
     items[i].film->samples += items[i].count;
@@ -1794,6 +1829,19 @@ int argent_ctx_set_counting(ArgentCtx* ctx, int on) {
   ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_trav_counts, z, 6 * sizeof(unsigned long long)));
   ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_trav_hist, z, sizeof(z)));
   ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_trav_max, zm, sizeof(zm)));
+  std::vector<unsigned long long> zb(2 * ARGENT_MAX_DEPTH, 0ull);
+  ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_bounce_counts, zb.data(), zb.size() * sizeof(unsigned long long)));
+  ctx->counting = on != 0;
+  return ARGENT_OK;
+}
+
+int argent_ctx_bounce_counts(ArgentCtx* ctx, uint64_t* out) {
+  if (!ctx || !out) return set_error(ctx, ARGENT_E_INVALID, "NULL argument");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  unsigned long long b[2 * ARGENT_MAX_DEPTH];
+  ARGENT_CK(ctx, cudaMemcpyFromSymbol(b, dev::d_bounce_counts, sizeof(b)));
+  for (int i = 0; i < 2 * ARGENT_MAX_DEPTH; ++i) out[i] = b[i];
   return ARGENT_OK;
 }
 

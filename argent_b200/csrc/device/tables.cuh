@@ -24,5 +24,10 @@ __device__ unsigned long long d_trav_counts[6];
 // closest-hit then any-hit, and the largest visit count of each kind.
 __device__ unsigned long long d_trav_hist[16];
 __device__ unsigned int d_trav_max[2];
+// Paths entering each bounce and shadow rays queued at each bounce (64
+// bounces, the path depth limit), summed over the waves run while counting
+// is on.
+#define ARGENT_BOUNCE_BINS 64
+__device__ unsigned long long d_bounce_counts[2 * ARGENT_BOUNCE_BINS];
 
 }  // namespace dev

@@ -141,6 +141,7 @@ struct ArgentCtx {
   cudaEvent_t film_ev[ARGENT_LANES] = {};
   int num_sms = 148;
   int lanes = 8;
+  bool counting = false;  // traversal instrumentation on (argent_ctx_set_counting)
   ArgentLimits limits{};
   std::string err;
   uint64_t launches = 0;
@@ -169,6 +170,10 @@ struct ArgentScene {
   std::vector<void*> allocs;
   uint64_t bytes = 0;
   float cam_m[9];
+  // Pinned staging copy for stream-ordered descriptor updates (turntable),
+  // and the event that marks its last copy done.
+  dev::DevScene* staged = nullptr;
+  cudaEvent_t staged_ev = nullptr;
 };
 
 struct ArgentFilm {

@@ -229,6 +229,14 @@ struct WaveArgs {
   uint32_t cap;
   uint32_t* counters;
   uint32_t* status;
+  // When every path of the wave belongs to one scene: that scene, a copy of
+  // its piece descriptor and its turntable rotation, so the traversal
+  // kernels read them from the parameter bank instead of following
+  // meta -> job -> scene for each ray (null otherwise).
+  const DevScene* uscene;
+  DevPiece upiece;
+  int32_t u_has_turn;
+  float u_to_obj_s, u_to_obj_c;
 };
 
 // Queue counters of one wave: active paths per bounce, shade-queue lengths
@@ -350,7 +358,9 @@ __device__ __forceinline__ void warp_append(bool pred, uint32_t value, uint32_t*
 // warp_first_batch.  Returns the queue index given to this lane (or ~0u)
 // and clears *more once the queue has run out; the decisions are
 // warp-uniform.
+#ifndef ARGENT_REFILL
 #define ARGENT_REFILL 8
+#endif
 __device__ __forceinline__ uint32_t lane_refill(bool idle, bool* first, bool* more, uint32_t count, uint32_t* work) {
   const unsigned lane = threadIdx.x & 31;
   unsigned need = __ballot_sync(0xffffffffu, idle);
@@ -375,30 +385,32 @@ __device__ __forceinline__ uint32_t lane_refill(bool idle, bool* first, bool* mo
 // kernel of its hit's material class.  Persistent lanes step their BVH
 // traversals one node or leaf at a time and take a new path as soon as
 // theirs is done.
+template <bool U>
 __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_intersect(WaveArgs a, int depth) {
   const uint32_t count = a.counters[CNT_ACT(depth)];
   uint32_t* work = a.counters + CNT_WORK(CNT_ACT(depth));
   uint2 stack[ARGENT_STACK_SIZE];
   ClosestTrav s;
-  const DevScene* sc = nullptr;
+  const DevScene* sc = U ? a.uscene : nullptr;
   uint32_t slot = 0;
   bool active = false, running = false, first = true, more = true;
   for (;;) {
     uint32_t j = lane_refill(!active, &first, &more, count, work);
     if (j != ~0u) {
       slot = a.q_in[j];
-      sc = a.jobs[a.meta[slot].w >> 16].scene;
+      if (!U) sc = a.jobs[a.meta[slot].w >> 16].scene;
       float4 of = a.o[slot], df = a.d[slot];
       V3 oo{of.x, of.y, of.z}, od{df.x, df.y, df.z};
-      if (sc->has_turn) {
-        oo = rot_y_sc(oo, sc->to_obj_s, sc->to_obj_c);
-        od = rot_y_sc(od, sc->to_obj_s, sc->to_obj_c);
+      if (U ? a.u_has_turn : sc->has_turn) {
+        float ts = U ? a.u_to_obj_s : sc->to_obj_s, tc = U ? a.u_to_obj_c : sc->to_obj_c;
+        oo = rot_y_sc(oo, ts, tc);
+        od = rot_y_sc(od, ts, tc);
       }
-      running = closest_begin(sc->piece, s, oo, od, INFINITY);
+      running = closest_begin(U ? a.upiece : sc->piece, s, oo, od, INFINITY);
       active = true;
     }
     if (__ballot_sync(0xffffffffu, active) == 0 && !more) break;
-    if (active && running) running = !closest_step(sc->piece, s, stack, a.status);
+    if (active && running) running = !closest_step(U ? a.upiece : sc->piece, s, stack, a.status);
     bool fin = active && !running;
     int cls = -1;
     if (fin) {
@@ -411,7 +423,7 @@ __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_intersect(WaveArgs 
       if (s.best.prim != ARGENT_NO_HIT_U) {
         t_max = s.best.t;
         rec = make_float4(s.best.t, s.best.u, s.best.v, __uint_as_float(s.best.prim));
-        cls = sc->mat_class[__ldg(&sc->piece.tri_idx[s.best.prim].w)];
+        cls = sc->mat_class[__ldg(&(U ? a.upiece : sc->piece).tri_idx[s.best.prim].w)];
       }
       for (int p = 0; p < sc->num_panels; ++p) {
         const DevPanel& pn = sc->panels[p];
@@ -759,8 +771,11 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
 
 // Surface shading is capped at 128 registers (4 blocks of 128 per SM)
 // instead of up to ~166, trading a little spilling for residency.
+#ifndef ARGENT_SHADE_BLOCKS
+#define ARGENT_SHADE_BLOCKS 4
+#endif
 template <int CLS>
-__global__ void __launch_bounds__(128, CLS == CLS_TERMINAL ? 1 : 4) k_shade(WaveArgs a, int depth) {
+__global__ void __launch_bounds__(128, CLS == CLS_TERMINAL ? 1 : ARGENT_SHADE_BLOCKS) k_shade(WaveArgs a, int depth) {
   uint32_t count = a.counters[CNT_CLS(depth, CLS)];
   const uint32_t* q = a.qc + (size_t)CLS * a.cap;
   uint32_t cap = a.cap;
@@ -804,6 +819,7 @@ __global__ void __launch_bounds__(128, CLS == CLS_TERMINAL ? 1 : 4) k_shade(Wave
 // unoccluded rays add their contribution to L.  Persistent lanes, so a
 // lane whose ray ends early takes a new one instead of idling until the
 // slowest ray of its warp ends.
+template <bool U>
 __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_shadow(WaveArgs a, int depth) {
   const uint32_t count = a.counters[CNT_SH(depth)];
   uint32_t* work = a.counters + CNT_WORK(CNT_SH(depth));
@@ -818,13 +834,12 @@ __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_shadow(WaveArgs a, 
     if (j != ~0u) {
       idx = j;
       float4 so = __ldcs(a.sh_o + j), sd = __ldcs(a.sh_d + j);
-      uint32_t slot = __float_as_uint(sd.w);
-      sc = a.jobs[a.meta[slot].w >> 16].scene;
-      state = any_begin(sc->piece, s, stack, V3{so.x, so.y, so.z}, V3{sd.x, sd.y, sd.z}, so.w);
+      if (!U) sc = a.jobs[a.meta[__float_as_uint(sd.w)].w >> 16].scene;
+      state = any_begin(U ? a.upiece : sc->piece, s, stack, V3{so.x, so.y, so.z}, V3{sd.x, sd.y, sd.z}, so.w);
       active = true;
     }
     if (__ballot_sync(0xffffffffu, active) == 0 && !more) break;
-    if (active && state == ARGENT_ANY_RUNNING) state = any_step(sc->piece, s, stack, a.status);
+    if (active && state == ARGENT_ANY_RUNNING) state = any_step(U ? a.upiece : sc->piece, s, stack, a.status);
     if (active && state != ARGENT_ANY_RUNNING) {
       count_visits(3, s.n_nodes, s.n_tris);
       if (state == ARGENT_ANY_CLEAR) {
@@ -835,6 +850,17 @@ __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_shadow(WaveArgs a, 
       }
       active = false;
     }
+  }
+}
+
+// Instrumentation: adds a finished wave's queue lengths per bounce to
+// d_bounce_counts (one thread per bounce).
+static_assert(ARGENT_BOUNCE_BINS == ARGENT_MAX_DEPTH, "one bounce counter per depth");
+__global__ void k_count_bounces(const uint32_t* counters, int depths) {
+  int d = threadIdx.x;
+  if (d < depths) {
+    atomicAdd(&d_bounce_counts[d], (unsigned long long)counters[CNT_ACT(d)]);
+    atomicAdd(&d_bounce_counts[ARGENT_BOUNCE_BINS + d], (unsigned long long)counters[CNT_SH(d)]);
   }
 }
 

@@ -84,6 +84,16 @@ class Context:
         k = ["closest_rays", "closest_nodes", "closest_tris", "any_rays", "any_nodes", "any_tris"]
         return dict(zip(k, [int(x) for x in out]))
 
+    def bounce_counts(self):
+        """(paths entering each bounce, shadow rays queued at each bounce),
+        trailing zeros dropped, since counting was turned on."""
+        out = (ctypes.c_uint64 * 128)()
+        self.check(self.lib.argent_ctx_bounce_counts(self.h, out))
+        v = [int(x) for x in out]
+        act, sh = v[:64], v[64:]
+        n = max([i + 1 for i, x in enumerate(act) if x] + [0])
+        return act[:n], sh[:n]
+
     def traversal_histogram(self):
         """Rays by node visits (bins 0, 1, 2-3, 4-7, 8-15, 16-63, 64-255,
         256+) and the largest visit count, per ray kind."""

@@ -127,6 +127,19 @@ def frame(points, azimuth, elevation, fill, focal_mm=100.0, f_stop=0.0, aspect=1
     return cam
 
 
+def band_camera(cam, height, y0, y1):
+    """The camera whose (y1 - y0)-row frame shows rows y0..y1 of `cam`'s
+    `height`-row frame (same width): the screen y of band row r,
+    1 - 2 (r + j) / hb, maps to frame row y0 + r through half_h' =
+    half_h * hb / H and shift' = (H - 2 y0 + shift * H) / hb - 1."""
+    hb = y1 - y0
+    b = N.ArgentCamera()
+    ctypes.memmove(ctypes.byref(b), ctypes.byref(cam), ctypes.sizeof(cam))
+    b.half_h = cam.half_h * hb / height
+    b.shift[1] = (height - 2 * y0 + cam.shift[1] * height) / hb - 1.0
+    return b
+
+
 def camera_ray(cam, sx, sy, lu, lv):
     """Camera::ray (camera.rs:57-69) for the autofocus probes."""
     f = np.float32

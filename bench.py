@@ -337,6 +337,10 @@ class StillPlan:
         return {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp,
                 "triangles": self.triangles, "max_depth": int(wl.settings.max_depth)}
 
+    def accuracy_target(self, ctx):
+        """(workload, scene, film holding its render at the workload's spp)."""
+        return self.wl, self.scene, self.films[0]
+
 
 class ReelPlan:
     """The batched workload: step k renders turntable frame k (mod 36) of
@@ -392,6 +396,12 @@ class ReelPlan:
                 "subset": f"each step is one turntable frame of all {self.renders} piece x alloy renders; "
                           f"steps walk the {self.W.REEL_FRAMES} frames"}
 
+    def accuracy_target(self, ctx):
+        """The 1.1M-triangle render of turntable frame 0, rendered afresh."""
+        run_plan(ctx, self, 0)
+        i = self.wls.index(self.cpu_wl)
+        return self.wls[i], self.scenes[i], self.films[i]
+
 
 def run_plan(ctx, plan, k, films=None, spp=None):
     from argent_b200.gpu import render_batch, render_pass
@@ -403,6 +413,51 @@ def run_plan(ctx, plan, k, films=None, spp=None):
         render_pass(ctx, *items[0])
     else:
         render_batch(ctx, items)
+
+
+ORACLE_SPP = 65536
+ORACLE_ROWS = 8
+
+
+def rel_rmse(img, ref):
+    """sqrt(sum (I - O)^2) / sqrt(sum O^2) per XYZ channel."""
+    img = np.asarray(img, np.float64).reshape(-1, 3)
+    ref = np.asarray(ref, np.float64).reshape(-1, 3)
+    return [float(v) for v in np.sqrt(((img - ref) ** 2).sum(0)) / np.sqrt((ref ** 2).sum(0))]
+
+
+def accuracy(ctx, plan, cpu_scene, threads):
+    """Error of the benchmarked render against the FP64 oracle: an
+    FP64-accumulated 65,536-spp render (on the device, through a band camera
+    and an independent seed) of ORACLE_ROWS rows at mid-frame, scored by
+    relRMSE per XYZ channel for the GPU render of the timed steps and, when
+    `cpu_scene` is given, for argent's algorithm (the CPU restatement) at the
+    same spp on the same rows."""
+    from argent_b200 import _native as N
+    from argent_b200 import workloads as W
+    from argent_b200.gpu import Film, render_pass
+
+    wl, scene, film = plan.accuracy_target(ctx)
+    y0 = wl.height // 2
+    y1 = min(wl.height, y0 + ORACLE_ROWS)
+    gpu = film.xyz()[y0:y1]
+    ref = Film(ctx, wl.width, y1 - y0, N.FILM_FP64)
+    t0 = time.perf_counter()
+    render_pass(ctx, scene, W.band_camera(wl.camera, wl.height, y0, y1), ref, wl.settings, ORACLE_SPP,
+                wl.seed ^ 0x5BD1E995)
+    o = ref.xyz()
+    dt = time.perf_counter() - t0
+    ref.close()
+    out = {"oracle": f"{wl.name}: rows {y0}..{y1}, FP64 film, {ORACLE_SPP} spp on the device, independent seed "
+                     f"({dt:.1f} s)",
+           "spp": wl.spp, "gpu_relrmse_xyz": rel_rmse(gpu, o)}
+    if cpu_scene is not None:
+        _, _, _, xyz = cpu_scene.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, wl.spp, wl.seed,
+                                             rows=(y0, y1), threads=threads)
+        cpu = xyz[y0:y1] / wl.spp
+        out["cpu_relrmse_xyz"] = rel_rmse(cpu, o)
+        out["gpu_vs_cpu_relrmse_xyz"] = rel_rmse(gpu, cpu)
+    return out
 
 
 def run_gpu(args, world, rank, device):
@@ -427,6 +482,7 @@ def run_gpu(args, world, rank, device):
     ctx.set_counting(True)
     run_plan(ctx, plan, 0, cfilms, 1)
     counts = ctx.traversal_counts()
+    bounce_act, bounce_sh = ctx.bounce_counts()
     hist = ctx.traversal_histogram()
     ctx.set_counting(False)
     for f in cfilms:
@@ -515,14 +571,17 @@ def run_gpu(args, world, rank, device):
         dt = max_over_ranks(dt, world, device)
         e2e_value = world * samples_per_step * args.e2e_steps / dt
 
-    cpu = None
+    cpu, cpu_scene = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
         wl = plan.cpu_wl
-        v, rows, nthr, _ = cpu_sample(wl, seconds=args.ref_seconds, threads=os.cpu_count() or 1)
+        v, rows, nthr, cpu_scene = cpu_sample(wl, seconds=args.ref_seconds, threads=os.cpu_count() or 1)
         cpu = {"value": v, "unit": "path-samples/s", "cores": nthr, "kind": "port",
                "sample": f"{wl.name}: rows {wl.height // 2}..{wl.height // 2 + rows} of the frame at {wl.spp} spp; "
                          f"argent's algorithm as restated in oracle/ (Rust reference not buildable here), "
                          f"OpenMP over rows"}
+    acc = None
+    if rank == 0 and not args.no_oracle:
+        acc = accuracy(ctx, plan, cpu_scene, os.cpu_count() or 1)
 
     if rank == 0:
         cfg = plan.config()
@@ -550,7 +609,10 @@ def run_gpu(args, world, rank, device):
             "kernel_ms": {k: round(v[0], 3) for k, v in kt.items()},
             "traversal_per_path_sample": {k: v / px for k, v in counts.items()},
             "traversal_nodes_per_ray_histogram": hist,
+            "rays_per_path_sample_by_bounce": {"closest": [round(x / px, 4) for x in bounce_act],
+                                               "shadow": [round(x / px, 4) for x in bounce_sh]},
             "cpu_baseline": cpu,
+            "error_vs_fp64_oracle": acc,
         }
         print(json.dumps(out), flush=True)
 
@@ -593,7 +655,7 @@ def run_serve(args, world, rank, device):
 
     launches0 = ctx.kernel_launches
     steps0 = srv.stats()
-    tickets = {}
+    tickets, reqs = {}, {}
     done = threading.Event()
     t_origin = srv.now()
 
@@ -602,7 +664,9 @@ def run_serve(args, world, rank, device):
             dt = t_origin + ta - srv.now()
             if dt > 0:
                 time.sleep(dt)
-            tickets[submit(cname, i, j)] = cname
+            t = submit(cname, i, j)
+            reqs[t] = (i, j)
+            tickets[t] = cname
         done.set()
 
     clocks = Clocks(smi_index(device))
@@ -610,6 +674,7 @@ def run_serve(args, world, rank, device):
     th = threading.Thread(target=driver)
     th.start()
     lat = {c: [] for c in W.SERVE_CLASSES}
+    kept = {}  # class -> ((mesh, alloy), colour film) of its first finished request
     finished = set()
     d2h = 0
     t_last = t_origin
@@ -625,6 +690,8 @@ def run_serve(args, world, rank, device):
                 c, a, n = srv.read(t)
                 d2h += c.nbytes + a.nbytes + n.nbytes
                 finished.add(t)
+                if cname not in kept:
+                    kept[cname] = (reqs[t], c)
         if done.is_set() and pending == 0 and len(finished) == len(tickets):
             break
         if pending == 0:
@@ -640,6 +707,26 @@ def run_serve(args, world, rank, device):
 
     def pct(v, q):
         return float(np.percentile(v, q)) if v else None
+
+    # Error of each class's first served film against the FP64 oracle (an
+    # FP64-accumulated 65,536-spp render of ORACLE_ROWS rows at mid-frame
+    # through a band camera, independent seed); serve hands back camera RGB,
+    # so the channels are camera RGB.
+    acc = {}
+    if not args.no_oracle:
+        from argent_b200 import _native as N
+        from argent_b200.gpu import Film, render_pass
+
+        for cname, ((i, j), c) in kept.items():
+            _, w, h, spp, _ = W.SERVE_CLASSES[cname]
+            y0, y1 = h // 2, h // 2 + ORACLE_ROWS
+            ref = Film(ctx, w, y1 - y0, N.FILM_FP64)
+            render_pass(ctx, scenes[(i, j)], W.band_camera(cams[(i, cname)], h, y0, y1), ref, ps, ORACLE_SPP,
+                        7 ^ 0x5BD1E995)
+            o, _, _ = ref.read()
+            ref.close()
+            acc[cname] = {"spp": spp, "mesh": i, "alloy": W.SERVE_ALLOYS[j],
+                          "relrmse_camera_rgb": rel_rmse(c[y0:y1], o)}
 
     if rank == 0:
         out = {
@@ -661,6 +748,9 @@ def run_serve(args, world, rank, device):
             "e2e": {"value": value, "unit": "path-samples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": d2h / max(1, len(finished)), "note": "per request: films read to host"},
             "gpu_launches": int(launches),
+            "error_vs_fp64_oracle": {"oracle": f"rows h/2..h/2+{ORACLE_ROWS} of each class's first served "
+                                               f"request, FP64 film, {ORACLE_SPP} spp on the device",
+                                     "classes": acc} if acc else None,
         }
         print(json.dumps(out), flush=True)
 
@@ -679,6 +769,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-oracle", action="store_true", help="skip the FP64 65,536-spp error measurement")
     ap.add_argument("--spp", type=int, default=0, help="override spp (short profiling runs)")
     ap.add_argument("--lanes", type=int, default=0, help="concurrent waves (0 = the library default)")
     ap.add_argument("--wave-paths", type=int, default=0, help="path slots per wave (0 = the library default)")

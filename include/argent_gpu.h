@@ -585,6 +585,10 @@ int argent_ctx_traversal_counts(ArgentCtx* ctx, uint64_t* out);
  * count of a closest-hit ray and of an any-hit ray, since the last
  * argent_ctx_set_counting. */
 int argent_ctx_traversal_histogram(ArgentCtx* ctx, uint64_t* out);
+/* out[128]: paths entering bounce d (out[d]) and shadow rays queued at
+ * bounce d (out[64 + d]), d < 64, summed over the waves run since the last
+ * argent_ctx_set_counting that turned counting on. */
+int argent_ctx_bounce_counts(ArgentCtx* ctx, uint64_t* out);
 
 #ifdef __cplusplus
 }

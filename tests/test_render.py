@@ -199,3 +199,69 @@ def test_reel_batch_matches_oracle():
         e = rel_rmse(f.xyz(), xyz / wl.spp)
         print(wl.name, "relRMSE XYZ vs oracle:", e)
         assert np.all(e <= RELRMSE_TOL), (wl.name, e)
+
+
+def test_band_camera_maps_band_rows_to_frame_rows():
+    """workloads.band_camera: the centre of band pixel (x, r) looks along the
+    ray of frame pixel (x, y0 + r), pinhole and thin lens."""
+    wl = W.signet_still(spp=1, mesh=W.M.Mesh(np.array([[-5, -5, -5], [5, 5, 5], [5, -5, 5]], np.float32),
+                                             np.array([[0, 1, 2]], np.uint32)))
+    cam = wl.camera
+    cam.lens_radius = 1.5
+    cam.focus_dist = 90.0
+    cam.shift[1] = 0.1
+    H, w, y0, y1 = wl.height, wl.width, 500, 516
+    band = W.band_camera(cam, H, y0, y1)
+    for x, r in [(0, 0), (w // 2, 7), (w - 1, 15)]:
+        sx = ((x + 0.5) * (2.0 / w)) - 1.0
+        sy_f = 1.0 - ((y0 + r + 0.5) * (2.0 / H))
+        sy_b = 1.0 - ((r + 0.5) * (2.0 / (y1 - y0)))
+        for lu, lv in [(0.5, 0.5), (0.1, 0.8)]:
+            of, df = W.camera_ray(cam, sx, sy_f, lu, lv)
+            ob, db = W.camera_ray(band, sx, sy_b, lu, lv)
+            assert np.allclose(of, ob, atol=1e-5) and np.allclose(df, db, atol=1e-6)
+
+
+@pytest.mark.gpu
+def test_band_camera_renders_the_same_rows():
+    """A band rendered through band_camera converges to the same rows of the
+    full frame (and not to rows 8 lower)."""
+    from argent_b200.gpu import Context, Film, Piece, Scene, render_pass
+
+    wl = W.ring_still()
+    ctx = Context(0)
+    piece = Piece(ctx, wl.mesh)
+    scene = Scene(ctx, piece, wl.desc)
+    full = Film(ctx, wl.width, wl.height)
+    render_pass(ctx, scene, wl.camera, full, wl.settings, 4096, wl.seed)
+    y0, y1 = 96, 112
+    band = Film(ctx, wl.width, y1 - y0, 2)
+    render_pass(ctx, scene, W.band_camera(wl.camera, wl.height, y0, y1), band, wl.settings, 4096, 99)
+    f, b = full.xyz(), band.xyz()
+    e = rel_rmse(b, f[y0:y1])
+    e_off = rel_rmse(b, f[y0 + 8:y1 + 8])
+    print("band vs frame rows relRMSE", e, "8 rows off", e_off)
+    assert np.all(e < 0.05) and np.all(3 * e < e_off), (e, e_off)
+
+
+@pytest.mark.gpu
+def test_bounce_counts_add_up_to_the_traversal_counts():
+    """Instrumentation: paths entering bounce 0 = path-samples; the queues
+    shrink with depth; their sums equal the rays the traversals counted."""
+    from argent_b200.gpu import Context, Film, Piece, Scene, render_pass
+
+    wl = W.ring_still()
+    ctx = Context(0)
+    piece = Piece(ctx, wl.mesh)
+    scene = Scene(ctx, piece, wl.desc)
+    film = Film(ctx, wl.width, wl.height)
+    ctx.set_counting(True)
+    render_pass(ctx, scene, wl.camera, film, wl.settings, 4, wl.seed)
+    act, sh = ctx.bounce_counts()
+    tc = ctx.traversal_counts()
+    ctx.set_counting(False)
+    print("paths per bounce", act, "shadow rays per bounce", sh)
+    assert act[0] == wl.width * wl.height * 4
+    assert all(b <= a for a, b in zip(act, act[1:]))
+    assert len(act) <= wl.settings.max_depth
+    assert sum(act) == tc["closest_rays"] and sum(sh) == tc["any_rays"]
