@@ -20,7 +20,8 @@ OK, E_OOM, E_INVALID, E_TIMEOUT, E_CUDA, E_OVERFLOW, E_BUSY = range(7)
 MAT_METAL, MAT_GEM, MAT_PLASTIC, MAT_OPAL, MAT_DIFFUSE, MAT_BLACK = range(6)
 GEM_TRANSPARENT, GEM_OPAL, GEM_OPAQUE = range(3)
 ENV_GRADIENT, ENV_MAP = range(2)
-FILM_KAHAN, FILM_FP64 = 1, 2
+FILM_KAHAN, FILM_FP64, FILM_PROGRESSIVE = 1, 2, 4
+FILM_FP64_AFTER = 4096
 
 c_float_p = ctypes.POINTER(ctypes.c_float)
 c_u32_p = ctypes.POINTER(ctypes.c_uint32)

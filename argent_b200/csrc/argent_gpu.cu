@@ -1620,6 +1620,31 @@ int argent_film_develop(ArgentFilm* f, const ArgentGrade* grade, int denoise, ui
 
 // ------------------------------------------------------------------ render
 
+// Long progressive renders switch their XYZ sums to FP64: the FP32 sums
+// with their Kahan compensation seed the FP64 sums (sum - compensation),
+// and from then on every film pass adds to both.
+__global__ void k_film_promote(const float* xyz, const float* comp, double* xyz64, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    xyz64[i] = (double)xyz[i] - (comp ? (double)comp[i] : 0.0);
+}
+
+static int promote_if_long(ArgentFilm* f, uint64_t end_samples) {
+  if (!(f->flags & ARGENT_FILM_PROGRESSIVE) || f->xyz64 || end_samples <= ARGENT_FILM_FP64_AFTER) return ARGENT_OK;
+  ArgentCtx* ctx = f->ctx;
+  size_t n = 3ull * f->w * f->h;
+  cudaError_t e = cudaMalloc(&f->xyz64, n * sizeof(double));
+  if (e != cudaSuccess) {
+    f->xyz64 = nullptr;
+    return set_error(ctx, ARGENT_E_OOM, "film: out of device memory for the FP64 sums");
+  }
+  f->bytes += n * sizeof(double);
+  k_film_promote<<<(int)std::min<size_t>((n + 255) / 256, 148 * 16), 256, 0, ctx->stream>>>(f->xyz, f->comp, f->xyz64,
+                                                                                          n);
+  ctx->launches++;
+  ARGENT_CK(ctx, cudaGetLastError());
+  return ARGENT_OK;
+}
+
 static int make_job(ArgentScene* scene, const ArgentCamera* cam, ArgentFilm* film, const ArgentPathSettings* ps,
                     uint32_t seed, dev::DevJob* j) {
   ArgentCtx* ctx = scene->ctx;
@@ -1659,7 +1684,9 @@ int argent_render_pass(ArgentCtx* ctx, ArgentScene* scene, const ArgentCamera* c
   ARGENT_CK(ctx, cudaSetDevice(ctx->device));
   if ((uint64_t)film->samples + count > 0xffffffffull) return set_error(ctx, ARGENT_E_INVALID, "sample index overflow");
   std::vector<dev::DevJob> jobs(1);
-  int rc = make_job(scene, camera, film, settings, seed, &jobs[0]);
+  int rc = promote_if_long(film, (uint64_t)film->samples + count);
+  if (rc != ARGENT_OK) return rc;
+  rc = make_job(scene, camera, film, settings, seed, &jobs[0]);
   if (rc != ARGENT_OK) return rc;
   std::vector<uint32_t> counts{count};
   std::vector<const ArgentScene*> scenes{scene};
@@ -1762,6 +1789,16 @@ int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n
   std::vector<dev::DevJob> jobs(n);
   std::vector<uint32_t> counts(n);
   std::vector<const ArgentScene*> scenes(n);
+  // A progressive film that this batch takes past the FP64 threshold gets
+  // its FP64 sums before any of its items is planned.
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!items[i].film || items[i].film->ctx != ctx) continue;  // refused below
+    uint64_t end = items[i].film->samples;
+    for (uint32_t k = 0; k < n; ++k)
+      if (items[k].film == items[i].film) end += items[k].count;
+    int rc = promote_if_long(items[i].film, end);
+    if (rc != ARGENT_OK) return rc;
+  }
   // Items that share a film run one after another: the second starts where
   // the first leaves film.samples.
   std::vector<uint32_t> pending(n, 0);

@@ -36,6 +36,20 @@ namespace dev {
 
 // ---------------------------------------------------------------- lights
 
+// |fl(x / y)| <= 1, as argent's `(q.dot(hu) / hu.length_squared()).abs() <= 1.0`
+// rounds it.  For a finite y > 0: |x| <= y passes without the division;
+// |x| above y (1 + 2^-22), rounded up, fails (the quotient then exceeds
+// 1 + 2^-22, which rounds above 1); only the band between, and any other y,
+// divides.
+__device__ __forceinline__ bool ratio_within_1(float x, float y) {
+  float ax = fabsf(x);
+  if (y > 0.0f && y < INFINITY) {
+    if (ax <= y) return true;
+    if (ax > __fmul_ru(y, 1.0000002384185791f)) return false;
+  }
+  return fabsf(x / y) <= 1.0f;
+}
+
 // light.rs:50-63
 __device__ __forceinline__ bool panel_intersect(const DevPanel& p, V3 o, V3 d, float t_max, float* t_out) {
   V3 n = ld3(p.n);
@@ -48,9 +62,7 @@ __device__ __forceinline__ bool panel_intersect(const DevPanel& p, V3 o, V3 d, f
   float t = num / denom;
   if (t <= 1e-6f || t >= t_max) return false;
   V3 q = (o + d * t) - ld3(p.c);
-  float a = dot(q, ld3(p.hu)) / p.hu_l2;
-  float b = dot(q, ld3(p.hv)) / p.hv_l2;
-  if (fabsf(a) <= 1.0f && fabsf(b) <= 1.0f) {
+  if (ratio_within_1(dot(q, ld3(p.hu)), p.hu_l2) && ratio_within_1(dot(q, ld3(p.hv)), p.hv_l2)) {
     *t_out = t;
     return true;
   }
@@ -361,6 +373,9 @@ __device__ __forceinline__ void warp_append(bool pred, uint32_t value, uint32_t*
 #ifndef ARGENT_REFILL
 #define ARGENT_REFILL 8
 #endif
+#ifndef ARGENT_FIN_BATCH
+#define ARGENT_FIN_BATCH 16
+#endif
 __device__ __forceinline__ uint32_t lane_refill(bool idle, bool* first, bool* more, uint32_t count, uint32_t* work) {
   const unsigned lane = threadIdx.x & 31;
   unsigned need = __ballot_sync(0xffffffffu, idle);
@@ -411,7 +426,14 @@ __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_intersect(WaveArgs 
     }
     if (__ballot_sync(0xffffffffu, active) == 0 && !more) break;
     if (active && running) running = !closest_step(U ? a.upiece : sc->piece, s, stack, a.status);
-    bool fin = active && !running;
+    // Lanes whose traversal is over wait until ARGENT_FIN_BATCH of them (or
+    // every active lane) can record their hits together: the panel and
+    // floor tests and the queue appends then run once for many lanes.
+    bool waiting = active && !running;
+    unsigned wm = __ballot_sync(0xffffffffu, waiting);
+    unsigned rm = __ballot_sync(0xffffffffu, active && running);
+    if (wm == 0 || (__popc(wm) < ARGENT_FIN_BATCH && rm != 0)) continue;
+    bool fin = waiting;
     int cls = -1;
     if (fin) {
       count_visits(0, s.n_nodes, s.n_tris);

@@ -265,3 +265,32 @@ def test_bounce_counts_add_up_to_the_traversal_counts():
     assert all(b <= a for a, b in zip(act, act[1:]))
     assert len(act) <= wl.settings.max_depth
     assert sum(act) == tc["closest_rays"] and sum(sh) == tc["any_rays"]
+
+
+@pytest.mark.gpu
+def test_progressive_film_switches_to_fp64_past_4096_samples():
+    """ARGENT_FILM_PROGRESSIVE: FP32 Kahan sums up to 4096 samples (equal to
+    a Kahan film bit for bit), FP64 sums once a pass goes past them, seeded
+    from the FP32 sums (equal to an FP64 film to the FP32 rounding of the
+    first 4000 samples)."""
+    from argent_b200 import _native as N
+    from argent_b200.gpu import Context, Film, Piece, Scene, render_pass
+
+    wl = W.ring_still(width=64, height=64)
+    ctx = Context(0)
+    piece = Piece(ctx, wl.mesh)
+    scene = Scene(ctx, piece, wl.desc)
+    prog = Film(ctx, 64, 64, N.FILM_KAHAN | N.FILM_PROGRESSIVE)
+    kahan = Film(ctx, 64, 64, N.FILM_KAHAN)
+    fp64 = Film(ctx, 64, 64, N.FILM_FP64)
+    for f in (prog, kahan, fp64):
+        render_pass(ctx, scene, wl.camera, f, wl.settings, 4000, wl.seed)
+    assert np.array_equal(prog.xyz(), kahan.xyz())
+    for f in (prog, kahan, fp64):
+        render_pass(ctx, scene, wl.camera, f, wl.settings, 200, wl.seed)
+    assert prog.samples == 4200
+    # The FP64 sums start from the compensated FP32 sums of the first 4000
+    # samples, whose per-wave partial sums round in FP32 (about 1e-5).
+    a, b = prog.xyz(), fp64.xyz()
+    assert np.allclose(a, b, rtol=1e-4, atol=1e-8), np.abs(a - b).max()
+    assert np.allclose(a, kahan.xyz(), rtol=1e-4, atol=1e-8)
