@@ -317,16 +317,27 @@ __device__ __forceinline__ bool closest_begin(const DevPiece& pc, ClosestTrav& s
   return true;
 }
 
-// Visits one node or one leaf; true when the traversal has finished.
-__device__ __forceinline__ bool closest_step(const DevPiece& pc, ClosestTrav& s, uint2* stack, uint32_t* status) {
-  if (!s.have) {
-    for (;;) {
-      if (s.sp == 0) return true;
-      --s.sp;
-      if (__uint_as_float(stack[s.sp].y) <= s.best.t) break;
+// Makes the next node or leaf current (popping entries that the running
+// best has pruned); false when the traversal is over.
+__device__ __forceinline__ bool closest_next(ClosestTrav& s, const uint2* stack) {
+  if (s.have) return true;
+  while (s.sp > 0) {
+    --s.sp;
+    uint2 e = stack[s.sp];
+    if (__uint_as_float(e.y) <= s.best.t) {
+      s.ref = e.x;
+      s.have = true;
+      return true;
     }
-    s.ref = stack[s.sp].x;
   }
+  return false;
+}
+
+__device__ __forceinline__ bool trav_at_leaf(uint32_t ref) { return (ref & ARGENT_LEAF_BIT) != 0; }
+
+// Visits the current node or leaf (closest_next returned true); true while
+// the traversal has more to visit.
+__device__ __forceinline__ bool closest_visit(const DevPiece& pc, ClosestTrav& s, uint2* stack, uint32_t* status) {
   s.have = false;
   uint32_t ref = s.ref;
   if (ref & ARGENT_LEAF_BIT) {
@@ -347,7 +358,7 @@ __device__ __forceinline__ bool closest_step(const DevPiece& pc, ClosestTrav& s,
         }
       }
     }
-    return s.sp == 0;
+    return s.sp > 0;
   }
   NodeView n = load_node(pc.nodes, ref);
   ++s.n_nodes;
@@ -361,11 +372,11 @@ __device__ __forceinline__ bool closest_step(const DevPiece& pc, ClosestTrav& s,
     k[c] = h ? ((__float_as_uint(tc) & ~7u) | (uint32_t)c) : 0xFFFFFFFFu;
     nh += h ? 1 : 0;
   }
-  if (nh == 0) return s.sp == 0;
+  if (nh == 0) return s.sp > 0;
   if (s.sp + nh - 1 > ARGENT_STACK_SIZE) {
     atomicOr(status, ARGENT_STATUS_STACK_OVERFLOW);
     s.sp = 0;
-    return true;
+    return false;
   }
   sort8(k);
 #pragma unroll
@@ -374,7 +385,13 @@ __device__ __forceinline__ bool closest_step(const DevPiece& pc, ClosestTrav& s,
   }
   s.ref = child_ref(n, (int)(k[0] & 7u));
   s.have = true;
-  return false;
+  return true;
+}
+
+// Visits one node or one leaf; true when the traversal has finished.
+__device__ __forceinline__ bool closest_step(const DevPiece& pc, ClosestTrav& s, uint2* stack, uint32_t* status) {
+  if (!closest_next(s, stack)) return true;
+  return !closest_visit(pc, s, stack, status);
 }
 
 __device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, float t_max, uint32_t* status) {
@@ -394,6 +411,8 @@ struct AnyTrav {
   RayQ rq;
   float t_max;
   int sp;
+  uint32_t ref;
+  bool have;  // ref holds a popped entry not yet visited
   uint32_t n_nodes, n_tris;
 };
 
@@ -408,6 +427,7 @@ __device__ __forceinline__ int any_begin(const DevPiece& pc, AnyTrav& s, uint32_
   s.d = d;
   s.t_max = t_max;
   s.sp = 0;
+  s.have = false;
   s.n_nodes = 0;
   s.n_tris = 0;
   if (pc.num_tris == 0) return ARGENT_ANY_CLEAR;
@@ -417,10 +437,20 @@ __device__ __forceinline__ int any_begin(const DevPiece& pc, AnyTrav& s, uint32_
   return ARGENT_ANY_RUNNING;
 }
 
-// Visits one node or one leaf.
-__device__ __forceinline__ int any_step(const DevPiece& pc, AnyTrav& s, uint32_t* stack, uint32_t* status) {
-  if (s.sp == 0) return ARGENT_ANY_CLEAR;
-  uint32_t ref = stack[--s.sp];
+// Pops the next node or leaf into s.ref; false when none is left.
+__device__ __forceinline__ bool any_next(AnyTrav& s, const uint32_t* stack) {
+  if (s.have) return true;
+  if (s.sp == 0) return false;
+  s.ref = stack[--s.sp];
+  s.have = true;
+  return true;
+}
+
+// Visits s.ref: ARGENT_ANY_HIT, or ARGENT_ANY_RUNNING / ARGENT_ANY_CLEAR by
+// whether entries remain.
+__device__ __forceinline__ int any_visit(const DevPiece& pc, AnyTrav& s, uint32_t* stack, uint32_t* status) {
+  s.have = false;
+  uint32_t ref = s.ref;
   if (ref & ARGENT_LEAF_BIT) {
     uint32_t start = ref & 0x07FFFFFFu;
     uint32_t cnt = ((ref >> 27) & 15u) + 1u;
@@ -453,6 +483,12 @@ __device__ __forceinline__ int any_step(const DevPiece& pc, AnyTrav& s, uint32_t
     stack[s.sp++] = child_ref(n, c);
   }
   return s.sp == 0 ? ARGENT_ANY_CLEAR : ARGENT_ANY_RUNNING;
+}
+
+// Visits one node or one leaf.
+__device__ __forceinline__ int any_step(const DevPiece& pc, AnyTrav& s, uint32_t* stack, uint32_t* status) {
+  if (!any_next(s, stack)) return ARGENT_ANY_CLEAR;
+  return any_visit(pc, s, stack, status);
 }
 
 __device__ __noinline__ bool trace_any(const DevPiece& pc, V3 o, V3 d, float t_max, uint32_t* status) {

@@ -371,10 +371,10 @@ __device__ __forceinline__ void warp_append(bool pred, uint32_t value, uint32_t*
 // and clears *more once the queue has run out; the decisions are
 // warp-uniform.
 #ifndef ARGENT_REFILL
-#define ARGENT_REFILL 8
+#define ARGENT_REFILL 16
 #endif
 #ifndef ARGENT_FIN_BATCH
-#define ARGENT_FIN_BATCH 16
+#define ARGENT_FIN_BATCH 24
 #endif
 __device__ __forceinline__ uint32_t lane_refill(bool idle, bool* first, bool* more, uint32_t count, uint32_t* work) {
   const unsigned lane = threadIdx.x & 31;
@@ -425,7 +425,16 @@ __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_intersect(WaveArgs 
       active = true;
     }
     if (__ballot_sync(0xffffffffu, active) == 0 && !more) break;
-    if (active && running) running = !closest_step(U ? a.upiece : sc->piece, s, stack, a.status);
+    // One step: the lanes at a leaf or the lanes at a node, whichever are
+    // more, visit it; the others wait, so the warp runs one of the two
+    // code paths per step instead of both.
+    if (active && running) running = closest_next(s, stack);
+    {
+      bool at_leaf = active && running && trav_at_leaf(s.ref);
+      bool at_node = active && running && !trav_at_leaf(s.ref);
+      bool leaves = __popc(__ballot_sync(0xffffffffu, at_leaf)) >= __popc(__ballot_sync(0xffffffffu, at_node));
+      if (leaves ? at_leaf : at_node) running = closest_visit(U ? a.upiece : sc->piece, s, stack, a.status);
+    }
     // Lanes whose traversal is over wait until ARGENT_FIN_BATCH of them (or
     // every active lane) can record their hits together: the panel and
     // floor tests and the queue appends then run once for many lanes.
@@ -861,7 +870,14 @@ __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_shadow(WaveArgs a, 
       active = true;
     }
     if (__ballot_sync(0xffffffffu, active) == 0 && !more) break;
-    if (active && state == ARGENT_ANY_RUNNING) state = any_step(U ? a.upiece : sc->piece, s, stack, a.status);
+    if (active && state == ARGENT_ANY_RUNNING && !any_next(s, stack)) state = ARGENT_ANY_CLEAR;
+    {
+      bool run = active && state == ARGENT_ANY_RUNNING;
+      bool at_leaf = run && trav_at_leaf(s.ref);
+      bool at_node = run && !trav_at_leaf(s.ref);
+      bool leaves = __popc(__ballot_sync(0xffffffffu, at_leaf)) >= __popc(__ballot_sync(0xffffffffu, at_node));
+      if (leaves ? at_leaf : at_node) state = any_visit(U ? a.upiece : sc->piece, s, stack, a.status);
+    }
     if (active && state != ARGENT_ANY_RUNNING) {
       count_visits(3, s.n_nodes, s.n_tris);
       if (state == ARGENT_ANY_CLEAR) {
