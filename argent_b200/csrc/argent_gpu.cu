@@ -231,9 +231,9 @@ int argent_ctx_create(int device, const ArgentLimits* limits, ArgentCtx** out) {
   ctx->lanes = ctx->limits.lanes ? (int)ctx->limits.lanes : 8;
   cudaError_t r = cudaSetDevice(device);
   if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
-  ctx->lane_stream[0] = ctx->stream;
-  for (int l = 1; l < ctx->lanes && r == cudaSuccess; ++l)
+  for (int l = 0; l < ctx->lanes && r == cudaSuccess; ++l)
     r = cudaStreamCreateWithFlags(&ctx->lane_stream[l], cudaStreamNonBlocking);
+  if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking);
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming);
   if (r == cudaSuccess) r = cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming);
   for (int l = 0; l < ctx->lanes && r == cudaSuccess; ++l)
@@ -259,13 +259,17 @@ void argent_ctx_destroy(ArgentCtx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (int l = 0; l < ARGENT_LANES; ++l)
+    if (ctx->lane_stream[l]) cudaStreamSynchronize(ctx->lane_stream[l]);
+  if (ctx->aux_stream) cudaStreamSynchronize(ctx->aux_stream);
   prof_collect(ctx);
   for (cudaEvent_t e : ctx->prof.pool) cudaEventDestroy(e);
   for (int l = 0; l < ARGENT_LANES; ++l) ctx->wave[l].release();
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->resolve) cudaFree(ctx->resolve);
-  for (int l = 1; l < ARGENT_LANES; ++l)
+  for (int l = 0; l < ARGENT_LANES; ++l)
     if (ctx->lane_stream[l]) cudaStreamDestroy(ctx->lane_stream[l]);
+  if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
   for (int l = 0; l < ARGENT_LANES; ++l)
@@ -278,6 +282,9 @@ int argent_ctx_sync(ArgentCtx* ctx) {
   if (!ctx) return set_error(nullptr, ARGENT_E_INVALID, "ctx is NULL");
   ARGENT_CK(ctx, cudaSetDevice(ctx->device));
   ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int l = 0; l < ARGENT_LANES; ++l)
+    if (ctx->lane_stream[l]) ARGENT_CK(ctx, cudaStreamSynchronize(ctx->lane_stream[l]));
+  if (ctx->aux_stream) ARGENT_CK(ctx, cudaStreamSynchronize(ctx->aux_stream));
   return ctx_check_status(ctx);
 }
 
@@ -963,7 +970,7 @@ static int ensure_tables(ArgentCtx* ctx) {
 
 // Streams and events for lanes 0 .. n-1 (created once, kept).
 static int ensure_lane_streams(ArgentCtx* ctx, int n) {
-  for (int l = 1; l < n; ++l)
+  for (int l = 0; l < n; ++l)
     if (!ctx->lane_stream[l]) ARGENT_CK(ctx, cudaStreamCreateWithFlags(&ctx->lane_stream[l], cudaStreamNonBlocking));
   for (int l = 0; l < n; ++l)
     if (!ctx->film_ev[l]) ARGENT_CK(ctx, cudaEventCreateWithFlags(&ctx->film_ev[l], cudaEventDisableTiming));
@@ -975,6 +982,8 @@ static int ensure_lane_streams(ArgentCtx* ctx, int n) {
 static int ensure_wave(ArgentCtx* ctx, int lane, uint64_t cap) {
   WaveBuffers& w = ctx->wave[lane];
   if (w.cap >= cap) return ARGENT_OK;
+  // Waves of earlier batches may still run on this lane.
+  if (w.cap > 0) ARGENT_CK(ctx, cudaStreamSynchronize(ctx->lane_stream[lane]));
   w.release();
   auto alloc = [&](void** p, size_t bytes) -> bool {
     if (cudaMalloc(p, bytes) != cudaSuccess) return false;
@@ -1080,8 +1089,13 @@ static void fill_args(dev::WaveArgs& a, const WaveBuffers& wb) {
 // (its own stream and path state); the film kernels of successive waves are
 // chained by events, so films accumulate in wave order exactly as on one
 // stream.  The lanes fork from and join back into the context stream.
+// Plans and launches the waves of `jobs`.  With `done` null the lanes join
+// the context stream at the end (work after this call on the context stream
+// sees the films finished); otherwise the lanes do not join: `done` is
+// recorded once the batch has finished, and the next batch's waves queue
+// behind this one's on each lane, so consecutive batches overlap.
 static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const std::vector<uint32_t>& counts,
-                    const std::vector<const ArgentScene*>& job_scenes) {
+                    const std::vector<const ArgentScene*>& job_scenes, cudaEvent_t done = nullptr) {
   int rc = ensure_tables(ctx);
   if (rc != ARGENT_OK) return rc;
   // Waves of up to wave_paths slots; a call with fewer path-samples than
@@ -1094,8 +1108,11 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   if (waves.empty()) return ARGENT_OK;
   rc = ensure_lane_streams(ctx, ctx->lanes);
   if (rc != ARGENT_OK) return rc;
-  for (int l = 0; l < std::min<int>(ctx->lanes, (int)waves.size()); ++l) {
-    rc = ensure_wave(ctx, l, cap);
+  const int nlanes = ctx->lanes;
+  const int start = ctx->next_lane % nlanes;
+  const int used = (int)std::min<size_t>((size_t)nlanes, waves.size());
+  for (int k = 0; k < used; ++k) {
+    rc = ensure_wave(ctx, (start + k) % nlanes, cap);
     if (rc != ARGENT_OK) return rc;
   }
   dev::DevJob* d_jobs = nullptr;
@@ -1103,9 +1120,9 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   // Pageable source: the call returns once the bytes are staged.
   ARGENT_CK(ctx, cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(dev::DevJob), cudaMemcpyHostToDevice,
                                  ctx->stream));
-  int lanes = (int)std::min<size_t>((size_t)ctx->lanes, waves.size());
   ARGENT_CK(ctx, cudaEventRecord(ctx->fork_ev, ctx->stream));
-  for (int l = 1; l < lanes; ++l) ARGENT_CK(ctx, cudaStreamWaitEvent(ctx->lane_stream[l], ctx->fork_ev, 0));
+  for (int k = 0; k < used; ++k)
+    ARGENT_CK(ctx, cudaStreamWaitEvent(ctx->lane_stream[(start + k) % nlanes], ctx->fork_ev, 0));
   dev::WaveArgs args[ARGENT_LANES];
   for (int l = 0; l < ARGENT_LANES; ++l) {
     args[l] = dev::WaveArgs{};
@@ -1122,7 +1139,7 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   int g_film = grid_for(ctx, (const void*)dev::k_film, 256, cap);
   for (size_t wi = 0; wi < waves.size(); ++wi) {
     const dev::WaveDesc& w = waves[wi];
-    int lane = (int)(wi % lanes);
+    int lane = (int)((start + wi) % nlanes);
     cudaStream_t st = ctx->lane_stream[lane];
     dev::WaveArgs& a = args[lane];
     const WaveBuffers& wb = ctx->wave[lane];
@@ -1180,20 +1197,25 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
       ctx->launches++;
     }
     // Films accumulate in wave order: wait for the previous wave's film pass.
-    if (wi > 0 && lanes > 1) ARGENT_CK(ctx, cudaStreamWaitEvent(st, ctx->film_ev[(lane + lanes - 1) % lanes], 0));
+    if (ctx->last_film_lane >= 0 && ctx->last_film_lane != lane)
+      ARGENT_CK(ctx, cudaStreamWaitEvent(st, ctx->film_ev[ctx->last_film_lane], 0));
     {
       ProfScope ps(ctx, KC_FILM, st);
       dev::k_film<<<g_film, 256, 0, st>>>(a, w);
     }
     ARGENT_CK(ctx, cudaEventRecord(ctx->film_ev[lane], st));
+    ctx->last_film_lane = lane;
     ctx->launches++;
   }
-  for (int l = 1; l < lanes; ++l) {
-    ARGENT_CK(ctx, cudaEventRecord(ctx->join_ev, ctx->lane_stream[l]));
-    ARGENT_CK(ctx, cudaStreamWaitEvent(ctx->stream, ctx->join_ev, 0));
+  ctx->next_lane = (int)((start + waves.size()) % nlanes);
+  cudaStream_t join = done ? ctx->aux_stream : ctx->stream;
+  for (int k = 0; k < used; ++k) {
+    ARGENT_CK(ctx, cudaEventRecord(ctx->join_ev, ctx->lane_stream[(start + k) % nlanes]));
+    ARGENT_CK(ctx, cudaStreamWaitEvent(join, ctx->join_ev, 0));
   }
   cudaError_t e = cudaGetLastError();
-  cudaFreeAsync(d_jobs, ctx->stream);
+  cudaFreeAsync(d_jobs, join);
+  if (done) ARGENT_CK(ctx, cudaEventRecord(done, join));
   if (e != cudaSuccess) return set_error(ctx, ARGENT_E_CUDA, std::string("render launch: ") + cudaGetErrorString(e));
   return ARGENT_OK;
 }
@@ -1783,7 +1805,10 @@ int argent_ctx_config(const ArgentCtx* ctx, uint32_t* lanes, uint64_t* wave_path
   return ARGENT_OK;
 }
 
-int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n) {
+}  // extern "C"
+
+// argent_render_batch; with `done` the batch overlaps the next one (run_jobs).
+static int render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n, cudaEvent_t done) {
   if (!ctx || (n && !items)) return set_error(ctx, ARGENT_E_INVALID, "argent_render_batch: NULL argument");
   ARGENT_CK(ctx, cudaSetDevice(ctx->device));
   std::vector<dev::DevJob> jobs(n);
@@ -1818,7 +1843,7 @@ int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n
     counts[i] = it.count;
     scenes[i] = it.scene;
   }
-  int rc = run_jobs(ctx, jobs, counts, scenes);
+  int rc = run_jobs(ctx, jobs, counts, scenes, done);
   if (rc != ARGENT_OK) return rc;
   for (uint32_t i = 0; i < n; ++i) {
     items[i].film->samples += items[i].count;
@@ -1826,6 +1851,17 @@ int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n
     std::memcpy(items[i].film->cam_m, items[i].scene->cam_m, sizeof(float) * 9);
   }
   return ARGENT_OK;
+}
+
+int render_batch_overlapped(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n, cudaEvent_t done) {
+  if (!done) return set_error(ctx, ARGENT_E_INVALID, "render_batch_overlapped: no completion event");
+  return render_batch(ctx, items, n, done);
+}
+
+extern "C" {
+
+int argent_render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n) {
+  return render_batch(ctx, items, n, nullptr);
 }
 
 }  // extern "C"

@@ -64,6 +64,28 @@ __device__ __forceinline__ float coated_pdf(Ggx ggx, float eta, const Spec& base
   return ps * p_spec + (1.0f - ps) * wi.z * ARGENT_FRAC_1_PI_F;
 }
 
+// coated_eval and coated_pdf of the same directions, sharing the half
+// vector and the Fresnel term of wo: the same values as the two calls.
+__device__ __forceinline__ void coated_eval_pdf(Ggx ggx, float eta, const Spec& base, V3 wo, V3 wi, Spec* f,
+                                                float* pdf) {
+  if (wo.z <= 0.0f || wi.z <= 0.0f) {
+    *f = spec(0.0f);
+    *pdf = 0.0f;
+    return;
+  }
+  V3 h = normalize(wo + wi);
+  float fo = fresnel_dielectric(wo.z, eta);
+  float fs = fresnel_dielectric(dot(wo, h), eta);
+  float sp = ggx_d(ggx, h) * ggx_g2(ggx, wo, wi) * fs / (4.0f * wo.z * wi.z);
+  float fi = fresnel_dielectric(wi.z, eta);
+  *f = base * ((1.0f - fo) * (1.0f - fi) * ARGENT_FRAC_1_PI_F) + spec(sp);
+  // coat_spec_prob(wo.z, eta, base) from the same Fresnel value
+  float d = average(base) * (1.0f - fo);
+  float ps = rclamp(fo / fmaxf(fo + d, 1e-6f), 0.15f, 0.95f);
+  float p_spec = ggx_d_visible(ggx, wo, h) / (4.0f * fmaxf(dot(wo, h), 1e-8f));
+  *pdf = ps * p_spec + (1.0f - ps) * wi.z * ARGENT_FRAC_1_PI_F;
+}
+
 // bsdf.rs:219-254
 __device__ __forceinline__ float bragg(float spacing_nm, float cos_t, float l) {
   float peak = 2.0f * spacing_nm * 1.37f * rclamp(cos_t, 0.0f, 1.0f);
@@ -157,6 +179,32 @@ __device__ float bsdf_pdf(const Bsdf& b, V3 wo, V3 wi) {
   }
 }
 
+// bsdf_eval and bsdf_pdf of the same directions; conductor and coated lobes
+// share their half vector (and the coat its Fresnel term of wo).
+template <unsigned KM = KM_ALL>
+__device__ __forceinline__ void bsdf_eval_pdf(const Bsdf& b, V3 wo, V3 wi, Spec* f, float* pdf) {
+  if (KM_HAS(KM, B_COATED) && b.kind == B_COATED) {
+    coated_eval_pdf(b.ggx, b.eta1, b.base, wo, wi, f, pdf);
+    return;
+  }
+  if (KM_HAS(KM, B_CONDUCTOR) && b.kind == B_CONDUCTOR) {
+    if (wo.z <= 0.0f || wi.z <= 0.0f || is_smooth(b.ggx)) {
+      *f = spec(0.0f);
+      *pdf = 0.0f;
+      return;
+    }
+    V3 h = normalize(wo + wi);
+    Spec fr = fresnel_conductor(dot(wo, h), b.eta, b.k);
+    float base = ggx_d(b.ggx, h) * ggx_g2(b.ggx, wo, wi) / (4.0f * wo.z * wi.z);
+    float e = b.e_wo;
+    *f = fr * base * (spec(1.0f) + b.f0 * ((1.0f - e) / e));
+    *pdf = ggx_d_visible(b.ggx, wo, h) / (4.0f * fmaxf(dot(wo, h), 1e-8f));
+    return;
+  }
+  *f = bsdf_eval<KM>(b, wo, wi);
+  *pdf = bsdf_pdf<KM>(b, wo, wi);
+}
+
 // Coated lobe sampling (bsdf.rs:164-182).
 __device__ __forceinline__ bool coated_sample(Ggx ggx, float eta, const Spec& base, V3 wo, float u0, float u1,
                                               float u2, BsdfSample* out) {
@@ -170,10 +218,12 @@ __device__ __forceinline__ bool coated_sample(Ggx ggx, float eta, const Spec& ba
     wi = cosine_hemisphere(u1, u2);
   }
   if (wi.z <= 0.0f) return false;
-  float p = coated_pdf(ggx, eta, base, wo, wi);
+  float p;
+  Spec f;
+  coated_eval_pdf(ggx, eta, base, wo, wi, &f, &p);
   if (p <= 0.0f) return false;
   out->wi = wi;
-  out->f = coated_eval(ggx, eta, base, wo, wi);
+  out->f = f;
   out->pdf = p;
   out->delta = out->transmit = out->terminate_secondary = false;
   return true;

@@ -10,24 +10,39 @@
 // A request's film receives exactly the sample indices a single
 // render_pass of `spp` samples would, in chunks (render.rs:70,86).
 //
-// Admission: queued requests enter the active set in (priority, ticket)
-// order while the active set is below max_active and their films fit in the
-// film budget; films come from a pool keyed by (width, height, flags).
+// Order: a request's urgency is its priority minus its waiting time over
+// the aging period (so a final that has waited long outranks a fresh
+// preview), ties by ticket.  Admission: queued requests enter the active set
+// in that order while the active set is below max_active and their films
+// fit in the film budget; films come from a pool keyed by (width, height,
+// flags).
+//
+// Chunks: the step's budget of path-samples grows with the work pending
+// (a quarter of it, between step_path_samples and step_path_samples_max), so a
+// deep queue runs in larger, more efficient batches.  Active requests take
+// chunks in urgency order; a request whose remaining work is under a
+// sixteenth of the budget finishes in this step, and every active request
+// advances by at least one sample, so none starves.
 //
 // Threads: submit, poll and cancel lock the queue and may be called from
 // any thread.  step and read drive the context and belong to the thread
 // that owns it (a context is single-stream and not thread-safe).
+#include <cuda_runtime.h>
+
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <mutex>
 #include <new>
 #include <string>
 #include <tuple>
+#include <utility>
 #include <vector>
 
 #include "../../../include/argent_gpu.h"
+#include "overlap.h"
 
 namespace {
 
@@ -35,7 +50,9 @@ struct Request {
   uint64_t ticket;
   ArgentServeRequest req;
   int32_t state;
-  uint32_t samples;
+  uint32_t samples;    // finished
+  uint32_t scheduled;  // issued: finished or in a batch in flight
+  uint32_t in_flight;  // batches in flight that hold a chunk of it
   bool cancel;
   ArgentFilm* film;
   uint64_t film_bytes;
@@ -61,6 +78,13 @@ struct ArgentServe {
   uint64_t pool_bytes = 0;
   std::chrono::steady_clock::time_point t0;
   uint64_t steps = 0, path_samples = 0;
+  // Batches in flight, oldest first: completion event and (ticket, samples).
+  struct Batch {
+    cudaEvent_t done;
+    std::vector<std::pair<uint64_t, uint32_t>> parts;
+  };
+  std::deque<Batch> flight;
+  std::vector<cudaEvent_t> idle_events;
 
   double now() const {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -110,9 +134,61 @@ bool pooled(ArgentServe* s, const ArgentServeRequest& r) {
   return it != s->pool.end() && !it->second.empty();
 }
 
-bool urgent_first(const Request* a, const Request* b) {
-  if (a->req.priority != b->req.priority) return a->req.priority < b->req.priority;
-  return a->ticket < b->ticket;
+double urgency(const Request* q, double now, double aging_s) {
+  return (double)q->req.priority - (now - q->t_submit) / aging_s;
+}
+
+void sort_urgent_first(std::vector<Request*>& v, double now, double aging_s) {
+  std::sort(v.begin(), v.end(), [&](const Request* a, const Request* b) {
+    double ua = urgency(a, now, aging_s), ub = urgency(b, now, aging_s);
+    if (ua != ub) return ua < ub;
+    return a->ticket < b->ticket;
+  });
+}
+
+// Path-samples not yet issued.
+uint64_t remaining(const Request* q) {
+  return (uint64_t)(q->req.spp - q->scheduled) * q->req.width * q->req.height;
+}
+
+// Applies finished batches in order: waits for the oldest when `wait`,
+// otherwise takes only those already done.  Returns the first failure.
+int retire(ArgentServe* s, bool wait) {
+  int rc = ARGENT_OK;
+  while (!s->flight.empty()) {
+    ArgentServe::Batch& b = s->flight.front();
+    cudaError_t e = wait ? cudaEventSynchronize(b.done) : cudaEventQuery(b.done);
+    if (e == cudaErrorNotReady) break;
+    wait = false;
+    int st = e == cudaSuccess ? ARGENT_OK : ARGENT_E_CUDA;
+    if (st == ARGENT_OK) st = ctx_check_status(s->ctx);
+    if (st != ARGENT_OK && rc == ARGENT_OK) rc = st;
+    std::lock_guard<std::mutex> g(s->mu);
+    double t = s->now();
+    for (auto& part : b.parts) {
+      auto it = s->reqs.find(part.first);
+      if (it == s->reqs.end()) continue;
+      Request& q = it->second;
+      --q.in_flight;
+      if (st != ARGENT_OK) {
+        if (q.state == ARGENT_REQ_ACTIVE) {
+          q.state = ARGENT_REQ_FAILED;
+          q.t_done = t;
+        }
+      } else {
+        q.samples += part.second;
+        s->path_samples += (uint64_t)part.second * q.req.width * q.req.height;
+        if (q.state == ARGENT_REQ_ACTIVE && q.samples >= q.req.spp) {
+          q.state = ARGENT_REQ_DONE;
+          q.t_done = t;
+        }
+      }
+      if (q.in_flight == 0 && q.state == ARGENT_REQ_FAILED) give_film(s, q);
+    }
+    s->idle_events.push_back(b.done);
+    s->flight.pop_front();
+  }
+  return rc;
 }
 
 }  // namespace
@@ -129,7 +205,10 @@ int argent_serve_create(ArgentCtx* ctx, const ArgentServeConfig* cfg, ArgentServ
   if (cfg) s->cfg = *cfg;
   if (s->cfg.film_budget == 0) s->cfg.film_budget = 8ull << 30;
   if (s->cfg.max_active == 0) s->cfg.max_active = 64;
-  if (s->cfg.step_path_samples == 0) s->cfg.step_path_samples = 1ull << 25;
+  if (s->cfg.step_path_samples == 0) s->cfg.step_path_samples = 1ull << 26;
+  if (s->cfg.aging_ms == 0) s->cfg.aging_ms = 1000;
+  if (s->cfg.step_path_samples_max == 0) s->cfg.step_path_samples_max = 2 * s->cfg.step_path_samples;
+  s->cfg.step_path_samples_max = std::max(s->cfg.step_path_samples_max, s->cfg.step_path_samples);
   s->t0 = std::chrono::steady_clock::now();
   *out = s;
   return ARGENT_OK;
@@ -137,6 +216,9 @@ int argent_serve_create(ArgentCtx* ctx, const ArgentServeConfig* cfg, ArgentServ
 
 void argent_serve_destroy(ArgentServe* s) {
   if (!s) return;
+  argent_ctx_sync(s->ctx);
+  for (auto& b : s->flight) cudaEventDestroy(b.done);
+  for (cudaEvent_t e : s->idle_events) cudaEventDestroy(e);
   for (auto& kv : s->reqs)
     if (kv.second.film) argent_film_destroy(kv.second.film);
   drain_pool(s);
@@ -192,15 +274,17 @@ int argent_serve_cancel(ArgentServe* s, uint64_t ticket) {
 
 int argent_serve_step(ArgentServe* s, uint32_t* pending) {
   if (!s) return ARGENT_E_INVALID;
+  int rc = retire(s, false);
   std::vector<ArgentBatchItem> items;
   std::vector<Request*> in_batch;
   std::vector<uint32_t> chunk;
   {
     std::lock_guard<std::mutex> g(s->mu);
-    // Cancellations take effect between batches, as in queue.rs:605-608.
+    // Cancellations take effect between batches, as in queue.rs:605-608,
+    // once none of the request's batches is in flight.
     for (auto& kv : s->reqs) {
       Request& q = kv.second;
-      if (q.cancel && (q.state == ARGENT_REQ_QUEUED || q.state == ARGENT_REQ_ACTIVE)) {
+      if (q.cancel && q.in_flight == 0 && (q.state == ARGENT_REQ_QUEUED || q.state == ARGENT_REQ_ACTIVE)) {
         give_film(s, q);
         q.state = ARGENT_REQ_CANCELLED;
         q.t_done = s->now();
@@ -211,7 +295,8 @@ int argent_serve_step(ArgentServe* s, uint32_t* pending) {
       if (kv.second.state == ARGENT_REQ_ACTIVE) active.push_back(&kv.second);
       if (kv.second.state == ARGENT_REQ_QUEUED) queued.push_back(&kv.second);
     }
-    std::sort(queued.begin(), queued.end(), urgent_first);
+    const double now = s->now(), aging_s = s->cfg.aging_ms * 1e-3;
+    sort_urgent_first(queued, now, aging_s);
     for (Request* q : queued) {
       if (active.size() >= s->cfg.max_active) break;
       if (!pooled(s, q->req) && s->film_in_use + s->pool_bytes + q->film_bytes > s->cfg.film_budget) {
@@ -219,8 +304,8 @@ int argent_serve_step(ArgentServe* s, uint32_t* pending) {
         drain_pool(s);
         if (s->film_in_use + q->film_bytes > s->cfg.film_budget) break;
       }
-      int rc = take_film(s, q->req, &q->film);
-      if (rc != ARGENT_OK) {
+      int frc = take_film(s, q->req, &q->film);
+      if (frc != ARGENT_OK) {
         q->state = ARGENT_REQ_FAILED;
         q->t_done = s->now();
         continue;
@@ -230,18 +315,20 @@ int argent_serve_step(ArgentServe* s, uint32_t* pending) {
       q->t_start = s->now();
       active.push_back(q);
     }
-    std::sort(active.begin(), active.end(), urgent_first);
-    // Chunks: the most urgent requests first, each as many whole samples of
-    // its frame as the step's budget leaves (at least one for the first).
-    uint64_t left = s->cfg.step_path_samples;
+    sort_urgent_first(active, now, aging_s);
+    uint64_t pending_work = 0;
+    for (auto& kv : s->reqs)
+      if (kv.second.state == ARGENT_REQ_QUEUED || kv.second.state == ARGENT_REQ_ACTIVE)
+        pending_work += remaining(&kv.second);
+    const uint64_t budget =
+        std::min(s->cfg.step_path_samples_max, std::max(s->cfg.step_path_samples, pending_work / 4));
+    uint64_t left = budget;
     for (Request* q : active) {
+      if (q->cancel || q->scheduled >= q->req.spp) continue;
       uint64_t px = (uint64_t)q->req.width * q->req.height;
-      uint64_t want = q->req.spp - q->samples;
-      uint64_t n = std::min<uint64_t>(want, left / px);
-      if (n == 0) {
-        if (!items.empty()) break;
-        n = 1;
-      }
+      uint64_t want = q->req.spp - q->scheduled;
+      uint64_t n = remaining(q) <= budget / 16 ? want : std::min<uint64_t>(want, left / px);
+      if (n == 0) n = 1;
       ArgentBatchItem it;
       std::memset(&it, 0, sizeof(it));
       it.scene = q->req.scene;
@@ -254,32 +341,52 @@ int argent_serve_step(ArgentServe* s, uint32_t* pending) {
       in_batch.push_back(q);
       chunk.push_back((uint32_t)n);
       left = n * px >= left ? 0 : left - n * px;
-      if (left == 0) break;
     }
   }
-  int rc = ARGENT_OK;
   if (!items.empty()) {
-    rc = argent_render_batch(s->ctx, items.data(), (uint32_t)items.size());
-    if (rc == ARGENT_OK) rc = argent_ctx_sync(s->ctx);
+    cudaEvent_t done = nullptr;
+    if (!s->idle_events.empty()) {
+      done = s->idle_events.back();
+      s->idle_events.pop_back();
+    } else if (cudaEventCreateWithFlags(&done, cudaEventDisableTiming) != cudaSuccess) {
+      done = nullptr;
+    }
+    int brc = done ? render_batch_overlapped(s->ctx, items.data(), (uint32_t)items.size(), done) : ARGENT_E_CUDA;
+    std::lock_guard<std::mutex> g(s->mu);
+    if (brc == ARGENT_OK) {
+      ArgentServe::Batch b;
+      b.done = done;
+      for (size_t i = 0; i < in_batch.size(); ++i) {
+        in_batch[i]->scheduled += chunk[i];
+        ++in_batch[i]->in_flight;
+        b.parts.emplace_back(in_batch[i]->ticket, chunk[i]);
+      }
+      s->flight.push_back(std::move(b));
+      ++s->steps;
+    } else {
+      if (done) s->idle_events.push_back(done);
+      double t = s->now();
+      for (Request* q : in_batch) {
+        q->state = ARGENT_REQ_FAILED;
+        q->t_done = t;
+      }
+      if (rc == ARGENT_OK) rc = brc;
+    }
+  }
+  if (rc != ARGENT_OK) {
+    // After a failure nothing stays in flight: wait for every batch.
+    argent_ctx_sync(s->ctx);
+    int r2 = retire(s, false);
+    (void)r2;
+  } else {
+    // Without overlap wait for this step's batch; with it, for the older
+    // of two in flight (or for the one in flight when nothing was issued).
+    size_t depth = s->cfg.overlap ? 2 : 1;
+    if (s->flight.size() >= depth || (items.empty() && !s->flight.empty())) rc = retire(s, true);
   }
   std::lock_guard<std::mutex> g(s->mu);
-  double t = s->now();
-  for (size_t i = 0; i < in_batch.size(); ++i) {
-    Request* q = in_batch[i];
-    if (rc != ARGENT_OK) {
-      q->state = ARGENT_REQ_FAILED;
-      q->t_done = t;
-      give_film(s, *q);
-      continue;
-    }
-    q->samples += chunk[i];
-    s->path_samples += (uint64_t)chunk[i] * q->req.width * q->req.height;
-    if (q->samples >= q->req.spp) {
-      q->state = ARGENT_REQ_DONE;
-      q->t_done = t;
-    }
-  }
-  if (!items.empty()) ++s->steps;
+  for (auto& kv : s->reqs)
+    if (kv.second.state == ARGENT_REQ_FAILED && kv.second.in_flight == 0) give_film(s, kv.second);
   if (pending) {
     uint32_t n = 0;
     for (auto& kv : s->reqs)
@@ -313,6 +420,7 @@ int argent_serve_release(ArgentServe* s, uint64_t ticket) {
   if (it == s->reqs.end()) return ARGENT_E_INVALID;
   Request& q = it->second;
   if (q.state == ARGENT_REQ_QUEUED || q.state == ARGENT_REQ_ACTIVE) return ARGENT_E_INVALID;
+  if (q.in_flight > 0) return ARGENT_E_BUSY;  // a failed request's batch still runs
   give_film(s, q);
   s->reqs.erase(it);
   return ARGENT_OK;

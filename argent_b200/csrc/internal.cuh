@@ -139,6 +139,13 @@ struct ArgentCtx {
   cudaStream_t lane_stream[ARGENT_LANES] = {};
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   cudaEvent_t film_ev[ARGENT_LANES] = {};
+  // Waves rotate over the lanes across calls: the next call starts at
+  // next_lane, and its first film pass waits for the film pass of the last
+  // wave before it (on last_film_lane), so films accumulate in wave order
+  // also when batches overlap.
+  int next_lane = 0, last_film_lane = -1;
+  // Completion stream of batches that do not join the context stream.
+  cudaStream_t aux_stream = nullptr;
   int num_sms = 148;
   int lanes = 8;
   bool counting = false;  // traversal instrumentation on (argent_ctx_set_counting)

@@ -648,10 +648,11 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
         V3 dir = envmap_sample(sc, u1, u2, &pdf_dir);
         if (pdf_dir > 0.0f && dot(dir, ngu) > 0.0f) {
           V3 wi = to_local(frame, dir);
-          Spec f = bsdf_eval<KM>(bsdf, wo, wi);
+          Spec f;
+          float p_bsdf;
+          bsdf_eval_pdf<KM>(bsdf, wo, wi, &f, &p_bsdf);
           if (!is_black(f)) {
             float p_light = sc->env_pick * pdf_dir;
-            float p_bsdf = bsdf_pdf<KM>(bsdf, wo, wi);
             float w = p_light * p_light / (p_light * p_light + p_bsdf * p_bsdf);
             // sky_visibility (scene.rs:123-140): panels and floor here, the
             // piece in k_shadow.
@@ -707,10 +708,11 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
         float cos_l = dot(-dir, ld3(pn.n));
         if (cos_l > 0.0f && dot(dir, ngu) > 0.0f) {
           V3 wi = to_local(frame, dir);
-          Spec f = bsdf_eval<KM>(bsdf, wo, wi);
+          Spec f;
+          float p_bsdf;
+          bsdf_eval_pdf<KM>(bsdf, wo, wi, &f, &p_bsdf);
           if (!is_black(f)) {
             float p_light = pick * d2 / (cos_l * pn.area);
-            float p_bsdf = bsdf_pdf<KM>(bsdf, wo, wi);
             float w = p_light * p_light / (p_light * p_light + p_bsdf * p_bsdf);
             V3 origin = offset_origin(p, ngu, dir);
             // visible (scene.rs:222-243): panels and floor here.

@@ -500,11 +500,13 @@ def run_gpu(args, world, rank, device):
     launches0 = ctx.kernel_launches
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    tw0 = time.perf_counter()
     e0.record(stream)
     for i in range(args.steps):
         run_plan(ctx, plan, args.warmup + i)
     e1.record(stream)
     e1.synchronize()
+    wall_ms = 1e3 * (time.perf_counter() - tw0)
     ctx.sync()
     launches = ctx.kernel_launches - launches0
     kt = ctx.kernel_times()
@@ -553,23 +555,52 @@ def run_gpu(args, world, rank, device):
         traffic = tr["dram_bytes_per_ray"] * rays * path_samples_timed / max(dom_n, 1)
         issue = tr.get("issue_active_pct")
 
+    # The batched workload's renders one render_pass at a time (the plain
+    # single-render path), device-timed like the batch, for comparison.
+    plain = None
+    if plan.renders > 1 and args.steps > 0:
+        from argent_b200.gpu import render_pass
+
+        barrier(world, device)
+        ctx.sync()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for i in range(args.steps):
+            for it in plan.items(args.warmup + i):
+                it[2].clear()
+                render_pass(ctx, *it)
+        p1.record(stream)
+        p1.synchronize()
+        pms = max_over_ranks(p0.elapsed_time(p1), world, device)
+        plain = {"value": world * samples_per_step * args.steps / (pms / 1000.0), "unit": "path-samples/s",
+                 "ms_per_step": pms / args.steps,
+                 "form": f"the same {plan.renders} renders per step, one render_pass each"}
+
     # End-to-end through the C ABI with host buffers.
-    e2e_value = None
+    e2e_value, e2e_split = None, None
     h2d = plan.renders * (ctypes.sizeof(N.ArgentCamera) + ctypes.sizeof(N.ArgentPathSettings) + 8)
     d2h = 3 * px * 3 * 4
     if args.e2e_steps > 0:
         bufs = [tuple(np.zeros((f.height, f.width, 3), np.float32) for _ in range(3)) for f in plan.films]
         fp = ctypes.POINTER(ctypes.c_float)
         barrier(world, device)
+        t_issue = t_read = 0.0
         t0 = time.perf_counter()
         for i in range(args.e2e_steps):
+            ta = time.perf_counter()
             run_plan(ctx, plan, i)
+            tb = time.perf_counter()
             for f, (c, a, nrm) in zip(plan.films, bufs):
                 ctx.check(ctx.lib.argent_film_read(f.h, c.ctypes.data_as(fp), a.ctypes.data_as(fp),
                                                    nrm.ctypes.data_as(fp)))
+            t_issue += tb - ta
+            t_read += time.perf_counter() - tb
         dt = time.perf_counter() - t0
         dt = max_over_ranks(dt, world, device)
         e2e_value = world * samples_per_step * args.e2e_steps / dt
+        e2e_split = {"issue_ms_per_step": 1e3 * t_issue / args.e2e_steps,
+                     "wait_and_read_ms_per_step": 1e3 * t_read / args.e2e_steps}
 
     cpu, cpu_scene = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -592,12 +623,13 @@ def run_gpu(args, world, rank, device):
         out = {
             "metric": "path-samples/s", "value": value, "unit": "path-samples/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "wall_ms_per_step": wall_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": value / PUBLISHED_CPU, "dtype": "f32",
             "data": f"synthetic ({DATA[args.workload]})",
             "config": cfg,
             "clocks": ck,
             "e2e": {"value": e2e_value, "unit": "path-samples/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "split": e2e_split},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "kernel": f"k_{dom}",
@@ -612,6 +644,7 @@ def run_gpu(args, world, rank, device):
             "rays_per_path_sample_by_bounce": {"closest": [round(x / px, 4) for x in bounce_act],
                                                "shadow": [round(x / px, 4) for x in bounce_sh]},
             "cpu_baseline": cpu,
+            "plain_form": plain,
             "error_vs_fp64_oracle": acc,
         }
         print(json.dumps(out), flush=True)
@@ -641,15 +674,18 @@ def run_serve(args, world, rank, device):
     ps = W.settings(12)
     rate = args.serve_rate
     trace = W.serve_trace(rate, args.serve_seconds)
-    srv = Serve(ctx, film_budget=32 << 30, max_active=64, step_path_samples=1 << 25)
+    srv = Serve(ctx, film_budget=32 << 30, max_active=64, step_path_samples=args.serve_step,
+                step_path_samples_max=args.serve_step_max, aging_ms=args.serve_aging_ms,
+                overlap=not args.serve_no_overlap)
 
     def submit(cname, i, j):
         _, w, h, spp, prio = W.SERVE_CLASSES[cname]
         return srv.submit(scenes[(i, j)], cams[(i, cname)], ps, w, h, spp, 7, prio)
 
-    # Warm-up: previews rendered to completion before the trace.
-    for k in range(args.warmup):
-        t = submit("preview", k % len(meshes), k % len(W.SERVE_ALLOYS))
+    # Warm-up before the trace: one request of each class (path state and
+    # films reach their full sizes), then previews.
+    for k, cname in enumerate(list(W.SERVE_CLASSES) + ["preview"] * args.warmup):
+        t = submit(cname, k % len(meshes), k % len(W.SERVE_ALLOYS))
         srv.run()
         srv.read(t)
 
@@ -708,6 +744,16 @@ def run_serve(args, world, rank, device):
     def pct(v, q):
         return float(np.percentile(v, q)) if v else None
 
+    # The same stream through argent's own discipline (one job at a time).
+    plain = None
+    if not args.no_plain:
+        pv, plat = serve_plain(ctx, trace, scenes, cams, ps)
+        plain = {"value": pv, "unit": "path-samples/s",
+                 "latency_s": {c: {"n": len(v), "p50": pct(v, 50), "p99": pct(v, 99), "max": max(v) if v else None}
+                               for c, v in plat.items()},
+                 "discipline": "one job at a time in arrival order, render_pass in chunks of 2..64 spp sized to "
+                               "about 1.5 s (serve/queue.rs:599-617), film read to host"}
+
     # Error of each class's first served film against the FP64 oracle (an
     # FP64-accumulated 65,536-spp render of ORACLE_ROWS rows at mid-frame
     # through a band camera, independent seed); serve hands back camera RGB,
@@ -738,7 +784,9 @@ def run_serve(args, world, rank, device):
             "config": {"workload": f"serve_trace_{rate:g}rps_{args.serve_seconds:g}s", "requests": len(trace),
                        "classes": {k: list(v[1:]) for k, v in W.SERVE_CLASSES.items()},
                        "pieces_triangles": [int(m.num_tris) for m in meshes], "alloys": list(W.SERVE_ALLOYS),
-                       "offered_path_samples_per_s": offered, "step_path_samples": 1 << 25,
+                       "offered_path_samples_per_s": offered, "step_path_samples": args.serve_step,
+                       "step_path_samples_max": args.serve_step_max or 2 * args.serve_step,
+                       "aging_ms": args.serve_aging_ms or 1000, "overlap": not args.serve_no_overlap,
                        "parallelism": f"replicas{world}",
                        "timing": "wall clock of the serve loop (latency is a wall-clock quantity); each step "
                                  "synchronises its batch"},
@@ -748,11 +796,69 @@ def run_serve(args, world, rank, device):
             "e2e": {"value": value, "unit": "path-samples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": d2h / max(1, len(finished)), "note": "per request: films read to host"},
             "gpu_launches": int(launches),
+            "plain_form": plain,
             "error_vs_fp64_oracle": {"oracle": f"rows h/2..h/2+{ORACLE_ROWS} of each class's first served "
                                                f"request, FP64 film, {ORACLE_SPP} spp on the device",
                                      "classes": acc} if acc else None,
         }
         print(json.dumps(out), flush=True)
+
+
+def serve_plain(ctx, trace, scenes, cams, ps):
+    """argent's own serve discipline on the GPU, for comparison with the
+    continuous-batching scheduler on the same request stream: one job at a
+    time in arrival order, each rendered by render_pass in chunks that start
+    at 2 spp and adapt to about 1.5 s each (capped at 64 spp), then read to
+    host memory (serve/queue.rs:599-617).  Returns (path-samples/s,
+    {class: latencies})."""
+    import queue
+
+    from argent_b200 import workloads as W
+    from argent_b200.gpu import Film, render_pass
+
+    q = queue.Queue()
+    t0 = time.perf_counter()
+
+    def driver():
+        for (ta, cname, i, j) in trace:
+            dt = t0 + ta - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            q.put((time.perf_counter(), cname, i, j))
+        q.put(None)
+
+    th = threading.Thread(target=driver)
+    th.start()
+    lat = {c: [] for c in W.SERVE_CLASSES}
+    films = {}
+    served, t_last = 0, t0
+    while True:
+        item = q.get()
+        if item is None:
+            break
+        t_sub, cname, i, j = item
+        _, w, h, spp, _ = W.SERVE_CLASSES[cname]
+        f = films.get((w, h))
+        if f is None:
+            f = films[(w, h)] = Film(ctx, w, h)
+        f.clear()
+        done, chunk = 0, 2
+        while done < spp:
+            n = min(chunk, spp - done)
+            t = time.perf_counter()
+            render_pass(ctx, scenes[(i, j)], cams[(i, cname)], f, ps, n, 7)
+            ctx.sync()
+            per = (time.perf_counter() - t) / n
+            done += n
+            chunk = int(min(max(1.5 / max(per, 1e-4), 1), 64))
+        f.read()
+        t_last = time.perf_counter()
+        lat[cname].append(t_last - t_sub)
+        served += w * h * spp
+    th.join()
+    for f in films.values():
+        f.close()
+    return served / (t_last - t0), lat
 
 
 def ctx_wave_mb(args):
@@ -770,11 +876,16 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-oracle", action="store_true", help="skip the FP64 65,536-spp error measurement")
+    ap.add_argument("--no-plain", action="store_true", help="serve_trace: skip the one-job-at-a-time comparison")
     ap.add_argument("--spp", type=int, default=0, help="override spp (short profiling runs)")
     ap.add_argument("--lanes", type=int, default=0, help="concurrent waves (0 = the library default)")
     ap.add_argument("--wave-paths", type=int, default=0, help="path slots per wave (0 = the library default)")
-    ap.add_argument("--serve-rate", type=float, default=1.0, help="serve_trace: requests per second")
+    ap.add_argument("--serve-rate", type=float, default=4.0, help="serve_trace: requests per second")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serve_trace: trace length")
+    ap.add_argument("--serve-step", type=int, default=1 << 26, help="serve_trace: least path-samples per step")
+    ap.add_argument("--serve-step-max", type=int, default=0, help="serve_trace: most path-samples per step")
+    ap.add_argument("--serve-aging-ms", type=int, default=0, help="serve_trace: aging period (0 = default)")
+    ap.add_argument("--serve-no-overlap", action="store_true", help="serve_trace: wait for each step's batch")
     args = ap.parse_args()
     if args.impl == "reference":
         # CPU only: rank 0 measures, the other ranks have nothing to do.

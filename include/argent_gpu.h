@@ -209,9 +209,13 @@ typedef struct ArgentLimits {
 
 /* Film flags. */
 enum {
-  ARGENT_FILM_KAHAN = 1, /* FP32 sums with Kahan compensation (default) */
-  ARGENT_FILM_FP64 = 2   /* FP64 sums (oracle-grade accumulation) */
+  ARGENT_FILM_KAHAN = 1,      /* FP32 sums with Kahan compensation (default) */
+  ARGENT_FILM_FP64 = 2,       /* FP64 sums (oracle-grade accumulation) */
+  ARGENT_FILM_PROGRESSIVE = 4 /* with KAHAN: FP64 sums join once a pass takes the film past
+                                 ARGENT_FILM_FP64_AFTER samples (long progressive renders),
+                                 seeded with the compensated FP32 sums */
 };
+#define ARGENT_FILM_FP64_AFTER 4096
 
 /* ------------------------------------------------------------------ */
 /* Context, piece, scene, film.                                       */
@@ -480,14 +484,23 @@ int argent_mesh_smooth(const float* positions, uint32_t nv, const uint32_t* tris
  * one job at a time, render_pass in chunks sized for ~1.5 s, seed 7, a
  * cancel check between chunks) and its progressive live passes
  * (serve/live.rs:747, 767).  Here all requests in flight advance together:
- * each argent_serve_step is one argent_render_batch in which the active
- * requests, lowest priority value first and then in submission order, take
- * whole samples of their frame up to step_path_samples (the first at least
- * one).  Chunks continue each film's sample indices, so a finished film
- * holds what one argent_render_pass of `spp` samples with the same seed
- * gives (up to the order of the FP32 sums).
+ * each argent_serve_step issues one batch (as argent_render_batch) in which
+ * the active requests, most urgent first, take whole samples of their frame
+ * up to the step's budget.  Urgency is the priority value minus the time
+ * waited over aging_ms (lower first; ties in submission order).  The budget
+ * is a quarter of the pending work, between step_path_samples and
+ * step_path_samples_max; a request whose remaining work is under a sixteenth
+ * of it finishes in that batch, and every active request advances by at
+ * least one sample.  Chunks continue each film's sample indices, so a
+ * finished film holds what one argent_render_pass of `spp` samples with the
+ * same seed gives (up to the order of the FP32 sums).
  *
- * Admission: a queued request becomes active, in the same order, while
+ * With `overlap` set, a step issues its batch while the previous one still
+ * runs (at most two in flight) and waits only for the older one, so the
+ * device does not drain between steps; without it each step waits for its
+ * own batch.
+ *
+ * Admission: a queued request becomes active, in urgency order, while
  * fewer than max_active are active and its film fits in film_budget
  * together with the films in use and pooled (pooled films of other sizes
  * are freed first).  Films are pooled by (width, height, flags).
@@ -501,8 +514,12 @@ typedef struct ArgentServe ArgentServe;
 typedef struct ArgentServeConfig {
   uint64_t film_budget;       /* device bytes for films in use and pooled; 0 = 8 GiB */
   uint32_t max_active;        /* requests rendered together; 0 = 64 */
+  uint32_t aging_ms;          /* waiting this long raises a request one priority level; 0 = 1000 */
+  uint64_t step_path_samples; /* least path-samples per step; 0 = 2^26 (about 45 ms of rendering) */
+  uint64_t step_path_samples_max; /* a step takes a quarter of the pending work, up to this;
+                                     0 = 2 x step_path_samples */
+  uint32_t overlap;           /* 1 = keep the next batch in flight while one runs */
   uint32_t reserved;
-  uint64_t step_path_samples; /* path-samples per step; 0 = 2^25 (about 30 ms of rendering) */
 } ArgentServeConfig;
 
 typedef struct ArgentServeRequest {
@@ -538,16 +555,20 @@ void argent_serve_destroy(ArgentServe* serve);
 /* Queues a request.  ARGENT_E_BUSY if its film alone exceeds film_budget. */
 int argent_serve_submit(ArgentServe* serve, const ArgentServeRequest* req, uint64_t* ticket);
 int argent_serve_poll(ArgentServe* serve, uint64_t ticket, ArgentServeStatus* status);
-/* Marks a queued or active request; it is cancelled at the next step. */
+/* Marks a queued or active request; it is cancelled at the next step that
+ * finds none of its batches in flight. */
 int argent_serve_cancel(ArgentServe* serve, uint64_t ticket);
-/* One scheduling round: cancellations, admission, one batch (waits for it),
- * completions.  *pending (may be NULL) = requests still queued or active.
- * A failed batch marks its requests ARGENT_REQ_FAILED and returns the code. */
+/* One scheduling round: completions of finished batches, cancellations,
+ * admission, one batch issued, and a wait for its batch (or, with overlap,
+ * for the older batch in flight).  *pending (may be NULL) = requests still
+ * queued or active.  A failed batch marks its requests ARGENT_REQ_FAILED
+ * and returns the code. */
 int argent_serve_step(ArgentServe* serve, uint32_t* pending);
 /* Averages of a finished request's film (as argent_film_read; any pointer
  * may be NULL), then forgets the request and pools its film. */
 int argent_serve_read(ArgentServe* serve, uint64_t ticket, float* color, float* albedo, float* normal);
-/* Forgets a finished, cancelled or failed request without reading it. */
+/* Forgets a finished, cancelled or failed request without reading it
+ * (ARGENT_E_BUSY while a batch holding a chunk of it still runs). */
 int argent_serve_release(ArgentServe* serve, uint64_t ticket);
 /* Steps that ran a batch, path-samples rendered, film bytes in use. */
 int argent_serve_stats(ArgentServe* serve, uint64_t* steps, uint64_t* path_samples, uint64_t* film_bytes_in_use);

@@ -40,7 +40,10 @@ def _cam(wl, w, h):
     return cam
 
 
-def test_mix_equals_alone(ring_setup):
+@pytest.mark.parametrize("overlap", [False, True])
+def test_mix_equals_alone(ring_setup, overlap):
+    """Every request of a mix equals its standalone render, with batches run
+    one at a time or two in flight."""
     from argent_b200.gpu import Serve
 
     ctx, _, scenes, wl = ring_setup
@@ -48,7 +51,7 @@ def test_mix_equals_alone(ring_setup):
             ("gold14k", 48, 48, 24, 1, 0)]
     # A small step budget splits every request into several chunks that
     # share batches with the others.
-    srv = Serve(ctx, step_path_samples=40000)
+    srv = Serve(ctx, step_path_samples=40000, step_path_samples_max=40000, overlap=overlap)
     tickets = []
     for alloy, w, h, spp, seed, prio in reqs:
         tickets.append(srv.submit(scenes[alloy], _cam(wl, w, h), W.settings(8), w, h, spp, seed, prio))
