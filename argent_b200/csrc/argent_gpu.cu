@@ -267,6 +267,8 @@ void argent_ctx_destroy(ArgentCtx* ctx) {
   for (int l = 0; l < ARGENT_LANES; ++l) ctx->wave[l].release();
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->resolve) cudaFree(ctx->resolve);
+  if (ctx->d_jobs_buf) cudaFree(ctx->d_jobs_buf);
+  for (auto& g : ctx->graph_cache) cudaGraphExecDestroy(g.exec);
   for (int l = 0; l < ARGENT_LANES; ++l)
     if (ctx->lane_stream[l]) cudaStreamDestroy(ctx->lane_stream[l]);
   if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
@@ -285,6 +287,7 @@ int argent_ctx_sync(ArgentCtx* ctx) {
   for (int l = 0; l < ARGENT_LANES; ++l)
     if (ctx->lane_stream[l]) ARGENT_CK(ctx, cudaStreamSynchronize(ctx->lane_stream[l]));
   if (ctx->aux_stream) ARGENT_CK(ctx, cudaStreamSynchronize(ctx->aux_stream));
+  ctx->overlapped_pending = false;
   return ctx_check_status(ctx);
 }
 
@@ -1115,14 +1118,30 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
     rc = ensure_wave(ctx, (start + k) % nlanes, cap);
     if (rc != ARGENT_OK) return rc;
   }
+  // Joined batches (done == null) read their job records from a buffer the
+  // context keeps; overlapped ones from their own, freed when they finish.
+  const bool joined = done == nullptr;
   dev::DevJob* d_jobs = nullptr;
-  ARGENT_CK(ctx, cudaMallocAsync((void**)&d_jobs, jobs.size() * sizeof(dev::DevJob), ctx->stream));
+  if (joined) {
+    if (ctx->d_jobs_cap < jobs.size()) {
+      if (ctx->d_jobs_buf) {
+        ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->d_jobs_buf);
+      }
+      ctx->d_jobs_buf = nullptr;
+      ctx->d_jobs_cap = 0;
+      size_t n = std::max<size_t>(jobs.size(), 64);
+      if (cudaMalloc((void**)&ctx->d_jobs_buf, n * sizeof(dev::DevJob)) != cudaSuccess)
+        return set_error(ctx, ARGENT_E_OOM, "job records: out of device memory");
+      ctx->d_jobs_cap = n;
+    }
+    d_jobs = ctx->d_jobs_buf;
+  } else {
+    ARGENT_CK(ctx, cudaMallocAsync((void**)&d_jobs, jobs.size() * sizeof(dev::DevJob), ctx->stream));
+  }
   // Pageable source: the call returns once the bytes are staged.
   ARGENT_CK(ctx, cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(dev::DevJob), cudaMemcpyHostToDevice,
                                  ctx->stream));
-  ARGENT_CK(ctx, cudaEventRecord(ctx->fork_ev, ctx->stream));
-  for (int k = 0; k < used; ++k)
-    ARGENT_CK(ctx, cudaStreamWaitEvent(ctx->lane_stream[(start + k) % nlanes], ctx->fork_ev, 0));
   dev::WaveArgs args[ARGENT_LANES];
   for (int l = 0; l < ARGENT_LANES; ++l) {
     args[l] = dev::WaveArgs{};
@@ -1137,12 +1156,11 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   int g_any[2] = {grid_for(ctx, (const void*)dev::k_shadow<false>, 128, cap),
                   grid_for(ctx, (const void*)dev::k_shadow<true>, 128, cap)};
   int g_film = grid_for(ctx, (const void*)dev::k_film, 256, cap);
+  // Per wave: its classes and, for a one-scene wave, that scene.
+  std::vector<uint32_t> wclasses(waves.size());
+  std::vector<const ArgentScene*> wone(waves.size());
   for (size_t wi = 0; wi < waves.size(); ++wi) {
     const dev::WaveDesc& w = waves[wi];
-    int lane = (int)((start + wi) % nlanes);
-    cudaStream_t st = ctx->lane_stream[lane];
-    dev::WaveArgs& a = args[lane];
-    const WaveBuffers& wb = ctx->wave[lane];
     uint32_t classes = 1u << CLS_TERMINAL;
     const ArgentScene* one = job_scenes[w.seg[0].job];
     for (uint32_t sgi = 0; sgi < w.num_segments; ++sgi) {
@@ -1150,72 +1168,171 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
       classes |= sc->host.class_mask;
       if (sc != one) one = nullptr;
     }
-    const int uni = one ? 1 : 0;
-    a.uscene = one ? one->d_scene : nullptr;
-    a.upiece = one ? one->host.piece : dev::DevPiece{};
-    a.u_has_turn = one ? one->host.has_turn : 0;
-    a.u_to_obj_s = one ? one->host.to_obj_s : 0.0f;
-    a.u_to_obj_c = one ? one->host.to_obj_c : 1.0f;
-    a.q_in = wb.q0;
-    a.q_out = wb.q1;
-    {
-      ProfScope ps(ctx, KC_RAYGEN, st);
-      dev::k_raygen<<<g_ray, 256, 0, st>>>(a, w);
-    }
-    ctx->launches++;
-    for (uint32_t depth = 0; depth < depths[wi] && depth < ARGENT_MAX_DEPTH; ++depth) {
-      a.q_in = (depth & 1) ? wb.q1 : wb.q0;
-      a.q_out = (depth & 1) ? wb.q0 : wb.q1;
-      {
-        ProfScope ps(ctx, KC_INTERSECT, st);
-        if (uni)
-          dev::k_intersect<true><<<g_int[1], 128, 0, st>>>(a, (int)depth);
-        else
-          dev::k_intersect<false><<<g_int[0], 128, 0, st>>>(a, (int)depth);
-      }
-      {
-        ProfScope ps(ctx, KC_SHADE, st);
-        if (classes & (1u << CLS_TERMINAL)) dev::k_shade<CLS_TERMINAL><<<g_sh, 128, 0, st>>>(a, (int)depth);
-        if (classes & (1u << CLS_METAL)) dev::k_shade<CLS_METAL><<<g_sh, 128, 0, st>>>(a, (int)depth);
-        if (classes & (1u << CLS_COATED)) dev::k_shade<CLS_COATED><<<g_sh, 128, 0, st>>>(a, (int)depth);
-        if (classes & (1u << CLS_DIELECTRIC)) dev::k_shade<CLS_DIELECTRIC><<<g_sh, 128, 0, st>>>(a, (int)depth);
-        if (classes & (1u << CLS_OTHER)) dev::k_shade<CLS_OTHER><<<g_sh, 128, 0, st>>>(a, (int)depth);
-        ctx->launches += __builtin_popcount(classes) - 1;
-      }
-      {
-        ProfScope ps(ctx, KC_SHADOW, st);
-        if (uni)
-          dev::k_shadow<true><<<g_any[1], 128, 0, st>>>(a, (int)depth);
-        else
-          dev::k_shadow<false><<<g_any[0], 128, 0, st>>>(a, (int)depth);
-      }
-      ctx->launches += 3;
-    }
-    if (ctx->counting) {
-      dev::k_count_bounces<<<1, ARGENT_MAX_DEPTH, 0, st>>>(wb.counters, (int)std::min<uint32_t>(depths[wi],
-                                                                                            ARGENT_MAX_DEPTH));
-      ctx->launches++;
-    }
-    // Films accumulate in wave order: wait for the previous wave's film pass.
-    if (ctx->last_film_lane >= 0 && ctx->last_film_lane != lane)
-      ARGENT_CK(ctx, cudaStreamWaitEvent(st, ctx->film_ev[ctx->last_film_lane], 0));
-    {
-      ProfScope ps(ctx, KC_FILM, st);
-      dev::k_film<<<g_film, 256, 0, st>>>(a, w);
-    }
-    ARGENT_CK(ctx, cudaEventRecord(ctx->film_ev[lane], st));
-    ctx->last_film_lane = lane;
-    ctx->launches++;
+    wclasses[wi] = classes;
+    wone[wi] = one;
   }
+  // The first film pass waits for the last one before this batch unless the
+  // context stream already orders it (a joined batch after joined ones).
+  const bool chain_first = !joined || ctx->overlapped_pending;
+  const int last_lane = (int)((start + waves.size() - 1) % nlanes);
+  cudaStream_t join = joined ? ctx->stream : ctx->aux_stream;
+
+  // Issues the batch: fork from the context stream, each wave's kernels on
+  // its lane, join.  Counts the kernels it launches.
+  auto issue = [&](uint64_t* kernels) -> cudaError_t {
+    cudaError_t e = cudaEventRecord(ctx->fork_ev, ctx->stream);
+    for (int k = 0; k < used && e == cudaSuccess; ++k)
+      e = cudaStreamWaitEvent(ctx->lane_stream[(start + k) % nlanes], ctx->fork_ev, 0);
+    int prev_film = chain_first ? ctx->last_film_lane : -1;
+    for (size_t wi = 0; wi < waves.size() && e == cudaSuccess; ++wi) {
+      const dev::WaveDesc& w = waves[wi];
+      int lane = (int)((start + wi) % nlanes);
+      cudaStream_t st = ctx->lane_stream[lane];
+      dev::WaveArgs& a = args[lane];
+      const WaveBuffers& wb = ctx->wave[lane];
+      const uint32_t classes = wclasses[wi];
+      const ArgentScene* one = wone[wi];
+      const int uni = one ? 1 : 0;
+      a.uscene = one ? one->d_scene : nullptr;
+      a.upiece = one ? one->host.piece : dev::DevPiece{};
+      a.u_has_turn = one ? one->host.has_turn : 0;
+      a.u_to_obj_s = one ? one->host.to_obj_s : 0.0f;
+      a.u_to_obj_c = one ? one->host.to_obj_c : 1.0f;
+      a.q_in = wb.q0;
+      a.q_out = wb.q1;
+      {
+        ProfScope ps(ctx, KC_RAYGEN, st);
+        dev::k_raygen<<<g_ray, 256, 0, st>>>(a, w);
+      }
+      ++*kernels;
+      for (uint32_t depth = 0; depth < depths[wi] && depth < ARGENT_MAX_DEPTH; ++depth) {
+        a.q_in = (depth & 1) ? wb.q1 : wb.q0;
+        a.q_out = (depth & 1) ? wb.q0 : wb.q1;
+        {
+          ProfScope ps(ctx, KC_INTERSECT, st);
+          if (uni)
+            dev::k_intersect<true><<<g_int[1], 128, 0, st>>>(a, (int)depth);
+          else
+            dev::k_intersect<false><<<g_int[0], 128, 0, st>>>(a, (int)depth);
+        }
+        {
+          ProfScope ps(ctx, KC_SHADE, st);
+          if (classes & (1u << CLS_TERMINAL)) dev::k_shade<CLS_TERMINAL><<<g_sh, 128, 0, st>>>(a, (int)depth);
+          if (classes & (1u << CLS_METAL)) dev::k_shade<CLS_METAL><<<g_sh, 128, 0, st>>>(a, (int)depth);
+          if (classes & (1u << CLS_COATED)) dev::k_shade<CLS_COATED><<<g_sh, 128, 0, st>>>(a, (int)depth);
+          if (classes & (1u << CLS_DIELECTRIC)) dev::k_shade<CLS_DIELECTRIC><<<g_sh, 128, 0, st>>>(a, (int)depth);
+          if (classes & (1u << CLS_OTHER)) dev::k_shade<CLS_OTHER><<<g_sh, 128, 0, st>>>(a, (int)depth);
+          *kernels += __builtin_popcount(classes);
+        }
+        {
+          ProfScope ps(ctx, KC_SHADOW, st);
+          if (uni)
+            dev::k_shadow<true><<<g_any[1], 128, 0, st>>>(a, (int)depth);
+          else
+            dev::k_shadow<false><<<g_any[0], 128, 0, st>>>(a, (int)depth);
+        }
+        *kernels += 2;
+      }
+      if (ctx->counting) {
+        dev::k_count_bounces<<<1, ARGENT_MAX_DEPTH, 0, st>>>(wb.counters, (int)std::min<uint32_t>(depths[wi],
+                                                                                              ARGENT_MAX_DEPTH));
+        ++*kernels;
+      }
+      // Films accumulate in wave order: wait for the previous wave's film pass.
+      if (prev_film >= 0 && prev_film != lane) e = cudaStreamWaitEvent(st, ctx->film_ev[prev_film], 0);
+      {
+        ProfScope ps(ctx, KC_FILM, st);
+        dev::k_film<<<g_film, 256, 0, st>>>(a, w);
+      }
+      if (e == cudaSuccess) e = cudaEventRecord(ctx->film_ev[lane], st);
+      prev_film = lane;
+      ++*kernels;
+    }
+    for (int k = 0; k < used && e == cudaSuccess; ++k) {
+      e = cudaEventRecord(ctx->join_ev, ctx->lane_stream[(start + k) % nlanes]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(join, ctx->join_ev, 0);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return e;
+  };
+
+  cudaError_t e = cudaSuccess;
+  uint64_t kernels = 0;
+  // A joined batch without instrumentation is captured once as a CUDA graph
+  // and replayed while the same waves come again (a render repeated with new
+  // films, cameras or seeds changes only the job records).
+  const bool graphs = joined && !chain_first && !ctx->prof.on && !ctx->counting && ctx->graphs_on;
+  if (graphs) {
+    std::vector<uint8_t> key;
+    auto put = [&](const void* p, size_t n) {
+      const uint8_t* b = (const uint8_t*)p;
+      key.insert(key.end(), b, b + n);
+    };
+    put(&nlanes, sizeof(nlanes));
+    put(&start, sizeof(start));
+    put(&cap, sizeof(cap));
+    put(&d_jobs, sizeof(d_jobs));
+    for (int k = 0; k < used; ++k) put(&args[(start + k) % nlanes], sizeof(dev::WaveArgs));
+    for (size_t wi = 0; wi < waves.size(); ++wi) {
+      const dev::WaveDesc& w = waves[wi];
+      put(&w.num_segments, sizeof(w.num_segments));
+      put(&w.num_slots, sizeof(w.num_slots));
+      put(w.seg, w.num_segments * sizeof(dev::DevSegment));
+      put(&depths[wi], sizeof(uint32_t));
+      put(&wclasses[wi], sizeof(uint32_t));
+      const ArgentScene* one = wone[wi];
+      const void* sp = one ? (const void*)one->d_scene : nullptr;
+      put(&sp, sizeof(sp));
+      if (one) {
+        put(&one->host.piece, sizeof(one->host.piece));
+        put(&one->host.has_turn, sizeof(one->host.has_turn));
+        put(&one->host.to_obj_s, sizeof(float));
+        put(&one->host.to_obj_c, sizeof(float));
+      }
+    }
+    ArgentCtx::GraphEntry* hit = nullptr;
+    for (auto& g : ctx->graph_cache)
+      if (g.key == key) hit = &g;
+    if (!hit) {
+      cudaGraph_t graph = nullptr;
+      cudaGraphExec_t exec = nullptr;
+      e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        cudaError_t ie = issue(&kernels);
+        e = cudaStreamEndCapture(ctx->stream, &graph);
+        if (ie != cudaSuccess) e = ie;
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+      if (graph) cudaGraphDestroy(graph);
+      if (e != cudaSuccess) {
+        if (exec) cudaGraphExecDestroy(exec);
+        return set_error(ctx, ARGENT_E_CUDA, std::string("render graph: ") + cudaGetErrorString(e));
+      }
+      if (ctx->graph_cache.size() >= ARGENT_GRAPH_CACHE) {
+        auto lru = std::min_element(ctx->graph_cache.begin(), ctx->graph_cache.end(),
+                                    [](const ArgentCtx::GraphEntry& x, const ArgentCtx::GraphEntry& y) {
+                                      return x.last_use < y.last_use;
+                                    });
+        cudaGraphExecDestroy(lru->exec);
+        ctx->graph_cache.erase(lru);
+      }
+      ctx->graph_cache.push_back(ArgentCtx::GraphEntry{std::move(key), exec, kernels, 0});
+      hit = &ctx->graph_cache.back();
+    }
+    hit->last_use = ++ctx->graph_clock;
+    e = cudaGraphLaunch(hit->exec, ctx->stream);
+    kernels = hit->kernels;
+  } else {
+    e = issue(&kernels);
+  }
+  ctx->launches += kernels;
   ctx->next_lane = (int)((start + waves.size()) % nlanes);
-  cudaStream_t join = done ? ctx->aux_stream : ctx->stream;
-  for (int k = 0; k < used; ++k) {
-    ARGENT_CK(ctx, cudaEventRecord(ctx->join_ev, ctx->lane_stream[(start + k) % nlanes]));
-    ARGENT_CK(ctx, cudaStreamWaitEvent(join, ctx->join_ev, 0));
+  ctx->last_film_lane = last_lane;
+  if (!joined) {
+    cudaFreeAsync(d_jobs, join);
+    if (e == cudaSuccess) e = cudaEventRecord(done, join);
+    ctx->overlapped_pending = true;
   }
-  cudaError_t e = cudaGetLastError();
-  cudaFreeAsync(d_jobs, join);
-  if (done) ARGENT_CK(ctx, cudaEventRecord(done, join));
   if (e != cudaSuccess) return set_error(ctx, ARGENT_E_CUDA, std::string("render launch: ") + cudaGetErrorString(e));
   return ARGENT_OK;
 }
@@ -1887,6 +2004,18 @@ int argent_ctx_kernel_times(ArgentCtx* ctx, double* ms, uint64_t* launches) {
   for (int k = 0; k < KC_COUNT; ++k) {
     ms[k] = ctx->prof.ms[k];
     launches[k] = ctx->prof.n[k];
+  }
+  return ARGENT_OK;
+}
+
+int argent_ctx_set_graphs(ArgentCtx* ctx, int on) {
+  if (!ctx) return set_error(nullptr, ARGENT_E_INVALID, "ctx is NULL");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  ctx->graphs_on = on != 0;
+  if (!ctx->graphs_on) {
+    ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    for (auto& g : ctx->graph_cache) cudaGraphExecDestroy(g.exec);
+    ctx->graph_cache.clear();
   }
   return ARGENT_OK;
 }

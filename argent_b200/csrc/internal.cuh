@@ -132,6 +132,7 @@ struct KernelProfile {
 // SMs that another wave's kernel tails and small late-bounce launches leave
 // idle.  Lane 0 runs on the context stream.
 #define ARGENT_LANES 16
+#define ARGENT_GRAPH_CACHE 8
 
 struct ArgentCtx {
   int device = 0;
@@ -144,8 +145,24 @@ struct ArgentCtx {
   // wave before it (on last_film_lane), so films accumulate in wave order
   // also when batches overlap.
   int next_lane = 0, last_film_lane = -1;
-  // Completion stream of batches that do not join the context stream.
+  // Completion stream of batches that do not join the context stream, and
+  // whether one may still run (cleared by argent_ctx_sync).
   cudaStream_t aux_stream = nullptr;
+  bool overlapped_pending = false;
+  // Job records of joined batches (kept, so captured graphs can point at it).
+  dev::DevJob* d_jobs_buf = nullptr;
+  size_t d_jobs_cap = 0;
+  // Captured batches: the launch sequence of a joined batch, keyed by
+  // everything its kernel parameters depend on, least recently used evicted.
+  struct GraphEntry {
+    std::vector<uint8_t> key;
+    cudaGraphExec_t exec;
+    uint64_t kernels;
+    uint64_t last_use;
+  };
+  std::vector<GraphEntry> graph_cache;
+  uint64_t graph_clock = 0;
+  bool graphs_on = true;
   int num_sms = 148;
   int lanes = 8;
   bool counting = false;  // traversal instrumentation on (argent_ctx_set_counting)

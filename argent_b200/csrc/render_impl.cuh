@@ -513,8 +513,12 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
   V3 ro{of.x, of.y, of.z}, rd{df.x, df.y, df.z};
   float prev_pdf = df.w;
   Spec beta = spec4(a.beta[slot]);
-  Spec L = spec4(a.L[slot]);
-  float4 lf = a.lambda[slot], pf = a.pdf[slot];
+  // Radiance changes here only for terminal hits and floor fade misses, and
+  // the wavelength pdfs only when a dispersive refraction terminates the
+  // secondaries: the other classes read and write them only where they do.
+  constexpr bool kPdf = KM_HAS(KM, B_DIELECTRIC);
+  Spec L = CLS == CLS_TERMINAL ? spec4(a.L[slot]) : spec(0.0f);
+  float4 lf = a.lambda[slot], pf = kPdf ? a.pdf[slot] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   Wavelengths wl{{lf.x, lf.y, lf.z, lf.w}, {pf.x, pf.y, pf.z, pf.w}};
   bool clamp = rough_seen;
   float cl = job.clamp_indirect;
@@ -564,7 +568,9 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
         float pl = sc->env_pick * envmap_pdf(sc, rd);
         w = prev_pdf * prev_pdf / (prev_pdf * prev_pdf + pl * pl);
       }
+      if constexpr (CLS != CLS_TERMINAL) L = spec4(a.L[slot]);
       add_clamped(&L, beta * env_eval(sc, rd, wl) * w, clamp, cl);
+      if constexpr (CLS != CLS_TERMINAL) a.L[slot] = to_f4(L);
       done = true;
     } else {
       V3 n = rd.y < 0.0f ? V3{0.0f, 1.0f, 0.0f} : V3{0.0f, -1.0f, 0.0f};
@@ -788,7 +794,7 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
     out.alive = cont && ((uint32_t)depth + 1u < job.max_depth);
     // Store the state the next bounce (or the film) reads.
     a.beta[slot] = to_f4(beta);
-    a.pdf[slot] = make_float4(wl.pdf[0], wl.pdf[1], wl.pdf[2], wl.pdf[3]);
+    if constexpr (kPdf) a.pdf[slot] = make_float4(wl.pdf[0], wl.pdf[1], wl.pdf[2], wl.pdf[3]);
     if (out.alive) {
       a.o[slot] = make_float4(ro.x, ro.y, ro.z, 0.0f);
       a.d[slot] = make_float4(rd.x, rd.y, rd.z, prev_pdf);
@@ -798,7 +804,7 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
     }
   }
   }
-  a.L[slot] = to_f4(L);
+  if constexpr (CLS == CLS_TERMINAL) a.L[slot] = to_f4(L);
   return out;
 }
 

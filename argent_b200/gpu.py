@@ -78,6 +78,10 @@ class Context:
     def set_counting(self, on):
         self.check(self.lib.argent_ctx_set_counting(self.h, 1 if on else 0))
 
+    def set_graphs(self, on):
+        """Capture and replay repeated renders as CUDA graphs (default on)."""
+        self.check(self.lib.argent_ctx_set_graphs(self.h, 1 if on else 0))
+
     def traversal_counts(self):
         out = (ctypes.c_uint64 * 6)()
         self.check(self.lib.argent_ctx_traversal_counts(self.h, out))

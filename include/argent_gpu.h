@@ -596,6 +596,10 @@ int argent_ctx_set_profiling(ArgentCtx* ctx, int on);
 /* Summed device time (ms) and launch count per kernel class since the last
  * reset; synchronises the stream.  ms and launches hold ARGENT_KC_COUNT. */
 int argent_ctx_kernel_times(ArgentCtx* ctx, double* ms, uint64_t* launches);
+/* Renders that are not overlapped and not instrumented are captured as CUDA
+ * graphs and replayed when the same waves come again (on by default); off
+ * also frees the captured graphs. */
+int argent_ctx_set_graphs(ArgentCtx* ctx, int on);
 /* Traversal visit counters: on = count, and reset to zero. */
 int argent_ctx_set_counting(ArgentCtx* ctx, int on);
 /* out[6] = closest-hit rays, nodes, triangles; any-hit rays, nodes,

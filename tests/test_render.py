@@ -294,3 +294,31 @@ def test_progressive_film_switches_to_fp64_past_4096_samples():
     a, b = prog.xyz(), fp64.xyz()
     assert np.allclose(a, b, rtol=1e-4, atol=1e-8), np.abs(a - b).max()
     assert np.allclose(a, kahan.xyz(), rtol=1e-4, atol=1e-8)
+
+
+@pytest.mark.gpu
+def test_graph_replay_equals_direct_launches():
+    """A repeated render replays its captured graph (new films, same waves);
+    every film equals the one rendered with graphs off, bit for bit."""
+    from argent_b200.gpu import Context, Film, Piece, Scene, render_pass
+
+    wl = W.ring_still()
+    ctx = Context(0)
+    piece = Piece(ctx, wl.mesh)
+    scene = Scene(ctx, piece, wl.desc)
+    ctx.set_graphs(False)
+    ref = Film(ctx, wl.width, wl.height)
+    render_pass(ctx, scene, wl.camera, ref, wl.settings, 8, wl.seed)
+    want = ref.xyz()
+    ctx.set_graphs(True)
+    n0 = ctx.kernel_launches
+    for _ in range(3):
+        f = Film(ctx, wl.width, wl.height)
+        render_pass(ctx, scene, wl.camera, f, wl.settings, 8, wl.seed)
+        assert np.array_equal(f.xyz(), want)
+    per = (ctx.kernel_launches - n0) // 3
+    assert per > 0 and ctx.kernel_launches - n0 == 3 * per
+    # a different seed changes only the job record: the graph replays it
+    g = Film(ctx, wl.width, wl.height)
+    render_pass(ctx, scene, wl.camera, g, wl.settings, 8, wl.seed + 1)
+    assert not np.array_equal(g.xyz(), want)
