@@ -1970,6 +1970,8 @@ static int render_batch(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n
   return ARGENT_OK;
 }
 
+bool scene_belongs(const ArgentScene* scene, const ArgentCtx* ctx) { return scene && scene->ctx == ctx; }
+
 int render_batch_overlapped(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n, cudaEvent_t done) {
   if (!done) return set_error(ctx, ARGENT_E_INVALID, "render_batch_overlapped: no completion event");
   return render_batch(ctx, items, n, done);

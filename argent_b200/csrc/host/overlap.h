@@ -11,6 +11,9 @@
 
 int render_batch_overlapped(ArgentCtx* ctx, const ArgentBatchItem* items, uint32_t n, cudaEvent_t done);
 
+// Whether `scene` was uploaded on `ctx`.
+bool scene_belongs(const ArgentScene* scene, const ArgentCtx* ctx);
+
 // The context's device status word (traversal stack or queue overflow,
 // expired waits) as a status code, cleared once read.
 int ctx_check_status(ArgentCtx* ctx);

@@ -230,7 +230,8 @@ double argent_serve_now(ArgentServe* s) { return s ? s->now() : 0.0; }
 int argent_serve_submit(ArgentServe* s, const ArgentServeRequest* req, uint64_t* ticket) {
   if (!s || !req || !ticket) return ARGENT_E_INVALID;
   if (!req->scene || req->width == 0 || req->height == 0 || req->spp == 0 ||
-      (uint64_t)req->width * req->height > (1ull << 31))
+      (uint64_t)req->width * req->height > (1ull << 31) || !scene_belongs(req->scene, s->ctx) ||
+      req->settings.max_depth > 64)
     return ARGENT_E_INVALID;
   uint64_t fb = film_bytes(req->width, req->height, req->film_flags);
   if (fb > s->cfg.film_budget) return ARGENT_E_BUSY;

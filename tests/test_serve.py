@@ -133,3 +133,23 @@ def test_cancel_between_steps(ring_setup):
     with pytest.raises(N.ArgentError):
         srv.read(t)
     srv.release(t)
+
+
+def test_submission_refuses_foreign_scenes_and_deep_paths(ring_setup):
+    """A request whose scene belongs to another context, or whose path depth
+    exceeds 64, is refused when submitted, not when its batch runs."""
+    from argent_b200.gpu import Context, Piece, Scene, Serve
+
+    ctx, _, scenes, wl = ring_setup
+    other = Context(0)
+    foreign = Scene(other, Piece(other, wl.mesh), wl.desc)
+    srv = Serve(ctx)
+    with pytest.raises(N.ArgentError):
+        srv.submit(foreign, _cam(wl, 64, 64), W.settings(8), 64, 64, 4, 7)
+    with pytest.raises(N.ArgentError):
+        srv.submit(scenes["sterling"], _cam(wl, 64, 64), W.settings(65), 64, 64, 4, 7)
+    t = srv.submit(scenes["sterling"], _cam(wl, 64, 64), W.settings(8), 64, 64, 4, 7)
+    srv.run()
+    assert srv.poll(t).state == N.REQ_DONE
+    srv.release(t)
+    srv.close()
