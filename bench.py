@@ -35,16 +35,21 @@ sys.path.insert(0, ROOT)
 PUBLISHED_CPU = 17.7e6  # README.md:5-6: 1920x1080 x 256 spp in ~30 s on 32 cores
 
 
-def dist_setup(n):
+def dist_setup(n, backend=None):
+    """One process per GPU (replicas): rank, world and local rank from the
+    launcher's environment; NCCL on GPUs, gloo where there are none.  The
+    group's timeout is short so that ranks waiting on a lost peer end."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
+        import torch
         import torch.distributed as td
         from datetime import timedelta
 
-        backend = "nccl"
-        td.init_process_group(backend, timeout=timedelta(seconds=600))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        td.init_process_group(backend, timeout=timedelta(seconds=120))
     return world, rank, local
 
 
@@ -52,18 +57,26 @@ def barrier(world, device=None):
     if world > 1:
         import torch.distributed as td
 
-        td.barrier(device_ids=[device] if device is not None else None)
+        td.barrier(device_ids=[device] if device is not None and td.get_backend() == "nccl" else None)
 
 
 def max_over_ranks(x, world, device):
+    """The largest of every rank's x (timings are taken as the max over ranks)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as td
 
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+    on_gpu = device is not None and td.get_backend() == "nccl"
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}" if on_gpu else "cpu")
     td.all_reduce(t, op=td.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_rate(world, units_per_rank, seconds_max):
+    """Replicas: every rank processes the same units; the job's rate is all
+    ranks' units over the slowest rank's time."""
+    return world * units_per_rank / seconds_max
 
 
 class Clocks:
@@ -516,7 +529,7 @@ def run_gpu(args, world, rank, device):
     ms_max = max_over_ranks(ms, world, device)
     barrier(world, device)
     samples_per_step = plan.path_samples
-    value = world * samples_per_step * args.steps / (ms_max / 1000.0)
+    value = whole_job_rate(world, samples_per_step * args.steps, ms_max / 1000.0)
 
     # Roofline of the dominant kernel: closest-hit traversal, the largest
     # share of serialised device time in the ncu launch list
