@@ -809,12 +809,20 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
 }
 
 // Surface shading is capped at 128 registers (4 blocks of 128 per SM)
-// instead of up to ~166, trading a little spilling for residency.
+// instead of up to ~166, trading a little spilling for residency; lower
+// caps spill the metal and coated classes heavily and run slower.
 #ifndef ARGENT_SHADE_BLOCKS
 #define ARGENT_SHADE_BLOCKS 4
 #endif
+// The dielectric class fits 96 registers without spilling: 5 blocks.
+#ifndef ARGENT_SHADE_BLOCKS_DIELECTRIC
+#define ARGENT_SHADE_BLOCKS_DIELECTRIC 5
+#endif
 template <int CLS>
-__global__ void __launch_bounds__(128, CLS == CLS_TERMINAL ? 1 : ARGENT_SHADE_BLOCKS) k_shade(WaveArgs a, int depth) {
+__global__ void __launch_bounds__(128, CLS == CLS_TERMINAL      ? 1
+                                       : CLS == CLS_DIELECTRIC ? ARGENT_SHADE_BLOCKS_DIELECTRIC
+                                                               : ARGENT_SHADE_BLOCKS)
+    k_shade(WaveArgs a, int depth) {
   uint32_t count = a.counters[CNT_CLS(depth, CLS)];
   const uint32_t* q = a.qc + (size_t)CLS * a.cap;
   uint32_t cap = a.cap;
