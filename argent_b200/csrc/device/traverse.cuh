@@ -420,6 +420,13 @@ struct AnyTrav {
 #define ARGENT_ANY_HIT 1
 #define ARGENT_ANY_CLEAR 2
 
+// The test any_begin starts with: false when the piece is empty or the ray
+// (up to t_max) misses its box, so nothing of the piece can occlude it.
+__device__ __forceinline__ bool piece_may_occlude(const DevPiece& pc, V3 o, V3 d, float t_max) {
+  if (pc.num_tris == 0) return false;
+  return node_box_hit(pc.nodes, 0u, make_rayq(o, d), t_max);
+}
+
 // Returns ARGENT_ANY_RUNNING, or ARGENT_ANY_CLEAR when the ray misses the
 // piece outright.
 __device__ __forceinline__ int any_begin(const DevPiece& pc, AnyTrav& s, uint32_t* stack, V3 o, V3 d, float t_max) {

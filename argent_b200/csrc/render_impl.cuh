@@ -484,6 +484,20 @@ __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_intersect(WaveArgs 
   }
 }
 
+// A shadow ray that misses the piece's box is unoccluded: its contribution
+// is added here exactly as k_shadow adds a clear ray's (the stored radiance
+// plus c), and the ray is not queued.  The terminal class keeps its
+// radiance in `L` (stored at the end); the others read and write it here.
+template <int CLS>
+__device__ __forceinline__ void add_unoccluded(const WaveArgs& a, uint32_t slot, Spec* L, const Spec& c) {
+  if constexpr (CLS == CLS_TERMINAL) {
+    *L = *L + c;
+  } else {
+    float4 l = a.L[slot];
+    a.L[slot] = make_float4(l.x + c.v[0], l.y + c.v[1], l.z + c.v[2], l.w + c.v[3]);
+  }
+}
+
 struct ShadeOut {
   bool alive;
   bool shadow;
@@ -681,10 +695,14 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
                 oo = rot_y_sc(from, sc->to_obj_s, sc->to_obj_c);
                 od = rot_y_sc(dir, sc->to_obj_s, sc->to_obj_c);
               }
-              out.shadow = true;
-              out.sh_o = make_float4(oo.x, oo.y, oo.z, INFINITY);
-              out.sh_d = make_float4(od.x, od.y, od.z, __uint_as_float(slot));
-              out.sh_c = to_f4(c);
+              if (piece_may_occlude(sc->piece, oo, od, INFINITY)) {
+                out.shadow = true;
+                out.sh_o = make_float4(oo.x, oo.y, oo.z, INFINITY);
+                out.sh_d = make_float4(od.x, od.y, od.z, __uint_as_float(slot));
+                out.sh_c = to_f4(c);
+              } else {
+                add_unoccluded<CLS>(a, slot, &L, c);
+              }
             }
           }
         }
@@ -744,10 +762,14 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
                 oo = rot_y_sc(origin, sc->to_obj_s, sc->to_obj_c);
                 od = rot_y_sc(sdir, sc->to_obj_s, sc->to_obj_c);
               }
-              out.shadow = true;
-              out.sh_o = make_float4(oo.x, oo.y, oo.z, t_max);
-              out.sh_d = make_float4(od.x, od.y, od.z, __uint_as_float(slot));
-              out.sh_c = to_f4(c);
+              if (piece_may_occlude(sc->piece, oo, od, t_max)) {
+                out.shadow = true;
+                out.sh_o = make_float4(oo.x, oo.y, oo.z, t_max);
+                out.sh_d = make_float4(od.x, od.y, od.z, __uint_as_float(slot));
+                out.sh_c = to_f4(c);
+              } else {
+                add_unoccluded<CLS>(a, slot, &L, c);
+              }
             }
           }
         }
