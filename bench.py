@@ -162,6 +162,20 @@ def smi_index(device):
 
 # ------------------------------------------------------------------ reference arm (CPU)
 
+def cpu_model():
+    """The host CPU's model name (the CPU baseline's hardware)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or "unknown"
+
+
 def cpu_sample(wl, seconds=12.0, threads=0, rows=None):
     """argent's algorithm (the oracle) on a band of rows of the workload
     frame at the workload's spp.  Returns (samples/s, rows, threads)."""
@@ -303,7 +317,7 @@ def run_reference(args, world, rank):
         "ms_per_step": 1000.0 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": value / PUBLISHED_CPU, "dtype": "f32", "data": "synthetic",
         "config": cfg,
-        "cpu_baseline": {"value": value, "unit": "path-samples/s", "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": "path-samples/s", "cores": threads, "kind": "port", "cpu": cpu_model(),
                          "sample": sample + "; argent's Rust path cannot be built here (no cargo), so the C++ "
                                             "restatement (oracle/) runs, OpenMP over rows"},
         "e2e": {"value": value, "unit": "path-samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -630,7 +644,7 @@ def run_gpu(args, world, rank, device):
     if rank == 0 and world == 1 and not args.no_cpu:
         wl = plan.cpu_wl
         v, rows, nthr, cpu_scene = cpu_sample(wl, seconds=args.ref_seconds, threads=os.cpu_count() or 1)
-        cpu = {"value": v, "unit": "path-samples/s", "cores": nthr, "kind": "port",
+        cpu = {"value": v, "unit": "path-samples/s", "cores": nthr, "kind": "port", "cpu": cpu_model(),
                "sample": f"{wl.name}: rows {wl.height // 2}..{wl.height // 2 + rows} of the frame at {wl.spp} spp; "
                          f"argent's algorithm as restated in oracle/ (Rust reference not buildable here), "
                          f"OpenMP over rows"}
