@@ -223,7 +223,7 @@ int argent_ctx_create(int device, const ArgentLimits* limits, ArgentCtx** out) {
   ArgentCtx* ctx = new ArgentCtx();
   ctx->device = device;
   if (limits) ctx->limits = *limits;
-  if (ctx->limits.wave_paths == 0) ctx->limits.wave_paths = 1ull << 23;
+  if (ctx->limits.wave_paths == 0) ctx->limits.wave_paths = 1ull << 24;
   if (ctx->limits.wave_paths > (1ull << 30) || ctx->limits.lanes > ARGENT_LANES) {
     delete ctx;
     return set_error(nullptr, ARGENT_E_INVALID, "wave_paths above 2^30 or more than 16 lanes");
@@ -1853,7 +1853,7 @@ int argent_autotune(ArgentCtx* ctx, ArgentScene* scene, const ArgentCamera* came
   for (int l = 0; l < ARGENT_LANES; ++l) held += ctx->wave[l].bytes;
   uint64_t room = (uint64_t)fr / 2 + held;
   const uint32_t lanes_c[] = {2, 4, 8, 12, 16};
-  const uint64_t waves_c[] = {1ull << 21, 1ull << 22, 1ull << 23, 1ull << 24};
+  const uint64_t waves_c[] = {1ull << 21, 1ull << 22, 1ull << 23, 1ull << 24, 1ull << 25};
   uint64_t path_samples = (uint64_t)width * height * count;
   ArgentFilm* film = nullptr;
   int rc = argent_film_create(ctx, width, height, ARGENT_FILM_KAHAN, &film);
@@ -1868,7 +1868,7 @@ int argent_autotune(ArgentCtx* ctx, ArgentScene* scene, const ArgentCamera* came
   cudaEventCreate(&e1);
   for (uint32_t L : lanes_c) {
     for (uint64_t W : waves_c) {
-      if ((uint64_t)L * W * 224 > room) continue;
+      if ((uint64_t)L * W * 244 > room) continue;
       if (W > path_samples * 2 && W > (1ull << 21)) continue;  // waves larger than the render change nothing
       ctx->lanes = (int)L;
       ctx->limits.wave_paths = W;

@@ -494,7 +494,7 @@ def run_gpu(args, world, rank, device):
     from argent_b200.gpu import Context, Film
 
     torch.cuda.set_device(device)
-    ctx = Context(device, wave_paths=args.wave_paths, lanes=args.lanes)
+    ctx = Context(device, wave_paths=args.wave_paths or STILL_WAVE_PATHS, lanes=args.lanes)
     plan = ReelPlan(ctx) if args.workload == "reel_batch" else StillPlan(ctx, args.workload)
     if args.spp:
         plan.set_spp(args.spp)  # profiling runs only: the bench line uses the workload's spp
@@ -657,6 +657,7 @@ def run_gpu(args, world, rank, device):
         cfg.update({"parallelism": f"replicas{world}", "l2": "inputs larger than L2 (path state "
                     f"{ctx_wave_mb(args)} MB per wave x {args.lanes or 8} lanes + BVH/triangles "
                     f"{plan.device_bytes / 1e6:.0f} MB)",
+                    "context": {"lanes": ctx.config()[0], "wave_paths": ctx.config()[1]},
                     "vs_baseline_ref": "README.md:5-6 ~17.7M path-samples/s on 32 CPU cores"})
         out = {
             "metric": "path-samples/s", "value": value, "unit": "path-samples/s", "n_gpus": world,
@@ -699,7 +700,7 @@ def run_serve(args, world, rank, device):
     from argent_b200.gpu import Context, Piece, Scene, Serve
 
     torch.cuda.set_device(device)
-    ctx = Context(device)
+    ctx = Context(device, wave_paths=args.wave_paths or SERVE_WAVE_PATHS, lanes=args.lanes)
     meshes = W.serve_pieces()
     pieces = [Piece(ctx, m) for m in meshes]
     cams, scenes = {}, {}
@@ -899,8 +900,13 @@ def serve_plain(ctx, trace, scenes, cams, ps):
     return served / (t_last - t0), lat
 
 
+PATH_STATE_BYTES = 244  # per path slot per lane
+STILL_WAVE_PATHS = 1 << 25  # the stills' and batch's context: 2^25-path waves (8 lanes hold 65 GB of path state)
+SERVE_WAVE_PATHS = 1 << 23  # the serve context: 2^23-path waves
+
+
 def ctx_wave_mb(args):
-    return 224 * (args.wave_paths or 2 ** 23) // 10 ** 6
+    return PATH_STATE_BYTES * (args.wave_paths or STILL_WAVE_PATHS) // 10 ** 6
 
 
 def main():
@@ -917,7 +923,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="serve_trace: skip the one-job-at-a-time comparison")
     ap.add_argument("--spp", type=int, default=0, help="override spp (short profiling runs)")
     ap.add_argument("--lanes", type=int, default=0, help="concurrent waves (0 = the library default)")
-    ap.add_argument("--wave-paths", type=int, default=0, help="path slots per wave (0 = the library default)")
+    ap.add_argument("--wave-paths", type=int, default=0,
+                    help="path slots per wave (0 = 2^25 for stills and batches, 2^23 for the serve trace)")
     ap.add_argument("--serve-rate", type=float, default=4.0, help="serve_trace: requests per second")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serve_trace: trace length")
     ap.add_argument("--serve-step", type=int, default=1 << 26, help="serve_trace: least path-samples per step")

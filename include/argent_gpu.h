@@ -197,11 +197,11 @@ typedef struct ArgentHit {
   uint32_t prim;
 } ArgentHit;
 
-/* Context limits; zero fields take defaults.  Path state is 224 bytes per
+/* Context limits; zero fields take defaults.  Path state is 244 bytes per
  * slot per lane and grows on demand to what a render needs, so the defaults
- * (8 lanes of 2^23 slots) hold about 15 GB once a large frame has run. */
+ * (8 lanes of 2^24 slots) hold about 33 GB once a large frame has run. */
 typedef struct ArgentLimits {
-  uint64_t wave_paths;      /* path slots per wavefront wave (default 2^23, at most 2^30) */
+  uint64_t wave_paths;      /* path slots per wavefront wave (default 2^24, at most 2^30) */
   uint64_t memory_budget;   /* bytes the serve loop may hold (default 3/4 of free) */
   uint32_t lanes;           /* concurrent waves, each with its own stream and path state (default 8, at most 16) */
   uint32_t reserved;
@@ -366,7 +366,7 @@ typedef struct ArgentTuneResult {
 
 /*
  * Times `count` samples of the given frame (after one warm-up pass) for each
- * lane count in {2, 4, 8, 12, 16} and wave size in {2^21 .. 2^24} whose path
+ * lane count in {2, 4, 8, 12, 16} and wave size in {2^21 .. 2^25} whose path
  * state fits in half of the free device memory, keeps the fastest as the
  * context's configuration, and frees the path state of unused lanes.
  * results (may be NULL when max_results is 0) receives up to max_results
