@@ -206,7 +206,7 @@ int argent_serve_create(ArgentCtx* ctx, const ArgentServeConfig* cfg, ArgentServ
   if (s->cfg.film_budget == 0) s->cfg.film_budget = 8ull << 30;
   if (s->cfg.max_active == 0) s->cfg.max_active = 64;
   if (s->cfg.step_path_samples == 0) s->cfg.step_path_samples = 1ull << 26;
-  if (s->cfg.aging_ms == 0) s->cfg.aging_ms = 1000;
+  if (s->cfg.aging_ms == 0) s->cfg.aging_ms = 250;
   if (s->cfg.step_path_samples_max == 0) s->cfg.step_path_samples_max = 2 * s->cfg.step_path_samples;
   s->cfg.step_path_samples_max = std::max(s->cfg.step_path_samples_max, s->cfg.step_path_samples);
   s->t0 = std::chrono::steady_clock::now();

@@ -789,7 +789,7 @@ def run_serve(args, world, rank, device):
         pv, plat = serve_plain(ctx, trace, scenes, cams, ps)
         plain = {"value": pv, "unit": "path-samples/s",
                  "latency_s": {c: {"n": len(v), "p50": pct(v, 50), "p99": pct(v, 99), "max": max(v) if v else None}
-                               for c, v in plat.items()},
+                               for c, v in list(plat.items()) + [("all", sum(plat.values(), []))]},
                  "discipline": "one job at a time in arrival order, render_pass in chunks of 2..64 spp sized to "
                                "about 1.5 s (serve/queue.rs:599-617), film read to host"}
 
@@ -825,12 +825,12 @@ def run_serve(args, world, rank, device):
                        "pieces_triangles": [int(m.num_tris) for m in meshes], "alloys": list(W.SERVE_ALLOYS),
                        "offered_path_samples_per_s": offered, "step_path_samples": args.serve_step,
                        "step_path_samples_max": args.serve_step_max or 2 * args.serve_step,
-                       "aging_ms": args.serve_aging_ms or 1000, "overlap": not args.serve_no_overlap,
+                       "aging_ms": args.serve_aging_ms or 250, "overlap": not args.serve_no_overlap,
                        "parallelism": f"replicas{world}",
                        "timing": "wall clock of the serve loop (latency is a wall-clock quantity); each step "
                                  "synchronises its batch"},
             "latency_s": {c: {"n": len(v), "p50": pct(v, 50), "p99": pct(v, 99), "max": max(v) if v else None}
-                          for c, v in lat.items()},
+                          for c, v in list(lat.items()) + [("all", sum(lat.values(), []))]},
             "clocks": ck,
             "e2e": {"value": value, "unit": "path-samples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": d2h / max(1, len(finished)), "note": "per request: films read to host"},

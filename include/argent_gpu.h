@@ -514,7 +514,7 @@ typedef struct ArgentServe ArgentServe;
 typedef struct ArgentServeConfig {
   uint64_t film_budget;       /* device bytes for films in use and pooled; 0 = 8 GiB */
   uint32_t max_active;        /* requests rendered together; 0 = 64 */
-  uint32_t aging_ms;          /* waiting this long raises a request one priority level; 0 = 1000 */
+  uint32_t aging_ms;          /* waiting this long raises a request one priority level; 0 = 250 */
   uint64_t step_path_samples; /* least path-samples per step; 0 = 2^26 (about 45 ms of rendering) */
   uint64_t step_path_samples_max; /* a step takes a quarter of the pending work, up to this;
                                      0 = 2 x step_path_samples */
