@@ -1088,6 +1088,16 @@ static void fill_args(dev::WaveArgs& a, const WaveBuffers& wb) {
   a.cap = (uint32_t)wb.cap;
 }
 
+// One shading launch of class CLS; `map` tells whether any scene of the wave
+// has an env map.
+template <int CLS>
+static void launch_shade(bool map, int grid, cudaStream_t st, const dev::WaveArgs& a, int depth) {
+  if (map)
+    dev::k_shade<CLS, true><<<grid, 128, 0, st>>>(a, depth);
+  else
+    dev::k_shade<CLS, false><<<grid, 128, 0, st>>>(a, depth);
+}
+
 // Renders every job's samples, wave by wave.  Wave i runs on lane i % 2
 // (its own stream and path state); the film kernels of successive waves are
 // chained by events, so films accumulate in wave order exactly as on one
@@ -1152,23 +1162,27 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   int g_ray = grid_for(ctx, (const void*)dev::k_raygen, 256, cap);
   int g_int[2] = {grid_for(ctx, (const void*)dev::k_intersect<false>, 128, cap),
                    grid_for(ctx, (const void*)dev::k_intersect<true>, 128, cap)};
-  int g_sh = grid_for(ctx, (const void*)dev::k_shade<CLS_METAL>, 128, cap);
+  int g_sh = grid_for(ctx, (const void*)dev::k_shade<CLS_METAL, true>, 128, cap);
   int g_any[2] = {grid_for(ctx, (const void*)dev::k_shadow<false>, 128, cap),
                   grid_for(ctx, (const void*)dev::k_shadow<true>, 128, cap)};
   int g_film = grid_for(ctx, (const void*)dev::k_film, 256, cap);
-  // Per wave: its classes and, for a one-scene wave, that scene.
-  std::vector<uint32_t> wclasses(waves.size());
+  // Per wave: its classes, whether any of its scenes has an env map (the
+  // shading kernels without one leave the map code out) and, for a one-scene
+  // wave, that scene.
+  std::vector<uint32_t> wclasses(waves.size()), wmap(waves.size());
   std::vector<const ArgentScene*> wone(waves.size());
   for (size_t wi = 0; wi < waves.size(); ++wi) {
     const dev::WaveDesc& w = waves[wi];
-    uint32_t classes = 1u << CLS_TERMINAL;
+    uint32_t classes = 1u << CLS_TERMINAL, map = 0;
     const ArgentScene* one = job_scenes[w.seg[0].job];
     for (uint32_t sgi = 0; sgi < w.num_segments; ++sgi) {
       const ArgentScene* sc = job_scenes[w.seg[sgi].job];
       classes |= sc->host.class_mask;
+      if (sc->host.env_is_map) map = 1;
       if (sc != one) one = nullptr;
     }
     wclasses[wi] = classes;
+    wmap[wi] = map;
     wone[wi] = one;
   }
   // The first film pass waits for the last one before this batch unless the
@@ -1191,6 +1205,7 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
       dev::WaveArgs& a = args[lane];
       const WaveBuffers& wb = ctx->wave[lane];
       const uint32_t classes = wclasses[wi];
+      const bool map = wmap[wi] != 0;
       const ArgentScene* one = wone[wi];
       const int uni = one ? 1 : 0;
       a.uscene = one ? one->d_scene : nullptr;
@@ -1217,11 +1232,11 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
         }
         {
           ProfScope ps(ctx, KC_SHADE, st);
-          if (classes & (1u << CLS_TERMINAL)) dev::k_shade<CLS_TERMINAL><<<g_sh, 128, 0, st>>>(a, (int)depth);
-          if (classes & (1u << CLS_METAL)) dev::k_shade<CLS_METAL><<<g_sh, 128, 0, st>>>(a, (int)depth);
-          if (classes & (1u << CLS_COATED)) dev::k_shade<CLS_COATED><<<g_sh, 128, 0, st>>>(a, (int)depth);
-          if (classes & (1u << CLS_DIELECTRIC)) dev::k_shade<CLS_DIELECTRIC><<<g_sh, 128, 0, st>>>(a, (int)depth);
-          if (classes & (1u << CLS_OTHER)) dev::k_shade<CLS_OTHER><<<g_sh, 128, 0, st>>>(a, (int)depth);
+          if (classes & (1u << CLS_TERMINAL)) launch_shade<CLS_TERMINAL>(map, g_sh, st, a, (int)depth);
+          if (classes & (1u << CLS_METAL)) launch_shade<CLS_METAL>(map, g_sh, st, a, (int)depth);
+          if (classes & (1u << CLS_COATED)) launch_shade<CLS_COATED>(map, g_sh, st, a, (int)depth);
+          if (classes & (1u << CLS_DIELECTRIC)) launch_shade<CLS_DIELECTRIC>(map, g_sh, st, a, (int)depth);
+          if (classes & (1u << CLS_OTHER)) launch_shade<CLS_OTHER>(map, g_sh, st, a, (int)depth);
           *kernels += __builtin_popcount(classes);
         }
         {
@@ -1280,6 +1295,7 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
       put(w.seg, w.num_segments * sizeof(dev::DevSegment));
       put(&depths[wi], sizeof(uint32_t));
       put(&wclasses[wi], sizeof(uint32_t));
+      put(&wmap[wi], sizeof(uint32_t));
       const ArgentScene* one = wone[wi];
       const void* sp = one ? (const void*)one->d_scene : nullptr;
       put(&sp, sizeof(sp));

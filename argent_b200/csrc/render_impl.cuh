@@ -193,9 +193,10 @@ __device__ V3 envmap_sample(const DevScene* sc, float u1, float u2, float* pdf_o
   *pdf_out = envmap_pdf(sc, d);
   return d;
 }
-// light.rs:111-127
+// light.rs:111-127.  MAP false: the caller's scenes have no env map.
+template <bool MAP>
 __device__ Spec env_eval(const DevScene* sc, V3 dir, const Wavelengths& wl) {
-  if (sc->env_is_map) return envmap_eval(sc, dir, wl);
+  if (MAP && sc->env_is_map) return envmap_eval(sc, dir, wl);
   float y = rclamp(dir.y, -1.0f, 1.0f);
   if (y >= 0.0f) {
     float t = powf(y, sc->env_power);
@@ -506,8 +507,9 @@ struct ShadeOut {
 
 // integrator.rs:59-218, one bounce of one path whose hit belongs to class
 // CLS: CLS_TERMINAL takes misses and panel hits, the other classes take
-// surface hits (piece or floor) of their materials.
-template <int CLS>
+// surface hits (piece or floor) of their materials.  MAP false compiles the
+// env-map code out, for waves whose scenes have none.
+template <int CLS, bool MAP>
 __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot, int depth) {
   constexpr unsigned KM = ClassKinds<CLS>::value;
   ShadeOut out;
@@ -546,7 +548,7 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
     for (int i = 0; i < 4; ++i) e.v[i] = expf(-sig.v[i] * t);
     beta = beta * e;
   }
-  bool env_map = sc->env_is_map != 0;
+  const bool env_map = MAP && sc->env_is_map != 0;
   V3 p, p_obj, ng, ns;
   uint32_t mat_id = 0;
   float cavity = 0.0f;
@@ -557,7 +559,7 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
       float pl = sc->env_pick * envmap_pdf(sc, rd);
       w = prev_pdf * prev_pdf / (prev_pdf * prev_pdf + pl * pl);
     }
-    add_clamped(&L, beta * env_eval(sc, rd, wl) * w, clamp, cl);
+    add_clamped(&L, beta * env_eval<MAP>(sc, rd, wl) * w, clamp, cl);
     done = true;
   } else if (CLS == CLS_TERMINAL) {  // panel (light.rs:67-72, integrator.rs:84-98)
     int idx = (int)(kind & 0x0FFFFFFFu);
@@ -583,7 +585,7 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
         w = prev_pdf * prev_pdf / (prev_pdf * prev_pdf + pl * pl);
       }
       if constexpr (CLS != CLS_TERMINAL) L = spec4(a.L[slot]);
-      add_clamped(&L, beta * env_eval(sc, rd, wl) * w, clamp, cl);
+      add_clamped(&L, beta * env_eval<MAP>(sc, rd, wl) * w, clamp, cl);
       if constexpr (CLS != CLS_TERMINAL) a.L[slot] = to_f4(L);
       done = true;
     } else {
@@ -663,49 +665,23 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
       float ul = s.next();
       float u1 = s.next();
       float u2 = s.next();
-      if (env_map && ul < sc->env_pick) {
+      // The light sample: the env map (with probability env_pick when the
+      // scene has one) or a panel by the power CDF.  From the BSDF value on,
+      // both take one code path (MIS weight, the panel and floor visibility
+      // tests, the shadow ray), so a warp whose paths chose different lights
+      // evaluates the BSDF once.  The arithmetic of each case is unchanged:
+      // a panel sample's visibility factor is exactly 1.
+      const bool use_env = env_map && ul < sc->env_pick;
+      bool valid = false;
+      V3 dir{0.0f, 0.0f, 0.0f};  // toward the sample, from p
+      V3 lp{0.0f, 0.0f, 0.0f};   // the point on the sampled panel
+      float p_light = 0.0f;
+      int li = -1;  // the sampled panel, left out of the visibility test
+      if (use_env) {
         float pdf_dir;
-        V3 dir = envmap_sample(sc, u1, u2, &pdf_dir);
-        if (pdf_dir > 0.0f && dot(dir, ngu) > 0.0f) {
-          V3 wi = to_local(frame, dir);
-          Spec f;
-          float p_bsdf;
-          bsdf_eval_pdf<KM>(bsdf, wo, wi, &f, &p_bsdf);
-          if (!is_black(f)) {
-            float p_light = sc->env_pick * pdf_dir;
-            float w = p_light * p_light / (p_light * p_light + p_bsdf * p_bsdf);
-            // sky_visibility (scene.rs:123-140): panels and floor here, the
-            // piece in k_shadow.
-            V3 from = offset_origin(p, ngu, dir);
-            float vis = 1.0f;
-            for (int q = 0; q < sc->num_panels && vis > 0.0f; ++q) {
-              float tt;
-              if (panel_intersect(sc->panels[q], from, dir, INFINITY, &tt)) vis = 0.0f;
-            }
-            if (vis > 0.0f && sc->floor_enabled) {
-              float tt;
-              if (floor_intersect(sc, from, dir, INFINITY, &tt)) vis = 1.0f - floor_presence(sc, from + dir * tt);
-            }
-            if (vis > 0.0f) {
-              Spec le = envmap_eval(sc, dir, wl);
-              Spec c = beta * f * le * (fabsf(wi.z) * w * vis / p_light);
-              c = clamped(c, rough_seen, cl);
-              V3 oo = from, od = dir;
-              if (sc->has_turn) {
-                oo = rot_y_sc(from, sc->to_obj_s, sc->to_obj_c);
-                od = rot_y_sc(dir, sc->to_obj_s, sc->to_obj_c);
-              }
-              if (piece_may_occlude(sc->piece, oo, od, INFINITY)) {
-                out.shadow = true;
-                out.sh_o = make_float4(oo.x, oo.y, oo.z, INFINITY);
-                out.sh_d = make_float4(od.x, od.y, od.z, __uint_as_float(slot));
-                out.sh_c = to_f4(c);
-              } else {
-                add_unoccluded<CLS>(a, slot, &L, c);
-              }
-            }
-          }
-        }
+        dir = envmap_sample(sc, u1, u2, &pdf_dir);
+        valid = pdf_dir > 0.0f && dot(dir, ngu) > 0.0f;
+        p_light = sc->env_pick * pdf_dir;
       } else if (sc->num_lights > 0) {
         // scene.rs:149-156
         float u = sc->env_pick > 0.0f ? (ul - sc->env_pick) / (1.0f - sc->env_pick) : ul;
@@ -722,54 +698,62 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
           k = min(lo, sc->num_lights - 1);
         }
         float pick = sc->light_cdf[k] - (k == 0 ? 0.0f : sc->light_cdf[k - 1]);
-        int li = sc->lights[k];
+        li = sc->lights[k];
         pick = pick * (1.0f - sc->env_pick);
         const DevPanel& pn = sc->panels[li];
-        V3 lp = ld3(pn.c) + ld3(pn.hu) * (2.0f * u1 - 1.0f) + ld3(pn.hv) * (2.0f * u2 - 1.0f);
+        lp = ld3(pn.c) + ld3(pn.hu) * (2.0f * u1 - 1.0f) + ld3(pn.hv) * (2.0f * u2 - 1.0f);
         V3 to = lp - p;
         float d2 = length_squared(to);
-        V3 dir = to / sqrtf(d2);
+        dir = to / sqrtf(d2);
         float cos_l = dot(-dir, ld3(pn.n));
-        if (cos_l > 0.0f && dot(dir, ngu) > 0.0f) {
-          V3 wi = to_local(frame, dir);
-          Spec f;
-          float p_bsdf;
-          bsdf_eval_pdf<KM>(bsdf, wo, wi, &f, &p_bsdf);
-          if (!is_black(f)) {
-            float p_light = pick * d2 / (cos_l * pn.area);
-            float w = p_light * p_light / (p_light * p_light + p_bsdf * p_bsdf);
-            V3 origin = offset_origin(p, ngu, dir);
-            // visible (scene.rs:222-243): panels and floor here.
+        valid = cos_l > 0.0f && dot(dir, ngu) > 0.0f;
+        p_light = pick * d2 / (cos_l * pn.area);
+      }
+      if (valid) {
+        V3 wi = to_local(frame, dir);
+        Spec f;
+        float p_bsdf;
+        bsdf_eval_pdf<KM>(bsdf, wo, wi, &f, &p_bsdf);
+        if (!is_black(f)) {
+          float w = p_light * p_light / (p_light * p_light + p_bsdf * p_bsdf);
+          // sky_visibility (scene.rs:123-140) for the map, visible
+          // (scene.rs:222-243) for a panel: panels and floor here, the piece
+          // in k_shadow.
+          V3 origin = offset_origin(p, ngu, dir);
+          V3 sdir = dir;
+          float t_max = INFINITY;
+          if (!use_env) {
             V3 dd = lp - origin;
             float dist = length(dd);
-            V3 sdir = dd / dist;
-            float t_max = dist * (1.0f - 1e-4f);
-            bool vis = true;
-            for (int q = 0; q < sc->num_panels && vis; ++q) {
-              float tt;
-              if (q != li && panel_intersect(sc->panels[q], origin, sdir, t_max, &tt)) vis = false;
+            sdir = dd / dist;
+            t_max = dist * (1.0f - 1e-4f);
+          }
+          float vis = 1.0f;
+          for (int q = 0; q < sc->num_panels && vis > 0.0f; ++q) {
+            float tt;
+            if (q != li && panel_intersect(sc->panels[q], origin, sdir, t_max, &tt)) vis = 0.0f;
+          }
+          if (vis > 0.0f && sc->floor_enabled) {
+            float tt;
+            if (floor_intersect(sc, origin, sdir, t_max, &tt))
+              vis = use_env ? 1.0f - floor_presence(sc, origin + sdir * tt) : 0.0f;
+          }
+          if (vis > 0.0f) {
+            Spec le = use_env ? envmap_eval(sc, dir, wl) : panel_le(sc->panels[li], lp, dir, wl);
+            Spec c = beta * f * le * (fabsf(wi.z) * w * vis / p_light);
+            c = clamped(c, rough_seen, cl);
+            V3 oo = origin, od = sdir;
+            if (sc->has_turn) {
+              oo = rot_y_sc(origin, sc->to_obj_s, sc->to_obj_c);
+              od = rot_y_sc(sdir, sc->to_obj_s, sc->to_obj_c);
             }
-            if (vis && sc->floor_enabled) {
-              float tt;
-              if (floor_intersect(sc, origin, sdir, t_max, &tt)) vis = false;
-            }
-            if (vis) {
-              Spec le = panel_le(pn, lp, dir, wl);
-              Spec c = beta * f * le * (fabsf(wi.z) * w / p_light);
-              c = clamped(c, rough_seen, cl);
-              V3 oo = origin, od = sdir;
-              if (sc->has_turn) {
-                oo = rot_y_sc(origin, sc->to_obj_s, sc->to_obj_c);
-                od = rot_y_sc(sdir, sc->to_obj_s, sc->to_obj_c);
-              }
-              if (piece_may_occlude(sc->piece, oo, od, t_max)) {
-                out.shadow = true;
-                out.sh_o = make_float4(oo.x, oo.y, oo.z, t_max);
-                out.sh_d = make_float4(od.x, od.y, od.z, __uint_as_float(slot));
-                out.sh_c = to_f4(c);
-              } else {
-                add_unoccluded<CLS>(a, slot, &L, c);
-              }
+            if (piece_may_occlude(sc->piece, oo, od, t_max)) {
+              out.shadow = true;
+              out.sh_o = make_float4(oo.x, oo.y, oo.z, t_max);
+              out.sh_d = make_float4(od.x, od.y, od.z, __uint_as_float(slot));
+              out.sh_c = to_f4(c);
+            } else {
+              add_unoccluded<CLS>(a, slot, &L, c);
             }
           }
         }
@@ -840,7 +824,7 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
 #ifndef ARGENT_SHADE_BLOCKS_DIELECTRIC
 #define ARGENT_SHADE_BLOCKS_DIELECTRIC 5
 #endif
-template <int CLS>
+template <int CLS, bool MAP>
 __global__ void __launch_bounds__(128, CLS == CLS_TERMINAL      ? 1
                                        : CLS == CLS_DIELECTRIC ? ARGENT_SHADE_BLOCKS_DIELECTRIC
                                                                : ARGENT_SHADE_BLOCKS)
@@ -859,7 +843,7 @@ __global__ void __launch_bounds__(128, CLS == CLS_TERMINAL      ? 1
     uint32_t slot = 0;
     if (i < count) {
       slot = q[i];
-      r = shade_path<CLS>(a, slot, depth);
+      r = shade_path<CLS, MAP>(a, slot, depth);
     }
     warp_append(r.alive, slot, next_counter, a.q_out, cap, a.status);
     // Shadow rays: the record is written at the queue position.

@@ -322,3 +322,50 @@ def test_graph_replay_equals_direct_launches():
     g = Film(ctx, wl.width, wl.height)
     render_pass(ctx, scene, wl.camera, g, wl.settings, 8, wl.seed + 1)
     assert not np.array_equal(g.xyz(), want)
+
+
+@pytest.mark.gpu
+def test_graph_keys_keep_map_and_gradient_waves_apart():
+    """Waves whose scenes have no env map shade with kernels that leave the
+    map code out.  Two small renders share one wave (so the wave names no
+    single scene); a batch of two gradient-studio scenes and then a batch of
+    two env-map scenes of the same piece, materials, panels and sizes give
+    the same waves, and the second must not replay the first's graph: every
+    film equals its render with graphs off, bit for bit."""
+    from argent_b200.gpu import Context, Film, Piece, Scene, render_batch
+
+    m = W.reel_piece("61k")
+    env = W.hdri(256, 128)
+    radius, floor_y = W.piece_radius(m)
+    cam, _ = W.turntable_camera(W.hull(m), aspect=1.0)
+    ps = W.settings(8)
+
+    def descs(with_map):
+        out = []
+        for alloy in ("sterling", "bronze"):
+            if with_map:
+                out.append(W.reel_scene(m, alloy, env, 30.0))
+                continue
+            panels, grad, fm, fl, white = W.studio("noir", radius, floor_y)
+            mats = [W.metal(alloy, 0.05, 0.8), W.metal(alloy, 0.35, 0.8), fm]
+            fl.material = len(mats) - 1
+            out.append(W.SceneDesc(mats, panels, grad, fl, 30.0, white))
+        return out
+
+    ctx = Context(0)
+    piece = Piece(ctx, m)
+    batches = [[Scene(ctx, piece, d) for d in descs(with_map)] for with_map in (False, True)]
+
+    def render(scenes):
+        films = [Film(ctx, 64, 64) for _ in scenes]
+        render_batch(ctx, [(sc, cam, f, ps, 4, 7) for sc, f in zip(scenes, films)])
+        return [f.xyz() for f in films]
+
+    ctx.set_graphs(False)
+    want = [render(b) for b in batches]
+    ctx.set_graphs(True)
+    for _ in range(2):
+        for b, w in zip(batches, want):
+            for got, ref in zip(render(b), w):
+                assert np.array_equal(got, ref)
+    assert not np.array_equal(want[0][0], want[1][0])
