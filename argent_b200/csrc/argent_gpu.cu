@@ -1088,14 +1088,22 @@ static void fill_args(dev::WaveArgs& a, const WaveBuffers& wb) {
   a.cap = (uint32_t)wb.cap;
 }
 
+// Persistent grids of class CLS's two shading kernels (without and with the
+// env-map code) for queues of up to `cap` paths.
+template <int CLS>
+static void shade_grids(const ArgentCtx* ctx, uint64_t cap, int grid[2]) {
+  grid[0] = grid_for(ctx, (const void*)dev::k_shade<CLS, false>, 128, cap);
+  grid[1] = grid_for(ctx, (const void*)dev::k_shade<CLS, true>, 128, cap);
+}
+
 // One shading launch of class CLS; `map` tells whether any scene of the wave
 // has an env map.
 template <int CLS>
-static void launch_shade(bool map, int grid, cudaStream_t st, const dev::WaveArgs& a, int depth) {
+static void launch_shade(bool map, const int grid[2], cudaStream_t st, const dev::WaveArgs& a, int depth) {
   if (map)
-    dev::k_shade<CLS, true><<<grid, 128, 0, st>>>(a, depth);
+    dev::k_shade<CLS, true><<<grid[1], 128, 0, st>>>(a, depth);
   else
-    dev::k_shade<CLS, false><<<grid, 128, 0, st>>>(a, depth);
+    dev::k_shade<CLS, false><<<grid[0], 128, 0, st>>>(a, depth);
 }
 
 // Renders every job's samples, wave by wave.  Wave i runs on lane i % 2
@@ -1162,7 +1170,15 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   int g_ray = grid_for(ctx, (const void*)dev::k_raygen, 256, cap);
   int g_int[2] = {grid_for(ctx, (const void*)dev::k_intersect<false>, 128, cap),
                    grid_for(ctx, (const void*)dev::k_intersect<true>, 128, cap)};
-  int g_sh = grid_for(ctx, (const void*)dev::k_shade<CLS_METAL, true>, 128, cap);
+  // Shading grids: the metal class's for every class but the coated one,
+  // which has its own (more blocks per SM).
+  int g_sh[NUM_CLS][2];
+  shade_grids<CLS_METAL>(ctx, cap, g_sh[CLS_METAL]);
+  for (int c = 0; c < NUM_CLS; ++c) {
+    g_sh[c][0] = g_sh[CLS_METAL][0];
+    g_sh[c][1] = g_sh[CLS_METAL][1];
+  }
+  shade_grids<CLS_COATED>(ctx, cap, g_sh[CLS_COATED]);
   int g_any[2] = {grid_for(ctx, (const void*)dev::k_shadow<false>, 128, cap),
                   grid_for(ctx, (const void*)dev::k_shadow<true>, 128, cap)};
   int g_film = grid_for(ctx, (const void*)dev::k_film, 256, cap);
@@ -1232,11 +1248,11 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
         }
         {
           ProfScope ps(ctx, KC_SHADE, st);
-          if (classes & (1u << CLS_TERMINAL)) launch_shade<CLS_TERMINAL>(map, g_sh, st, a, (int)depth);
-          if (classes & (1u << CLS_METAL)) launch_shade<CLS_METAL>(map, g_sh, st, a, (int)depth);
-          if (classes & (1u << CLS_COATED)) launch_shade<CLS_COATED>(map, g_sh, st, a, (int)depth);
-          if (classes & (1u << CLS_DIELECTRIC)) launch_shade<CLS_DIELECTRIC>(map, g_sh, st, a, (int)depth);
-          if (classes & (1u << CLS_OTHER)) launch_shade<CLS_OTHER>(map, g_sh, st, a, (int)depth);
+          if (classes & (1u << CLS_TERMINAL)) launch_shade<CLS_TERMINAL>(map, g_sh[CLS_TERMINAL], st, a, (int)depth);
+          if (classes & (1u << CLS_METAL)) launch_shade<CLS_METAL>(map, g_sh[CLS_METAL], st, a, (int)depth);
+          if (classes & (1u << CLS_COATED)) launch_shade<CLS_COATED>(map, g_sh[CLS_COATED], st, a, (int)depth);
+          if (classes & (1u << CLS_DIELECTRIC)) launch_shade<CLS_DIELECTRIC>(map, g_sh[CLS_DIELECTRIC], st, a, (int)depth);
+          if (classes & (1u << CLS_OTHER)) launch_shade<CLS_OTHER>(map, g_sh[CLS_OTHER], st, a, (int)depth);
           *kernels += __builtin_popcount(classes);
         }
         {

@@ -814,19 +814,28 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
   return out;
 }
 
-// Surface shading is capped at 128 registers (4 blocks of 128 per SM)
-// instead of up to ~166, trading a little spilling for residency; lower
-// caps spill the metal and coated classes heavily and run slower.
+// Register budgets of the shading classes.  Metal and the other surface
+// classes are capped at 128 registers (4 blocks of 128 per SM) instead of up
+// to ~166; lower caps spill them heavily and run slower.  The coated class
+// (the studio floor, the largest shading launch) runs at 96 registers, 5
+// blocks, with about 60 B of spill, on a grid of its own 5 blocks per SM.
+// The dielectric class fits 96 registers without spilling.  Every class but
+// the coated one launches on the metal class's grid (4 blocks per SM):
+// wider grids for the terminal (8) and dielectric (5) classes took SMs from
+// the other lanes' kernels and ran slower.
 #ifndef ARGENT_SHADE_BLOCKS
 #define ARGENT_SHADE_BLOCKS 4
 #endif
-// The dielectric class fits 96 registers without spilling: 5 blocks.
 #ifndef ARGENT_SHADE_BLOCKS_DIELECTRIC
 #define ARGENT_SHADE_BLOCKS_DIELECTRIC 5
+#endif
+#ifndef ARGENT_SHADE_BLOCKS_COATED
+#define ARGENT_SHADE_BLOCKS_COATED 5
 #endif
 template <int CLS, bool MAP>
 __global__ void __launch_bounds__(128, CLS == CLS_TERMINAL      ? 1
                                        : CLS == CLS_DIELECTRIC ? ARGENT_SHADE_BLOCKS_DIELECTRIC
+                                       : CLS == CLS_COATED     ? ARGENT_SHADE_BLOCKS_COATED
                                                                : ARGENT_SHADE_BLOCKS)
     k_shade(WaveArgs a, int depth) {
   uint32_t count = a.counters[CNT_CLS(depth, CLS)];
