@@ -1170,14 +1170,14 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   int g_ray = grid_for(ctx, (const void*)dev::k_raygen, 256, cap);
   int g_int[2] = {grid_for(ctx, (const void*)dev::k_intersect<false>, 128, cap),
                    grid_for(ctx, (const void*)dev::k_intersect<true>, 128, cap)};
-  // Shading grids: the metal class's for every class but the coated one,
-  // which has its own (more blocks per SM).
+  // Shading grids: ARGENT_SHADE_BLOCKS blocks per SM for the terminal,
+  // dielectric and other classes; the metal and coated classes size their
+  // own from their occupancy.
   int g_sh[NUM_CLS][2];
+  const int g_shared = (int)std::max<uint64_t>(
+      1, std::min<uint64_t>((cap + 127) / 128, (uint64_t)ctx->num_sms * ARGENT_SHADE_BLOCKS));
+  for (int c = 0; c < NUM_CLS; ++c) g_sh[c][0] = g_sh[c][1] = g_shared;
   shade_grids<CLS_METAL>(ctx, cap, g_sh[CLS_METAL]);
-  for (int c = 0; c < NUM_CLS; ++c) {
-    g_sh[c][0] = g_sh[CLS_METAL][0];
-    g_sh[c][1] = g_sh[CLS_METAL][1];
-  }
   shade_grids<CLS_COATED>(ctx, cap, g_sh[CLS_COATED]);
   int g_any[2] = {grid_for(ctx, (const void*)dev::k_shadow<false>, 128, cap),
                   grid_for(ctx, (const void*)dev::k_shadow<true>, 128, cap)};

@@ -819,8 +819,9 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
 // to ~166; lower caps spill them heavily and run slower.  The coated class
 // (the studio floor, the largest shading launch) runs at 96 registers, 5
 // blocks, with about 60 B of spill, on a grid of its own 5 blocks per SM.
-// The dielectric class fits 96 registers without spilling.  Every class but
-// the coated one launches on the metal class's grid (4 blocks per SM):
+// The dielectric class fits 96 registers without spilling.  The terminal,
+// dielectric and other classes launch on a grid of ARGENT_SHADE_BLOCKS (4)
+// blocks per SM, metal and coated on grids of their own occupancy:
 // wider grids for the terminal (8) and dielectric (5) classes took SMs from
 // the other lanes' kernels and ran slower.
 #ifndef ARGENT_SHADE_BLOCKS
@@ -832,10 +833,14 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
 #ifndef ARGENT_SHADE_BLOCKS_COATED
 #define ARGENT_SHADE_BLOCKS_COATED 5
 #endif
+#ifndef ARGENT_SHADE_BLOCKS_METAL
+#define ARGENT_SHADE_BLOCKS_METAL ARGENT_SHADE_BLOCKS
+#endif
 template <int CLS, bool MAP>
 __global__ void __launch_bounds__(128, CLS == CLS_TERMINAL      ? 1
                                        : CLS == CLS_DIELECTRIC ? ARGENT_SHADE_BLOCKS_DIELECTRIC
                                        : CLS == CLS_COATED     ? ARGENT_SHADE_BLOCKS_COATED
+                                       : CLS == CLS_METAL      ? ARGENT_SHADE_BLOCKS_METAL
                                                                : ARGENT_SHADE_BLOCKS)
     k_shade(WaveArgs a, int depth) {
   uint32_t count = a.counters[CNT_CLS(depth, CLS)];
