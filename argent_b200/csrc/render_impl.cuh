@@ -136,12 +136,23 @@ __device__ __forceinline__ float lin_eval(const DevScene* sc, const float* w, fl
   }
   return fmaxf(v, 0.0f);
 }
-__device__ Spec envmap_eval(const DevScene* sc, V3 dir, const Wavelengths& wl) {
+// The texel a direction falls in, and its v; the map's eval and pdf of one
+// direction share it.
+struct EnvTexel {
+  uint32_t x, y;
+  float v;
+};
+__device__ __forceinline__ EnvTexel env_texel(const DevScene* sc, V3 dir) {
   float u, v;
   env_uv(sc, dir, &u, &v);
-  uint32_t x = min(sat_u32(u * (float)sc->map_w), (uint32_t)sc->map_w - 1u);
-  uint32_t y = min(sat_u32(v * (float)sc->map_h), (uint32_t)sc->map_h - 1u);
-  const float* wp = sc->map_weights + 3 * ((size_t)y * sc->map_w + x);
+  EnvTexel t;
+  t.x = min(sat_u32(u * (float)sc->map_w), (uint32_t)sc->map_w - 1u);
+  t.y = min(sat_u32(v * (float)sc->map_h), (uint32_t)sc->map_h - 1u);
+  t.v = v;
+  return t;
+}
+__device__ Spec envmap_eval_at(const DevScene* sc, EnvTexel t, const Wavelengths& wl) {
+  const float* wp = sc->map_weights + 3 * ((size_t)t.y * sc->map_w + t.x);
   float w[3] = {__ldg(wp), __ldg(wp + 1), __ldg(wp + 2)};
   Spec r;
 #pragma unroll
@@ -149,16 +160,12 @@ __device__ Spec envmap_eval(const DevScene* sc, V3 dir, const Wavelengths& wl) {
   return r;
 }
 // envmap.rs:375-387
-__device__ float envmap_pdf(const DevScene* sc, V3 dir) {
-  float u, v;
-  env_uv(sc, dir, &u, &v);
-  float st = sinf(ARGENT_PI_F * v);
+__device__ float envmap_pdf_at(const DevScene* sc, EnvTexel t) {
+  float st = sinf(ARGENT_PI_F * t.v);
   if (st <= 1e-6f) return 0.0f;
-  uint32_t x = min(sat_u32(u * (float)sc->map_w), (uint32_t)sc->map_w - 1u);
-  uint32_t y = min(sat_u32(v * (float)sc->map_h), (uint32_t)sc->map_h - 1u);
-  size_t row = (size_t)y * (sc->map_w + 1);
-  float pc = (__ldg(sc->map_cond + row + x + 1) - __ldg(sc->map_cond + row + x)) * (float)sc->map_w;
-  float pm = (__ldg(sc->map_marg + y + 1) - __ldg(sc->map_marg + y)) * (float)sc->map_h;
+  size_t row = (size_t)t.y * (sc->map_w + 1);
+  float pc = (__ldg(sc->map_cond + row + t.x + 1) - __ldg(sc->map_cond + row + t.x)) * (float)sc->map_w;
+  float pm = (__ldg(sc->map_marg + t.y + 1) - __ldg(sc->map_marg + t.y)) * (float)sc->map_h;
   return pc * pm / (2.0f * ARGENT_PI_F * ARGENT_PI_F * st);
 }
 __device__ __forceinline__ uint32_t partition_le(const float* a, uint32_t n, float u) {
@@ -173,7 +180,7 @@ __device__ __forceinline__ uint32_t partition_le(const float* a, uint32_t n, flo
   return lo;
 }
 // envmap.rs:390-402
-__device__ V3 envmap_sample(const DevScene* sc, float u1, float u2, float* pdf_out) {
+__device__ V3 envmap_sample(const DevScene* sc, float u1, float u2, float* pdf_out, EnvTexel* texel) {
   uint32_t w = (uint32_t)sc->map_w, h = (uint32_t)sc->map_h;
   uint32_t y = min(max(partition_le(sc->map_marg, h + 1, u1), 1u), h) - 1u;
   const float* cond = sc->map_cond + (size_t)y * (w + 1);
@@ -190,13 +197,14 @@ __device__ V3 envmap_sample(const DevScene* sc, float u1, float u2, float* pdf_o
   sincosf(theta, &st, &ct);
   sincosf(phi, &sp, &cp);
   V3 d = rot_y_sc(V3{st * sp, ct, -st * cp}, sc->map_to_world_s, sc->map_to_world_c);
-  *pdf_out = envmap_pdf(sc, d);
+  *texel = env_texel(sc, d);
+  *pdf_out = envmap_pdf_at(sc, *texel);
   return d;
 }
 // light.rs:111-127.  MAP false: the caller's scenes have no env map.
 template <bool MAP>
 __device__ Spec env_eval(const DevScene* sc, V3 dir, const Wavelengths& wl) {
-  if (MAP && sc->env_is_map) return envmap_eval(sc, dir, wl);
+  if (MAP && sc->env_is_map) return envmap_eval_at(sc, env_texel(sc, dir), wl);
   float y = rclamp(dir.y, -1.0f, 1.0f);
   if (y >= 0.0f) {
     float t = powf(y, sc->env_power);
@@ -555,11 +563,18 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
   bool done = false;
   if (CLS == CLS_TERMINAL && kind == HIT_MISS) {
     float w = 1.0f;
-    if (env_map && !specular) {
-      float pl = sc->env_pick * envmap_pdf(sc, rd);
-      w = prev_pdf * prev_pdf / (prev_pdf * prev_pdf + pl * pl);
+    Spec le;
+    if (env_map) {
+      EnvTexel et = env_texel(sc, rd);
+      if (!specular) {
+        float pl = sc->env_pick * envmap_pdf_at(sc, et);
+        w = prev_pdf * prev_pdf / (prev_pdf * prev_pdf + pl * pl);
+      }
+      le = envmap_eval_at(sc, et, wl);
+    } else {
+      le = env_eval<false>(sc, rd, wl);
     }
-    add_clamped(&L, beta * env_eval<MAP>(sc, rd, wl) * w, clamp, cl);
+    add_clamped(&L, beta * le * w, clamp, cl);
     done = true;
   } else if (CLS == CLS_TERMINAL) {  // panel (light.rs:67-72, integrator.rs:84-98)
     int idx = (int)(kind & 0x0FFFFFFFu);
@@ -580,12 +595,19 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
     V3 fp = ro + rd * t;
     if (s.next_random() >= floor_presence(sc, fp)) {
       float w = 1.0f;
-      if (env_map && !specular) {
-        float pl = sc->env_pick * envmap_pdf(sc, rd);
-        w = prev_pdf * prev_pdf / (prev_pdf * prev_pdf + pl * pl);
+      Spec le;
+      if (env_map) {
+        EnvTexel et = env_texel(sc, rd);
+        if (!specular) {
+          float pl = sc->env_pick * envmap_pdf_at(sc, et);
+          w = prev_pdf * prev_pdf / (prev_pdf * prev_pdf + pl * pl);
+        }
+        le = envmap_eval_at(sc, et, wl);
+      } else {
+        le = env_eval<false>(sc, rd, wl);
       }
       if constexpr (CLS != CLS_TERMINAL) L = spec4(a.L[slot]);
-      add_clamped(&L, beta * env_eval<MAP>(sc, rd, wl) * w, clamp, cl);
+      add_clamped(&L, beta * le * w, clamp, cl);
       if constexpr (CLS != CLS_TERMINAL) a.L[slot] = to_f4(L);
       done = true;
     } else {
@@ -675,11 +697,12 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
       bool valid = false;
       V3 dir{0.0f, 0.0f, 0.0f};  // toward the sample, from p
       V3 lp{0.0f, 0.0f, 0.0f};   // the point on the sampled panel
+      EnvTexel etx{0u, 0u, 0.0f};  // the map texel of a map sample
       float p_light = 0.0f;
       int li = -1;  // the sampled panel, left out of the visibility test
       if (use_env) {
         float pdf_dir;
-        dir = envmap_sample(sc, u1, u2, &pdf_dir);
+        dir = envmap_sample(sc, u1, u2, &pdf_dir, &etx);
         valid = pdf_dir > 0.0f && dot(dir, ngu) > 0.0f;
         p_light = sc->env_pick * pdf_dir;
       } else if (sc->num_lights > 0) {
@@ -739,7 +762,7 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
               vis = use_env ? 1.0f - floor_presence(sc, origin + sdir * tt) : 0.0f;
           }
           if (vis > 0.0f) {
-            Spec le = use_env ? envmap_eval(sc, dir, wl) : panel_le(sc->panels[li], lp, dir, wl);
+            Spec le = use_env ? envmap_eval_at(sc, etx, wl) : panel_le(sc->panels[li], lp, dir, wl);
             Spec c = beta * f * le * (fabsf(wi.z) * w * vis / p_light);
             c = clamped(c, rough_seen, cl);
             V3 oo = origin, od = sdir;
