@@ -1,0 +1,31 @@
+"""bench.py's reference arm (`--impl reference`) on the host cores: one JSON
+line with the bench contract's keys, argent's algorithm (the oracle) timed on
+a bounded band of the workload's frame, and no host/device traffic."""
+
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_prints_one_contract_line():
+    cmd = [sys.executable, "bench.py", "--impl", "reference", "--workload", "ring_still", "--steps", "2",
+           "--warmup", "1", "--ref-seconds", "0.5"]
+    out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, out.stdout[-2000:]
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    assert d["metric"] == "path-samples/s" and d["unit"] == "path-samples/s"
+    assert d["value"] > 0 and d["higher_is_better"] is True
+    assert d["steps"] == 2 and d["warmup"] == 1 and d["n_gpus"] == 1
+    assert d["config"]["workload"].startswith("ring_still")
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] == d["value"]
+    assert cb["sample"]
+    e = d["e2e"]
+    assert e["value"] == d["value"] and e["unit"] == d["unit"]
+    assert e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
