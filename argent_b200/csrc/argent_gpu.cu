@@ -1954,6 +1954,20 @@ int argent_ctx_config(const ArgentCtx* ctx, uint32_t* lanes, uint64_t* wave_path
   return ARGENT_OK;
 }
 
+int argent_ctx_set_config(ArgentCtx* ctx, uint32_t lanes, uint64_t wave_paths) {
+  if (!ctx) return set_error(nullptr, ARGENT_E_INVALID, "ctx is NULL");
+  if (lanes < 1 || lanes > ARGENT_LANES || wave_paths < (1ull << 16) || wave_paths > (1ull << 30))
+    return set_error(ctx, ARGENT_E_INVALID, "argent_ctx_set_config: lanes must be 1..16 and wave_paths 2^16..2^30");
+  // Work already queued keeps the lanes it was issued on; the next call
+  // starts its waves at lane 0 of the new rotation.
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->lanes = (int)lanes;
+  ctx->limits.wave_paths = wave_paths;
+  ctx->next_lane = 0;
+  return ARGENT_OK;
+}
+
 }  // extern "C"
 
 // argent_render_batch; with `done` the batch overlaps the next one (run_jobs).
@@ -2115,29 +2129,24 @@ int argent_ctx_traversal_counts(ArgentCtx* ctx, uint64_t* out6) {
 // Every GPU that loads the library holds the array until the process exits.
 
 #define ARGENT_NOALLOC_MAX_RAYS (1u << 18)
-#define ARGENT_NOALLOC_MAX_DEVICES 64
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[(size_t)ARGENT_NOALLOC_MAX_RAYS *
                                                                  (sizeof(ArgentRay) + sizeof(ArgentHit))];
 
-// Device address of g_noalloc_scratch per device, looked up once per device
-// with that device current (the name is only a host stand-in in host code).
-static void* g_noalloc_addr[ARGENT_NOALLOC_MAX_DEVICES];
-static std::mutex g_noalloc_mu;
-
+// Device address of g_noalloc_scratch (in host code the name is only a
+// host-side stand-in), looked up by a context's first call with its device
+// current and kept in the context.  A context made after a device reset
+// looks it up afresh, so it never uses an address of a context that is gone.
 static int noalloc_scratch(ArgentCtx* ctx, unsigned char** out) {
-  if (ctx->device < 0 || ctx->device >= ARGENT_NOALLOC_MAX_DEVICES)
-    return set_error(ctx, ARGENT_E_INVALID, "device index beyond the allocation-free table");
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[ctx->device]) {
+  if (!ctx->noalloc_addr) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
       return set_error(ctx, ARGENT_E_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") +
                                                cudaGetErrorString(e));
-    g_noalloc_addr[ctx->device] = p;
+    ctx->noalloc_addr = p;
   }
-  *out = (unsigned char*)g_noalloc_addr[ctx->device];
+  *out = (unsigned char*)ctx->noalloc_addr;
   return ARGENT_OK;
 }
 
@@ -2160,7 +2169,10 @@ extern "C" int argent_trace_closest_noalloc(ArgentCtx* ctx, ArgentPiece* piece, 
   ARGENT_CK(ctx, cudaMemcpyAsync(d_rays, rays, n * sizeof(ArgentRay), cudaMemcpyHostToDevice, ctx->stream));
   int block = 128;
   int grid = grid_for(ctx, (const void*)k_trace_closest, block, n);
-  k_trace_closest<<<grid, block, 0, ctx->stream>>>(piece->dev, d_rays, n, d_hits, ctx->d_status);
+  {
+    ProfScope ps(ctx, KC_TRACE);
+    k_trace_closest<<<grid, block, 0, ctx->stream>>>(piece->dev, d_rays, n, d_hits, ctx->d_status);
+  }
   ctx->launches++;
   ARGENT_CK(ctx, cudaGetLastError());
   ARGENT_CK(ctx, cudaMemcpyAsync(hits, d_hits, n * sizeof(ArgentHit), cudaMemcpyDeviceToHost, ctx->stream));

@@ -175,6 +175,9 @@ struct ArgentCtx {
   KernelProfile prof;
   float* resolve = nullptr;  // film-read staging (grown on demand)
   size_t resolve_floats = 0;
+  // Device address of the allocation-free entry point's static array,
+  // looked up by this context's first call of it.
+  void* noalloc_addr = nullptr;
 };
 
 struct ArgentPiece {

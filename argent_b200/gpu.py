@@ -75,6 +75,10 @@ class Context:
         self.check(self.lib.argent_ctx_config(self.h, ctypes.byref(lanes), ctypes.byref(wave)))
         return lanes.value, wave.value
 
+    def set_config(self, lanes, wave_paths):
+        """argent_ctx_set_config: lanes and wave size of the next calls."""
+        self.check(self.lib.argent_ctx_set_config(self.h, int(lanes), int(wave_paths)))
+
     def set_counting(self, on):
         self.check(self.lib.argent_ctx_set_counting(self.h, 1 if on else 0))
 

@@ -237,17 +237,46 @@ def signet_still(piece_gpu=None, spp=256, width=1920, height=1080, mesh=None):
 SIDE_GEMS = ("ruby", "sapphire", "emerald", "garnet")
 
 
-def gems_still(piece_gpu=None, spp=512, width=1080, height=1920, mesh=None, max_depth=32, center="diamond"):
+def gems_still(piece_gpu=None, spp=512, width=1080, height=1920, mesh=None, max_depth=32, center="diamond",
+               side=SIDE_GEMS):
     """The gems workload: 18k gold setting (about 0.9M triangles) with a
     diamond brilliant (argent's DIAMOND Sellmeier; `center="diamond_alt"`
     takes the workload's stated alternate fit, n_D about 2.261) and 36 side
     stones drawn from ruby / sapphire / emerald / garnet; white studio,
-    1080 x 1920, 512 spp, max depth 32, 100 mm pinhole, hero view."""
+    1080 x 1920, 512 spp, max depth 32, 100 mm pinhole, hero view.  `center`
+    and `side` (four names) swap the stones' materials, e.g. for opaque
+    stones (onyx, turquoise, lapis: a coat over a body colour)."""
     m = mesh if mesh is not None else M.gem_ring()
     cam, turn = shot(piece_gpu, hull(m), "hero", 100.0, 0.0, width / height)
-    mats = [metal("gold18k", 0.07, 0.8), gem(center)] + [gem(g) for g in SIDE_GEMS]
+    mats = [metal("gold18k", 0.07, 0.8), gem(center)] + [gem(g) for g in side]
     desc = _studio_scene(m, mats, "white", turn)
     return Workload(f"gems_still_{width}x{height}_{spp}spp", m, desc, cam, width, height, spp, settings(max_depth), 7)
+
+
+def opal(black, cell_mm=0.35):
+    """Material::opal (material.rs:63-66): black or white opal."""
+    m = N.ArgentMaterial()
+    N.host().argent_material_opal(1 if black else 0, cell_mm, ctypes.byref(m))
+    return m
+
+
+def opal_still(black=False, spp=8, width=128, height=128, cell_mm=0.35):
+    """The ring piece carved from precious opal (Voronoi domains of Bragg
+    lattices over a milky or dark body, material.rs:98-113, 208-237),
+    noir studio, 100 mm pinhole, hero view, depth 8."""
+    m = M.ring()
+    cam, turn = shot(None, hull(m), "hero", 100.0, 0.0, width / height)
+    desc = _studio_scene(m, [opal(black, cell_mm)], "noir", turn)
+    kind = "black" if black else "white"
+    return Workload(f"opal_{kind}_{width}x{height}_{spp}spp", m, desc, cam, width, height, spp, settings(8), 7)
+
+
+def with_cavity(mesh, cavity):
+    """`mesh` carrying the per-vertex cavity mask `cavity`
+    (cavity::patina_mask), as Prepared::build attaches it to the piece
+    (shot.rs:142): metal slots with a patina then darken the recesses
+    (material.rs:115-122)."""
+    return M.Mesh(mesh.positions, mesh.tris, mesh.normals, mesh.tri_material, cavity)
 
 
 def sphere(r=10.0, n=64):

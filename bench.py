@@ -176,26 +176,47 @@ def cpu_model():
     return platform.processor() or "unknown"
 
 
+def spread_bands(height, rows, n=8):
+    """n bands of `rows` rows spread evenly down a frame: band k is centred
+    on row (2k + 1) h / 2n, so together they sample the frame's average
+    (sky, piece, floor) rather than its busiest middle."""
+    out = []
+    for k in range(n):
+        c = (2 * k + 1) * height // (2 * n)
+        y0 = max(0, min(height - rows, c - rows // 2))
+        out.append((y0, y0 + rows))
+    return out
+
+
+def describe_bands(bands):
+    return ", ".join(f"{a}..{b}" for a, b in bands)
+
+
 def cpu_sample(wl, seconds=12.0, threads=0, rows=None):
-    """argent's algorithm (the oracle) on a band of rows of the workload
-    frame at the workload's spp.  Returns (samples/s, rows, threads)."""
+    """argent's algorithm (the oracle) on 8 bands of rows spread down the
+    workload frame at the workload's spp.  Returns (samples/s, bands,
+    threads, scene)."""
     import oracle as O
 
     sc = O.Scene(wl.mesh, wl.desc.c)
     h = wl.height
-    mid = h // 2
+
+    def run(bands):
+        for y0, y1 in bands:
+            sc.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, wl.spp, wl.seed, rows=(y0, y1),
+                           threads=threads, want_xyz=False)
+
     if rows is None:
         t0 = time.perf_counter()
-        sc.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, wl.spp, wl.seed, rows=(mid, mid + 1),
-                       threads=threads, want_xyz=False)
+        run(spread_bands(h, 1))
         dt = time.perf_counter() - t0
-        rows = int(max(1, min(h - mid, seconds / max(dt, 1e-3))))
+        rows = int(max(1, min(h // 8, seconds / max(dt, 1e-3))))
+    bands = spread_bands(h, rows)
     t0 = time.perf_counter()
-    sc.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, wl.spp, wl.seed, rows=(mid, mid + rows),
-                   threads=threads, want_xyz=False)
+    run(bands)
     dt = time.perf_counter() - t0
     nthr = threads if threads > 0 else (os.cpu_count() or 1)
-    return wl.width * rows * wl.spp / dt, rows, nthr, sc
+    return wl.width * rows * len(bands) * wl.spp / dt, bands, nthr, sc
 
 
 WORKLOADS = ("signet_still", "ring_still", "gems_still", "reel_batch", "serve_trace")
@@ -280,28 +301,28 @@ def run_reference(args, world, rank):
         for wl, sc in zip(wls, scenes):
             if reel:
                 sc.set_turntable(W.reel_frame_turn(turn[wl.name], k % W.REEL_FRAMES))
-            mid = wl.height // 2
-            sc.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, wl.spp, wl.seed, rows=(mid, mid + rows),
-                           threads=threads, want_xyz=False)
+            for y0, y1 in spread_bands(wl.height, rows):
+                sc.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, wl.spp, wl.seed, rows=(y0, y1),
+                               threads=threads, want_xyz=False)
 
     t0 = time.perf_counter()
     band(0, 1)
     dt = time.perf_counter() - t0
-    rows = int(max(1, min(wls[0].height // 2, args.ref_seconds / max(dt, 1e-3))))
+    rows = int(max(1, min(wls[0].height // 8, args.ref_seconds / max(dt, 1e-3))))
     times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         band(i, rows)
         if i >= args.warmup:
             times.append(time.perf_counter() - t0)
-    per = sum(wl.width * rows * wl.spp for wl in wls)
+    per = sum(wl.width * rows * 8 * wl.spp for wl in wls)
     value = per * len(times) / sum(times)
     wl = wls[0]
     what = (f"{len(wls)} renders (one per piece, 14k gold, turntable frame = step)" if reel else "the frame")
     if args.workload == "serve_trace":
         what = f"{len(wls)} renders (one per request class, 1.0M-triangle piece, 14k gold)"
-    sample = (f"rows {wl.height // 2}..{wl.height // 2 + rows} of {what}, {wl.width} wide at {wl.spp} spp "
-              f"({per} path-samples per step)")
+    sample = (f"8 bands of {rows} rows spread down {what} (rows {describe_bands(spread_bands(wl.height, rows))}), "
+              f"{wl.width} wide at {wl.spp} spp ({per} path-samples per step)")
     cfg = {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp,
            "triangles": int(wl.mesh.num_tris), "max_depth": int(wl.settings.max_depth),
            "parallelism": "cpu-threads"}
@@ -319,7 +340,7 @@ def run_reference(args, world, rank):
         "config": cfg,
         "cpu_baseline": {"value": value, "unit": "path-samples/s", "cores": threads, "kind": "port", "cpu": cpu_model(),
                          "sample": sample + "; argent's Rust path cannot be built here (no cargo), so the C++ "
-                                            "restatement (oracle/) runs, OpenMP over rows"},
+                                            "restatement (oracle/) runs, OpenMP over pixels"},
         "e2e": {"value": value, "unit": "path-samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -443,7 +464,8 @@ def run_plan(ctx, plan, k, films=None, spp=None):
 
 
 ORACLE_SPP = 65536
-ORACLE_ROWS = 8
+ORACLE_ROWS = 4  # rows per band; 8 bands spread down the frame
+CONVERGE_SPP = (1024, 4096, 16384)
 
 
 def rel_rmse(img, ref):
@@ -453,37 +475,72 @@ def rel_rmse(img, ref):
     return [float(v) for v in np.sqrt(((img - ref) ** 2).sum(0)) / np.sqrt((ref ** 2).sum(0))]
 
 
-def accuracy(ctx, plan, cpu_scene, threads):
-    """Error of the benchmarked render against the FP64 oracle: an
-    FP64-accumulated 65,536-spp render (on the device, through a band camera
-    and an independent seed) of ORACLE_ROWS rows at mid-frame, scored by
-    relRMSE per XYZ channel for the GPU render of the timed steps and, when
-    `cpu_scene` is given, for argent's algorithm (the CPU restatement) at the
-    same spp on the same rows."""
-    from argent_b200 import _native as N
+def render_bands(ctx, wl, scene, bands, spp, seed, flags):
+    """The frame's rows [y0, y1) of each band, rendered through band cameras
+    in one render_batch; returns the bands' XYZ stacked row-wise."""
     from argent_b200 import workloads as W
-    from argent_b200.gpu import Film, render_pass
+    from argent_b200.gpu import Film, render_batch
+
+    films = [Film(ctx, wl.width, y1 - y0, flags) for y0, y1 in bands]
+    render_batch(ctx, [(scene, W.band_camera(wl.camera, wl.height, y0, y1), f, wl.settings, spp, seed)
+                       for (y0, y1), f in zip(bands, films)])
+    out = np.concatenate([f.xyz() for f in films], 0)
+    for f in films:
+        f.close()
+    return out
+
+
+def accuracy(ctx, plan, cpu_scene, threads, gpu_rate=None, cpu_rate=None):
+    """Error against the FP64 oracle: an FP64-accumulated 65,536-spp render
+    (on the device, through band cameras, independent seed) of 8 bands of
+    ORACLE_ROWS rows spread down the frame, scored by relRMSE per XYZ channel
+    for the GPU render of the timed steps and, when `cpu_scene` is given,
+    for argent's algorithm (the CPU restatement) at the same spp on the same
+    rows.  Then the GPU renders the same bands at CONVERGE_SPP samples: the
+    first spp whose error is at most 1 % in every channel, and the frame time
+    that spp takes on the GPU and on the CPU at their measured rates."""
+    from argent_b200 import _native as N
 
     wl, scene, film = plan.accuracy_target(ctx)
-    y0 = wl.height // 2
-    y1 = min(wl.height, y0 + ORACLE_ROWS)
-    gpu = film.xyz()[y0:y1]
-    ref = Film(ctx, wl.width, y1 - y0, N.FILM_FP64)
+    bands = spread_bands(wl.height, ORACLE_ROWS)
+    full = film.xyz()
+    gpu = np.concatenate([full[y0:y1] for y0, y1 in bands], 0)
     t0 = time.perf_counter()
-    render_pass(ctx, scene, W.band_camera(wl.camera, wl.height, y0, y1), ref, wl.settings, ORACLE_SPP,
-                wl.seed ^ 0x5BD1E995)
-    o = ref.xyz()
+    o = render_bands(ctx, wl, scene, bands, ORACLE_SPP, wl.seed ^ 0x5BD1E995, N.FILM_FP64)
     dt = time.perf_counter() - t0
-    ref.close()
-    out = {"oracle": f"{wl.name}: rows {y0}..{y1}, FP64 film, {ORACLE_SPP} spp on the device, independent seed "
-                     f"({dt:.1f} s)",
+    out = {"oracle": f"{wl.name}: rows {describe_bands(bands)}, FP64 film, {ORACLE_SPP} spp on the device, "
+                     f"independent seed ({dt:.1f} s)",
            "spp": wl.spp, "gpu_relrmse_xyz": rel_rmse(gpu, o)}
     if cpu_scene is not None:
-        _, _, _, xyz = cpu_scene.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, wl.spp, wl.seed,
-                                             rows=(y0, y1), threads=threads)
-        cpu = xyz[y0:y1] / wl.spp
+        parts = []
+        for y0, y1 in bands:
+            _, _, _, xyz = cpu_scene.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, wl.spp, wl.seed,
+                                                 rows=(y0, y1), threads=threads)
+            parts.append(xyz[y0:y1] / wl.spp)
+        cpu = np.concatenate(parts, 0)
         out["cpu_relrmse_xyz"] = rel_rmse(cpu, o)
         out["gpu_vs_cpu_relrmse_xyz"] = rel_rmse(gpu, cpu)
+    # Convergence toward the oracle.  The oracle's own noise is the error
+    # at 256 spp scaled by sqrt(256 / 65536); it adds in quadrature.
+    curve = [[wl.spp, max(out["gpu_relrmse_xyz"])]]
+    for spp in CONVERGE_SPP:
+        if spp <= wl.spp:
+            continue
+        g = render_bands(ctx, wl, scene, bands, spp, wl.seed, N.FILM_KAHAN)
+        curve.append([spp, max(rel_rmse(g, o))])
+    reach = next((spp for spp, e in curve if e <= 0.01), None)
+    e0 = curve[0][1]
+    law = wl.spp * (e0 / 0.01) ** 2  # spp where an unbiased estimate's error falls to 1 % (1/sqrt(spp))
+    px = wl.width * wl.height
+    out["to_1pct"] = {
+        "curve_spp_max_relrmse": curve,
+        "first_measured_spp_at_or_below_1pct": reach,
+        "spp_by_inverse_sqrt_law": law,
+        "oracle_noise_relrmse": e0 * (wl.spp / ORACLE_SPP) ** 0.5,
+        "gpu_seconds_per_frame": (law * px / gpu_rate) if gpu_rate else None,
+        "cpu_seconds_per_frame": (law * px / cpu_rate) if cpu_rate else None,
+        "note": "frame time at the 1 % spp from the measured path-samples/s of each side",
+    }
     return out
 
 
@@ -523,7 +580,6 @@ def run_gpu(args, world, rank, device):
     clocks = Clocks(smi_index(device))
     clocks.start()
     time.sleep(0.3)
-    ctx.set_profiling(True)
     launches0 = ctx.kernel_launches
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -536,8 +592,6 @@ def run_gpu(args, world, rank, device):
     wall_ms = 1e3 * (time.perf_counter() - tw0)
     ctx.sync()
     launches = ctx.kernel_launches - launches0
-    kt = ctx.kernel_times()
-    ctx.set_profiling(False)
     ck = clocks.stop()
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(ms, world, device)
@@ -545,14 +599,29 @@ def run_gpu(args, world, rank, device):
     samples_per_step = plan.path_samples
     value = whole_job_rate(world, samples_per_step * args.steps, ms_max / 1000.0)
 
-    # Roofline of the dominant kernel: closest-hit traversal, the largest
-    # share of serialised device time in the ncu launch list
-    # (profiles/launches_signet_still.md).  With lanes overlapping, the live
-    # per-class event totals include time shared with other lanes' kernels,
-    # so they do not rank the kernels.
-    dom = "intersect"
+    # Roofline leg (not timed into `value`): one step on ONE lane with CUDA
+    # events around every launch.  On one lane each kernel runs alone on the
+    # device (the timed steps overlap eight lanes' kernels, so event pairs
+    # there bracket other lanes' work too); the per-kernel totals then give
+    # each kernel's own average launch time and its share of serialised
+    # device time, comparable with the ncu launch list.
+    lanes_cfg, wave_cfg = ctx.config()
+    ctx.set_config(1, wave_cfg)
+    run_plan(ctx, plan, 0)  # lane 0's buffers and graphs warm
+    ctx.sync()
+    ctx.set_profiling(True)
+    run_plan(ctx, plan, 0)
+    ctx.sync()
+    kt = ctx.kernel_times()
+    ctx.set_profiling(False)
+    ctx.set_config(lanes_cfg, wave_cfg)
+    serial_total = sum(v[0] for v in kt.values()) or 1.0
+
+    # Dominant kernel: the single kernel with the largest share of serialised
+    # device time (closest-hit traversal here; "shade" totals the five
+    # per-class shading kernels, each of which is smaller).
+    dom = max(("intersect", "shadow", "raygen", "film"), key=lambda k: kt[k][0])
     dom_ms, dom_n = kt[dom]
-    path_samples_timed = samples_per_step * args.steps
     per_sample = {}
     node_b, tri_b = 80, 48
     rays_c = counts["closest_rays"] / px
@@ -570,17 +639,22 @@ def run_gpu(args, world, rank, device):
         "intersect": (counts["closest_nodes"] * 128 + counts["closest_tris"] * 48) / px + rays_c * (32 + 16 + 16 + 4),
         "shadow": (counts["any_nodes"] * 128 + counts["any_tris"] * 48) / px + rays_a * (48 + 16 + 16)}
     per_sample["film"] = 64.0 + 12.0 * 3 / max(plan.config()["spp"], 1)
-    alg_bytes_total = per_sample[dom] * path_samples_timed
-    achieved = alg_bytes_total / (dom_ms / 1000.0) / 1e9  # GB/s
+    alg_bytes_step = per_sample[dom] * samples_per_step  # one step = the roofline leg's work
+    achieved = alg_bytes_step / (dom_ms / 1000.0) / 1e9  # GB/s over the kernel's own launch time
     peak, peak_kind = peaks()
-    # DRAM traffic per average launch: bytes per ray from the committed ncu
-    # capture (profiles/ncu_traffic.json) times this run's rays per launch.
-    traffic, issue = None, None
+    # DRAM and L2 traffic per launch: bytes per ray from the committed ncu
+    # capture of this kernel (profiles/ncu_traffic.json, which names its
+    # command) times this run's rays per launch of the roofline leg.
+    traffic, issue, l2 = None, None, None
     tr = ncu_traffic()
     if tr and tr.get("kernel") == f"k_{dom}" and tr.get("workload") == plan.name and dom in ("intersect", "shadow"):
-        rays = rays_c if dom == "intersect" else rays_a
-        traffic = tr["dram_bytes_per_ray"] * rays * path_samples_timed / max(dom_n, 1)
+        rays_step = (rays_c if dom == "intersect" else rays_a) * samples_per_step
+        traffic = tr["dram_bytes_per_ray"] * rays_step / max(dom_n, 1)
         issue = tr.get("issue_active_pct")
+        if tr.get("l2_bytes_per_ray"):
+            l2_launch = tr["l2_bytes_per_ray"] * rays_step / max(dom_n, 1)
+            l2 = {"bytes_per_launch": l2_launch, "gbs": l2_launch / (dom_ms / max(dom_n, 1) / 1000.0) / 1e9,
+                  "hit_rate_pct": tr.get("l2_hit_rate_pct")}
 
     # The batched workload's renders one render_pass at a time (the plain
     # single-render path), device-timed like the batch, for comparison.
@@ -643,14 +717,15 @@ def run_gpu(args, world, rank, device):
     cpu, cpu_scene = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
         wl = plan.cpu_wl
-        v, rows, nthr, cpu_scene = cpu_sample(wl, seconds=args.ref_seconds, threads=os.cpu_count() or 1)
+        v, bands, nthr, cpu_scene = cpu_sample(wl, seconds=args.ref_seconds, threads=os.cpu_count() or 1)
         cpu = {"value": v, "unit": "path-samples/s", "cores": nthr, "kind": "port", "cpu": cpu_model(),
-               "sample": f"{wl.name}: rows {wl.height // 2}..{wl.height // 2 + rows} of the frame at {wl.spp} spp; "
+               "sample": f"{wl.name}: 8 bands spread down the frame (rows {describe_bands(bands)}) at {wl.spp} spp; "
                          f"argent's algorithm as restated in oracle/ (Rust reference not buildable here), "
-                         f"OpenMP over rows"}
+                         f"OpenMP over pixels on every host thread"}
     acc = None
     if rank == 0 and not args.no_oracle:
-        acc = accuracy(ctx, plan, cpu_scene, os.cpu_count() or 1)
+        acc = accuracy(ctx, plan, cpu_scene, os.cpu_count() or 1, gpu_rate=value / world,
+                       cpu_rate=cpu["value"] if cpu else None)
 
     if rank == 0:
         cfg = plan.config()
@@ -675,9 +750,12 @@ def run_gpu(args, world, rank, device):
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "alg_bytes_per_path_sample": per_sample[dom],
                          "alg_bytes_per_path_sample_argent_layout": per_sample_ref.get(dom),
-                         "issue_active_pct": issue,
-                         "launches": dom_n, "avg_launch_ms": dom_ms / max(dom_n, 1)},
-            "kernel_ms": {k: round(v[0], 3) for k, v in kt.items()},
+                         "issue_active_pct": issue, "l2": l2,
+                         "launches": dom_n, "avg_launch_ms": dom_ms / max(dom_n, 1),
+                         "timing": "one step on one lane, CUDA events around each launch (each kernel alone "
+                                   "on the device)"},
+            "kernel_ms_alone": {k: round(v[0], 3) for k, v in kt.items()},
+            "kernel_share_alone": {k: round(v[0] / serial_total, 4) for k, v in kt.items()},
             "traversal_per_path_sample": {k: v / px for k, v in counts.items()},
             "traversal_nodes_per_ray_histogram": hist,
             "rays_per_path_sample_by_bounce": {"closest": [round(x / px, 4) for x in bounce_act],

@@ -316,9 +316,13 @@ int argent_trace_anyhit(ArgentCtx* ctx, ArgentPiece* piece, const ArgentRay* ray
  * flight on other streams.
  * Limit: n <= 262,144 rays (2^18); larger n returns ARGENT_E_INVALID.  The
  * device staging is one static array of 12 MiB (rays then hits) that every
- * GPU loading the library holds until exit.  The first call on a device looks
- * up the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  All calls share
+ * GPU loading the library holds until exit.  The first call on a context
+ * looks up the array's device address (cudaGetSymbolAddress) with the
+ * context's device current and keeps it in the context; make that first call
+ * before any stream capture.  A device reset (cudaDeviceReset) ends every
+ * context on the device, and a context created after it looks the address
+ * up again.  A call with the context's profiling on records its launch like
+ * the other trace entry points (events, no device memory).  All calls share
  * the array and it keeps the last call's contents: calls that overlap on the
  * GPU (e.g. two contexts on one device used from two threads) race.
  */
@@ -377,6 +381,14 @@ int argent_autotune(ArgentCtx* ctx, ArgentScene* scene, const ArgentCamera* came
                     ArgentTuneResult* results, uint32_t max_results, uint32_t* n_results);
 /* The context's current lanes and wave size. */
 int argent_ctx_config(const ArgentCtx* ctx, uint32_t* lanes, uint64_t* wave_paths);
+/*
+ * Sets the lanes (1..16) and the wave size (2^16..2^30 path slots) that the
+ * context's next calls use, e.g. a configuration argent_autotune found
+ * earlier for the same kind of render.  Waits for the context stream first.
+ * Lane buffers grow on first use; lanes left unused keep theirs.  Films do
+ * not depend on the configuration beyond the order of their FP32 sums.
+ */
+int argent_ctx_set_config(ArgentCtx* ctx, uint32_t lanes, uint64_t wave_paths);
 
 /* Kernels the library has launched on this context since creation. */
 uint64_t argent_ctx_kernel_launches(const ArgentCtx* ctx);

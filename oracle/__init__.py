@@ -101,22 +101,32 @@ class Bvh:
             lib().oracle_bvh_destroy(self.h)
             self.h = None
 
+    @staticmethod
+    def _rays(rays):
+        """(n, 8) float32 rays, contiguous: the C side reads them as a flat
+        array, so a strided view (rays[::2]) must be copied first."""
+        return np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+
     def intersect(self, rays, threads=0):
+        rays = self._rays(rays)
         hits = np.zeros((len(rays), 4), np.float32)
         lib().oracle_bvh_intersect(self.h, _ptr(rays), len(rays), _ptr(hits), threads)
         return hits
 
     def intersect_binary(self, rays):
+        rays = self._rays(rays)
         hits = np.zeros((len(rays), 4), np.float32)
         lib().oracle_bvh_intersect_binary(self.h, _ptr(rays), len(rays), _ptr(hits))
         return hits
 
     def occluded(self, rays, threads=0):
+        rays = self._rays(rays)
         occ = np.zeros(len(rays), np.uint8)
         lib().oracle_bvh_occluded(self.h, _ptr(rays), len(rays), _ptr(occ), threads)
         return occ
 
     def brute(self, rays, threads=0):
+        rays = self._rays(rays)
         hits = np.zeros((len(rays), 4), np.float32)
         lib().oracle_brute_intersect(_ptr(self.positions), _ptr(self.tris), len(self.tris), _ptr(rays), len(rays),
                                      _ptr(hits), threads)

@@ -1350,10 +1350,15 @@ void oracle_render_pass(const oracle_scene* sc, const ArgentCamera* cam, const A
   (void)energy_table();
   (void)LinearRgb::get();
   int nthr = threads > 0 ? threads : omp_get_max_threads();
-#pragma omp parallel for schedule(dynamic, 1) num_threads(nthr)
-  for (int64_t yy = (int64_t)y0; yy < (int64_t)y1; ++yy) {
-    uint32_t y = (uint32_t)yy;
-    for (uint32_t x = 0; x < w; ++x) {
+  // Work is handed out 16 pixels at a time, so a band of a few rows keeps
+  // every thread busy (pixels are independent: each writes only its own
+  // sums).
+  const int64_t npix = (int64_t)(y1 > y0 ? y1 - y0 : 0) * (int64_t)w;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthr)
+  for (int64_t ip = 0; ip < npix; ++ip) {
+    uint32_t y = y0 + (uint32_t)(ip / w);
+    {
+      uint32_t x = (uint32_t)(ip % w);
       uint32_t pix_seed = hash32((y * w + x) ^ seed_h);
       float acc[3] = {0, 0, 0}, aacc[3] = {0, 0, 0}, nacc[3] = {0, 0, 0};
       double xacc[3] = {0, 0, 0};

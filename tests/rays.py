@@ -108,7 +108,9 @@ def compare_hits(ref, got, bvh, rays, ulps=2):
     Buckets:
       match       same triangle, t within `ulps` (bit-equal expected)
       tie         another triangle at a bit-equal t (argent keeps the first
-                  in its traversal order, the GPU the lower index)
+                  in its traversal order, the GPU the lower index); the
+                  GPU's triangle must then have the lower index of the two
+                  (`tie_not_lower` counts those that do not)
       closer      the GPU hit is strictly closer than argent's, or argent
                   misses it, and the oracle's own Moller-Trumbore confirms the
                   GPU triangle at exactly that t: argent's slab test culled a
@@ -126,7 +128,7 @@ def compare_hits(ref, got, bvh, rays, ulps=2):
     gt = got[:, 0].view(np.int32).astype(np.int64)
     t_bad = same & (np.abs(rt - gt) > ulps)
     cand = np.nonzero((ref_hit | got_hit) & ~same)[0]
-    ties = closer = 0
+    ties = closer = tie_not_lower = 0
     bad = []
     for i in cand:
         if not got_hit[i]:
@@ -138,10 +140,12 @@ def compare_hits(ref, got, bvh, rays, ulps=2):
             continue
         if ref_hit[i] and got[i, 0] == ref[i, 0]:
             ties += 1
+            tie_not_lower += int(gp[i] > rp[i])
         elif (not ref_hit[i]) or got[i, 0] < ref[i, 0]:
             closer += 1
         else:
             bad.append(i)
-    out.update(match=int(same.sum() - t_bad.sum()), tie=ties, closer=closer, t_ulp_fail=int(t_bad.sum()),
+    out.update(match=int(same.sum() - t_bad.sum()), tie=ties, tie_not_lower=tie_not_lower, closer=closer,
+               t_ulp_fail=int(t_bad.sum()),
                mismatch=len(bad), mismatch_idx=np.array(bad[:20], np.int64))
     return out

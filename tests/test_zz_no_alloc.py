@@ -45,6 +45,60 @@ def test_noalloc_closest_hit_matches_allocating_entry_point():
         assert ulps.max() <= 2  # the traversal tests' tolerance on t
 
 
+def _cudart():
+    """The CUDA runtime the library was linked against (already loaded)."""
+    return ctypes.CDLL("libcudart.so.12")
+
+
+def _device_memory_state(rt, device=0):
+    """(free bytes on the device, reserved and used bytes of its default
+    stream-ordered memory pool)."""
+    free, total = ctypes.c_size_t(), ctypes.c_size_t()
+    assert rt.cudaMemGetInfo(ctypes.byref(free), ctypes.byref(total)) == 0
+    pool = ctypes.c_void_p()
+    assert rt.cudaDeviceGetDefaultMemPool(ctypes.byref(pool), device) == 0
+    out = [free.value]
+    for attr in (5, 7):  # cudaMemPoolAttrReservedMemCurrent, cudaMemPoolAttrUsedMemCurrent
+        v = ctypes.c_uint64()
+        assert rt.cudaMemPoolGetAttribute(pool, attr, ctypes.byref(v)) == 0
+        out.append(v.value)
+    return tuple(out), pool
+
+
+@pytest.mark.gpu
+def test_noalloc_allocates_no_device_memory():
+    """After a first call (which looks up the array's address and loads the
+    kernel), further calls leave the device's free memory and its default
+    memory pool exactly as they were."""
+    from argent_b200 import _native as N
+    from argent_b200 import mesh
+    from argent_b200.gpu import Context, Piece
+
+    ring = mesh.ring()
+    ctx = Context(0)
+    piece = Piece(ctx, ring)
+    n = 100_000
+    rays = np.ascontiguousarray(make_rays(ring.positions, ring.tris, n, seed=23))
+    hits = np.zeros((n, 4), np.float32)
+
+    def call():
+        rc = ctx.lib.argent_trace_closest_noalloc(ctx.h, piece.h, rays.ctypes.data_as(ctypes.c_void_p), n,
+                                                  hits.ctypes.data_as(ctypes.c_void_p))
+        assert rc == N.OK, ctx.lib.argent_last_error(ctx.h)
+
+    call()
+    ctx.sync()
+    rt = _cudart()
+    _, pool = _device_memory_state(rt)
+    assert rt.cudaMemPoolTrimTo(pool, ctypes.c_size_t(0)) == 0
+    before, _ = _device_memory_state(rt)
+    for _ in range(3):
+        call()
+    after, _ = _device_memory_state(rt)
+    assert after == before, (before, after)
+    assert (hits[:, 3].view(np.uint32) != 0xFFFFFFFF).sum() > n // 4
+
+
 @pytest.mark.gpu
 def test_noalloc_rejects_more_rays_than_its_array_holds():
     from argent_b200 import _native as N
