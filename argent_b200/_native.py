@@ -21,6 +21,7 @@ MAT_METAL, MAT_GEM, MAT_PLASTIC, MAT_OPAL, MAT_DIFFUSE, MAT_BLACK = range(6)
 GEM_TRANSPARENT, GEM_OPAL, GEM_OPAQUE = range(3)
 ENV_GRADIENT, ENV_MAP = range(2)
 FILM_KAHAN, FILM_FP64, FILM_PROGRESSIVE = 1, 2, 4
+TRI_MOLLER_TRUMBORE, TRI_WATERTIGHT = 0, 1
 FILM_FP64_AFTER = 4096
 
 c_float_p = ctypes.POINTER(ctypes.c_float)
@@ -105,7 +106,7 @@ class ArgentBatchItem(ctypes.Structure):
 class ArgentServeConfig(ctypes.Structure):
     _fields_ = [("film_budget", ctypes.c_uint64), ("max_active", ctypes.c_uint32), ("aging_ms", ctypes.c_uint32),
                 ("step_path_samples", ctypes.c_uint64), ("step_path_samples_max", ctypes.c_uint64),
-                ("overlap", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("overlap", ctypes.c_uint32), ("max_pending", ctypes.c_uint32)]
 
 
 class ArgentServeRequest(ctypes.Structure):
@@ -136,6 +137,11 @@ class ArgentPatinaSettings(ctypes.Structure):
     _fields_ = [("ao_samples", ctypes.c_uint32), ("ao_distance", ctypes.c_float),
                 ("curvature_radius", ctypes.c_float), ("concavity_weight", ctypes.c_float),
                 ("smooth_iterations", ctypes.c_uint32)]
+
+
+class ArgentTuning(ctypes.Structure):
+    _fields_ = [("lanes", ctypes.c_uint32), ("trace_blocks_per_sm", ctypes.c_uint32), ("wave_paths", ctypes.c_uint64),
+                ("shade_blocks_per_sm", ctypes.c_uint32 * 5), ("reserved", ctypes.c_uint32)]
 
 
 class ArgentTuneResult(ctypes.Structure):
@@ -194,6 +200,9 @@ GPU_FUNCS = {
     "argent_ctx_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
                                          ctypes.POINTER(ctypes.c_uint64)]),
     "argent_ctx_set_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64]),
+    "argent_ctx_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ArgentTuning)]),
+    "argent_ctx_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ArgentTuning)]),
+    "argent_piece_set_triangle_test": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
     "argent_trace_closest_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                     ctypes.c_uint64, ctypes.c_void_p]),
     "argent_ctx_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

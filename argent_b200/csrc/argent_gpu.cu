@@ -83,6 +83,27 @@ __global__ void k_trace_any(DevPiece pc, const ArgentRay* __restrict__ rays, uin
   }
 }
 
+// Rewrites every triangle record of a piece for a triangle test: (v0, e1,
+// e2) with e = v - v0 rounded as the host builder rounds it (argent's
+// Moller-Trumbore), or the three original vertices (v0, v1, v2) marked
+// watertight.  The record's original index (v0.w) names its vertices.
+__global__ void k_tri_records(float4* tris, const uint4* __restrict__ tri_idx, const float4* __restrict__ pos,
+                              uint32_t n, int watertight) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t prim = __float_as_uint(tris[3 * (size_t)i].w);
+    uint4 t = __ldg(tri_idx + prim);
+    float4 a = __ldg(pos + t.x), b = __ldg(pos + t.y), c = __ldg(pos + t.z);
+    tris[3 * (size_t)i] = make_float4(a.x, a.y, a.z, __uint_as_float(prim));
+    if (watertight) {
+      tris[3 * (size_t)i + 1] = make_float4(b.x, b.y, b.z, __uint_as_float(ARGENT_TRI_REC_WATERTIGHT));
+      tris[3 * (size_t)i + 2] = make_float4(c.x, c.y, c.z, 0.0f);
+    } else {
+      tris[3 * (size_t)i + 1] = make_float4(__fsub_rn(b.x, a.x), __fsub_rn(b.y, a.y), __fsub_rn(b.z, a.z), 0.0f);
+      tris[3 * (size_t)i + 2] = make_float4(__fsub_rn(c.x, a.x), __fsub_rn(c.y, a.y), __fsub_rn(c.z, a.z), 0.0f);
+    }
+  }
+}
+
 // ------------------------------------------------------------------ cavity ambient occlusion
 
 // cavity.rs:96-135, one thread per (vertex, sample): the ray from the
@@ -576,6 +597,26 @@ int argent_piece_upload_device_bvh(ArgentCtx* ctx, const float* positions, uint3
   p->dev.cavity = (const float*)dc;
   p->dev.num_tris = nt;
   *out = p;
+  return ARGENT_OK;
+}
+
+int argent_piece_set_triangle_test(ArgentCtx* ctx, ArgentPiece* piece, int test) {
+  if (!ctx || !piece) return set_error(ctx, ARGENT_E_INVALID, "argent_piece_set_triangle_test: NULL argument");
+  if (piece->ctx != ctx) return set_error(ctx, ARGENT_E_INVALID, "piece belongs to another context");
+  if (test != ARGENT_TRI_MOLLER_TRUMBORE && test != ARGENT_TRI_WATERTIGHT)
+    return set_error(ctx, ARGENT_E_INVALID, "unknown triangle test");
+  if (piece->nt == 0) return ARGENT_OK;
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  // Renders in flight read the records: rewrite them only once the
+  // context's work is done.
+  ARGENT_CK(ctx, cudaDeviceSynchronize());
+  int grid = grid_for(ctx, (const void*)k_tri_records, 256, piece->nt);
+  k_tri_records<<<grid, 256, 0, ctx->stream>>>(const_cast<float4*>(piece->dev.tris), piece->dev.tri_idx,
+                                                piece->dev.pos, piece->nt, test == ARGENT_TRI_WATERTIGHT ? 1 : 0);
+  ctx->launches++;
+  ARGENT_CK(ctx, cudaGetLastError());
+  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  piece->tri_test = test;
   return ARGENT_OK;
 }
 
@@ -1168,19 +1209,32 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
     fill_args(args[l], ctx->wave[l]);
   }
   int g_ray = grid_for(ctx, (const void*)dev::k_raygen, 256, cap);
-  int g_int[2] = {grid_for(ctx, (const void*)dev::k_intersect<false>, 128, cap),
-                   grid_for(ctx, (const void*)dev::k_intersect<true>, 128, cap)};
+  // Traversal grids: every resident block, or the tuned blocks per SM.
+  auto tuned_grid = [&](int g, int bpsm) {
+    if (bpsm <= 0) return g;
+    uint64_t want = std::min<uint64_t>((cap + 127) / 128, (uint64_t)ctx->num_sms * bpsm);
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)g));
+  };
+  int g_int[2] = {tuned_grid(grid_for(ctx, (const void*)dev::k_intersect<false>, 128, cap), ctx->trace_bpsm),
+                  tuned_grid(grid_for(ctx, (const void*)dev::k_intersect<true>, 128, cap), ctx->trace_bpsm)};
   // Shading grids: ARGENT_SHADE_BLOCKS blocks per SM for the terminal,
   // dielectric and other classes; the metal and coated classes size their
-  // own from their occupancy.
+  // own from their occupancy; a tuned class takes its tuned blocks per SM
+  // (blocks beyond those resident wait for a free slot, and the persistent
+  // loops take whatever work is left).
   int g_sh[NUM_CLS][2];
   const int g_shared = (int)std::max<uint64_t>(
       1, std::min<uint64_t>((cap + 127) / 128, (uint64_t)ctx->num_sms * ARGENT_SHADE_BLOCKS));
   for (int c = 0; c < NUM_CLS; ++c) g_sh[c][0] = g_sh[c][1] = g_shared;
   shade_grids<CLS_METAL>(ctx, cap, g_sh[CLS_METAL]);
   shade_grids<CLS_COATED>(ctx, cap, g_sh[CLS_COATED]);
-  int g_any[2] = {grid_for(ctx, (const void*)dev::k_shadow<false>, 128, cap),
-                  grid_for(ctx, (const void*)dev::k_shadow<true>, 128, cap)};
+  for (int c = 0; c < NUM_CLS; ++c) {
+    if (ctx->shade_bpsm[c] <= 0) continue;
+    g_sh[c][0] = g_sh[c][1] = (int)std::max<uint64_t>(
+        1, std::min<uint64_t>((cap + 127) / 128, (uint64_t)ctx->num_sms * ctx->shade_bpsm[c]));
+  }
+  int g_any[2] = {tuned_grid(grid_for(ctx, (const void*)dev::k_shadow<false>, 128, cap), ctx->trace_bpsm),
+                  tuned_grid(grid_for(ctx, (const void*)dev::k_shadow<true>, 128, cap), ctx->trace_bpsm)};
   int g_film = grid_for(ctx, (const void*)dev::k_film, 256, cap);
   // Per wave: its classes, whether any of its scenes has an env map (the
   // shading kernels without one leave the map code out) and, for a one-scene
@@ -1302,6 +1356,9 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
     put(&nlanes, sizeof(nlanes));
     put(&start, sizeof(start));
     put(&cap, sizeof(cap));
+    put(g_int, sizeof(g_int));
+    put(g_any, sizeof(g_any));
+    put(g_sh, sizeof(g_sh));
     put(&d_jobs, sizeof(d_jobs));
     for (int k = 0; k < used; ++k) put(&args[(start + k) % nlanes], sizeof(dev::WaveArgs));
     for (size_t wi = 0; wi < waves.size(); ++wi) {
@@ -1931,12 +1988,72 @@ int argent_autotune(ArgentCtx* ctx, ArgentScene* scene, const ArgentCamera* came
     }
     if (rc != ARGENT_OK) break;
   }
+  // Second phase at the best lanes and wave size: blocks per SM of each
+  // shading class the scene uses, then of the traversals, one knob at a
+  // time; a value is kept only when it is faster by more than 1 %, which
+  // is above the run-to-run spread of such a render.
+  const int keep_trace = ctx->trace_bpsm;
+  int keep_shade[NUM_CLS];
+  for (int c = 0; c < NUM_CLS; ++c) keep_shade[c] = ctx->shade_bpsm[c];
+  if (rc == ARGENT_OK && best > 0.0) {
+    ctx->lanes = best_lanes;
+    ctx->limits.wave_paths = best_wave;
+    auto measure = [&](double* v) -> int {
+      int r = argent_film_clear(film);
+      if (r == ARGENT_OK) r = argent_render_pass(ctx, scene, camera, film, settings, count, 1);  // warm-up
+      if (r == ARGENT_OK) r = argent_film_clear(film);
+      if (r != ARGENT_OK) return r;
+      cudaEventRecord(e0, ctx->stream);
+      r = argent_render_pass(ctx, scene, camera, film, settings, count, 1);
+      cudaEventRecord(e1, ctx->stream);
+      if (r == ARGENT_OK) r = argent_ctx_sync(ctx);
+      if (r != ARGENT_OK) return r;
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      *v = ms > 0.0f ? (double)path_samples / (ms * 1e-3) : 0.0;
+      return ARGENT_OK;
+    };
+    double cur = 0.0;
+    rc = measure(&cur);
+    const uint32_t classes = (1u << CLS_TERMINAL) | scene->host.class_mask;
+    const int shade_c[] = {2, 3, 4, 5, 6, 8};
+    for (int c = 0; c < NUM_CLS && rc == ARGENT_OK; ++c) {
+      if (!((classes >> c) & 1u)) continue;
+      int keep = ctx->shade_bpsm[c];
+      for (int v : shade_c) {
+        ctx->shade_bpsm[c] = v;
+        double r = 0.0;
+        rc = measure(&r);
+        if (rc != ARGENT_OK) break;
+        if (r > cur * 1.01) {
+          cur = r;
+          keep = v;
+        }
+      }
+      ctx->shade_bpsm[c] = keep;
+    }
+    const int trace_c[] = {4, 6, 8};
+    int keep_t = ctx->trace_bpsm;
+    for (int v : trace_c) {
+      if (rc != ARGENT_OK) break;
+      ctx->trace_bpsm = v;
+      double r = 0.0;
+      rc = measure(&r);
+      if (rc == ARGENT_OK && r > cur * 1.01) {
+        cur = r;
+        keep_t = v;
+      }
+    }
+    ctx->trace_bpsm = keep_t;
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   argent_film_destroy(film);
   if (rc != ARGENT_OK) {
     ctx->lanes = keep_lanes;
     ctx->limits.wave_paths = keep_wave;
+    ctx->trace_bpsm = keep_trace;
+    for (int c = 0; c < NUM_CLS; ++c) ctx->shade_bpsm[c] = keep_shade[c];
     return rc;
   }
   ctx->lanes = best_lanes;
@@ -1951,6 +2068,28 @@ int argent_ctx_config(const ArgentCtx* ctx, uint32_t* lanes, uint64_t* wave_path
   if (!ctx) return set_error(nullptr, ARGENT_E_INVALID, "ctx is NULL");
   if (lanes) *lanes = (uint32_t)ctx->lanes;
   if (wave_paths) *wave_paths = ctx->limits.wave_paths;
+  return ARGENT_OK;
+}
+
+int argent_ctx_tuning(const ArgentCtx* ctx, ArgentTuning* out) {
+  if (!ctx || !out) return set_error(ctx, ARGENT_E_INVALID, "argent_ctx_tuning: NULL argument");
+  std::memset(out, 0, sizeof(*out));
+  out->lanes = (uint32_t)ctx->lanes;
+  out->wave_paths = ctx->limits.wave_paths;
+  out->trace_blocks_per_sm = (uint32_t)ctx->trace_bpsm;
+  for (int c = 0; c < NUM_CLS; ++c) out->shade_blocks_per_sm[c] = (uint32_t)ctx->shade_bpsm[c];
+  return ARGENT_OK;
+}
+
+int argent_ctx_set_tuning(ArgentCtx* ctx, const ArgentTuning* t) {
+  if (!ctx || !t) return set_error(ctx, ARGENT_E_INVALID, "argent_ctx_set_tuning: NULL argument");
+  if (t->trace_blocks_per_sm > 64) return set_error(ctx, ARGENT_E_INVALID, "trace_blocks_per_sm above 64");
+  for (int c = 0; c < NUM_CLS; ++c)
+    if (t->shade_blocks_per_sm[c] > 64) return set_error(ctx, ARGENT_E_INVALID, "shade_blocks_per_sm above 64");
+  int rc = argent_ctx_set_config(ctx, t->lanes, t->wave_paths);
+  if (rc != ARGENT_OK) return rc;
+  ctx->trace_bpsm = (int)t->trace_blocks_per_sm;
+  for (int c = 0; c < NUM_CLS; ++c) ctx->shade_bpsm[c] = (int)t->shade_blocks_per_sm[c];
   return ARGENT_OK;
 }
 

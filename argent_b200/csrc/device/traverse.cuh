@@ -37,12 +37,83 @@ struct DevPiece {
   uint32_t num_tris;
 };
 
-// Moller-Trumbore, bvh.rs:391-410.  Returns t > 0 on a hit, else -1.
+// Watertight ray-triangle test (Woop, Benthin and Wald, "Watertight
+// Ray/Triangle Intersection", JCGT 2(1), 2013), the optional alternative to
+// argent's Moller-Trumbore.  The ray is sheared so that it runs along +z of
+// a permuted frame (kz = the axis of largest |d|); the three 2D edge
+// functions of the sheared vertices decide the hit.  Two triangles sharing
+// an edge evaluate that edge's function from the same two vertices with the
+// same arithmetic, so their signs agree and no ray passes between them; an
+// edge function of exactly zero is recomputed in double precision so that
+// its sign is exact.  Both faces count (argent's test is two-sided too).
+// The record holds the three original vertices (v0, v1, v2); the hit's
+// (u, v) weigh v1 and v2, as Moller-Trumbore's do.
+__device__ __forceinline__ float pick3(float x, float y, float z, int k) { return k == 0 ? x : (k == 1 ? y : z); }
+
+__device__ __forceinline__ bool wt_hit(float4 a, float4 b, float4 c, V3 o, V3 d, float t_max, float* t_out,
+                                       float* u_out, float* v_out) {
+  float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+  int kx = kz == 2 ? 0 : kz + 1;
+  int ky = kx == 2 ? 0 : kx + 1;
+  float dz = pick3(d.x, d.y, d.z, kz);
+  if (dz < 0.0f) {
+    int t = kx;
+    kx = ky;
+    ky = t;
+  }
+  float sx = __fdiv_rn(pick3(d.x, d.y, d.z, kx), dz), sy = __fdiv_rn(pick3(d.x, d.y, d.z, ky), dz);
+  float sz = __fdiv_rn(1.0f, dz);
+  // Vertices relative to the origin, then permuted (x, y, z) = (kx, ky, kz).
+  V3 A = V3{a.x, a.y, a.z} - o, B = V3{b.x, b.y, b.z} - o, C = V3{c.x, c.y, c.z} - o;
+  float Akz = pick3(A.x, A.y, A.z, kz), Bkz = pick3(B.x, B.y, B.z, kz), Ckz = pick3(C.x, C.y, C.z, kz);
+  float Ax = __fsub_rn(pick3(A.x, A.y, A.z, kx), __fmul_rn(sx, Akz));
+  float Ay = __fsub_rn(pick3(A.x, A.y, A.z, ky), __fmul_rn(sy, Akz));
+  float Bx = __fsub_rn(pick3(B.x, B.y, B.z, kx), __fmul_rn(sx, Bkz));
+  float By = __fsub_rn(pick3(B.x, B.y, B.z, ky), __fmul_rn(sy, Bkz));
+  float Cx = __fsub_rn(pick3(C.x, C.y, C.z, kx), __fmul_rn(sx, Ckz));
+  float Cy = __fsub_rn(pick3(C.x, C.y, C.z, ky), __fmul_rn(sy, Ckz));
+  float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+  float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+  float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+  if (U == 0.0f || V == 0.0f || W == 0.0f) {
+    // The product of two floats is exact in double, so the difference of
+    // two such products has the exact sign.
+    U = (float)__dsub_rn(__dmul_rn((double)Cx, (double)By), __dmul_rn((double)Cy, (double)Bx));
+    V = (float)__dsub_rn(__dmul_rn((double)Ax, (double)Cy), __dmul_rn((double)Ay, (double)Cx));
+    W = (float)__dsub_rn(__dmul_rn((double)Bx, (double)Ay), __dmul_rn((double)By, (double)Ax));
+  }
+  if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+  float det = __fadd_rn(__fadd_rn(U, V), W);
+  if (det == 0.0f) return false;
+  float T = __fadd_rn(__fadd_rn(__fmul_rn(U, __fmul_rn(sz, Akz)), __fmul_rn(V, __fmul_rn(sz, Bkz))),
+                      __fmul_rn(W, __fmul_rn(sz, Ckz)));
+  float inv = __fdiv_rn(1.0f, det);
+  float t = __fmul_rn(T, inv);
+  if (!(t > 1e-7f && t < t_max)) return false;
+  *t_out = t;
+  *u_out = __fmul_rn(V, inv);
+  *v_out = __fmul_rn(W, inv);
+  return true;
+}
+
+// The triangle test a record asks for: the bits of its second word's w are
+// 0 for argent's Moller-Trumbore (record = v0, e1, e2) and
+// ARGENT_TRI_REC_WATERTIGHT for the watertight test (record = v0, v1, v2).
+#define ARGENT_TRI_REC_WATERTIGHT 1u
+
+// Moller-Trumbore, bvh.rs:391-410 (or the watertight test, by the
+// record's marker).  True on a hit with t in (1e-7, t_max).
 __device__ __forceinline__ bool mt_hit(const float4* tri, V3 o, V3 d, float t_max, float* t_out, float* u_out,
                                        float* v_out, uint32_t* prim_out) {
   float4 a = __ldg(tri);
   float4 b = __ldg(tri + 1);
   float4 c = __ldg(tri + 2);
+  if (__float_as_uint(b.w) == ARGENT_TRI_REC_WATERTIGHT) {
+    if (!wt_hit(a, b, c, o, d, t_max, t_out, u_out, v_out)) return false;
+    *prim_out = __float_as_uint(a.w);
+    return true;
+  }
   V3 v0{a.x, a.y, a.z}, e1{b.x, b.y, b.z}, e2{c.x, c.y, c.z};
   V3 p = cross(d, e2);
   float det = dot(e1, p);
@@ -234,6 +305,42 @@ __device__ __forceinline__ bool child_q(const NodeQ& q, int c, float t_max, floa
   return tmin <= tmax;
 }
 
+// Traversal stacks.  LocalStack keeps a thread's whole stack in its local
+// memory.  ShortStack keeps the top S entries in shared memory (a ring per
+// thread: entry k in row k % S of the thread's column, so the 32 threads of
+// a warp touch 32 consecutive words and no bank twice) and moves older
+// entries to a local-memory spill array only while the stack is deeper than
+// S: a push that wraps onto an occupied row first writes that row's entry to
+// spill[sp - S], and a pop that uncovers a spilled entry moves it back into
+// the freed row.  The order of entries is the same either way, so
+// traversals, pruning and results do not depend on the stack kind.
+template <typename E>
+struct LocalStack {
+  E* a;
+  __device__ __forceinline__ void push(int& sp, E e) { a[sp++] = e; }
+  __device__ __forceinline__ E pop(int& sp) { return a[--sp]; }
+};
+
+template <typename E, int S, int STRIDE>
+struct ShortStack {
+  static_assert((S & (S - 1)) == 0, "ring size must be a power of two");
+  E* sh;     // this thread's column in the block's shared ring array
+  E* spill;  // this thread's local spill array
+  __device__ __forceinline__ void push(int& sp, E e) {
+    E* row = sh + (sp & (S - 1)) * STRIDE;
+    if (sp >= S) spill[sp - S] = *row;
+    *row = e;
+    ++sp;
+  }
+  __device__ __forceinline__ E pop(int& sp) {
+    --sp;
+    E* row = sh + (sp & (S - 1)) * STRIDE;
+    E e = *row;
+    if (sp >= S) *row = spill[sp - S];
+    return e;
+  }
+};
+
 struct TraceHit {
   float t, u, v;
   uint32_t prim;
@@ -286,7 +393,8 @@ __device__ __forceinline__ void sort8(uint32_t k[8]) {
 // The traversal is resumable: closest_begin sets it up and each
 // closest_step visits one node or one leaf, so a kernel can interleave the
 // steps of rays that start at different times (persistent lanes that take a
-// new ray as soon as theirs finishes).  The stack lives with the caller.
+// new ray as soon as theirs finishes).  The stack (LocalStack or
+// ShortStack) lives with the caller.
 struct ClosestTrav {
   V3 o, d;
   RayQ rq;
@@ -319,11 +427,11 @@ __device__ __forceinline__ bool closest_begin(const DevPiece& pc, ClosestTrav& s
 
 // Makes the next node or leaf current (popping entries that the running
 // best has pruned); false when the traversal is over.
-__device__ __forceinline__ bool closest_next(ClosestTrav& s, const uint2* stack) {
+template <class ST>
+__device__ __forceinline__ bool closest_next(ClosestTrav& s, ST& stack) {
   if (s.have) return true;
   while (s.sp > 0) {
-    --s.sp;
-    uint2 e = stack[s.sp];
+    uint2 e = stack.pop(s.sp);
     if (__uint_as_float(e.y) <= s.best.t) {
       s.ref = e.x;
       s.have = true;
@@ -337,7 +445,8 @@ __device__ __forceinline__ bool trav_at_leaf(uint32_t ref) { return (ref & ARGEN
 
 // Visits the current node or leaf (closest_next returned true); true while
 // the traversal has more to visit.
-__device__ __forceinline__ bool closest_visit(const DevPiece& pc, ClosestTrav& s, uint2* stack, uint32_t* status) {
+template <class ST>
+__device__ __forceinline__ bool closest_visit(const DevPiece& pc, ClosestTrav& s, ST& stack, uint32_t* status) {
   s.have = false;
   uint32_t ref = s.ref;
   if (ref & ARGENT_LEAF_BIT) {
@@ -381,7 +490,7 @@ __device__ __forceinline__ bool closest_visit(const DevPiece& pc, ClosestTrav& s
   sort8(k);
 #pragma unroll
   for (int j = 7; j >= 1; --j) {
-    if (j < nh) stack[s.sp++] = make_uint2(child_ref(n, (int)(k[j] & 7u)), k[j] & ~7u);
+    if (j < nh) stack.push(s.sp, make_uint2(child_ref(n, (int)(k[j] & 7u)), k[j] & ~7u));
   }
   s.ref = child_ref(n, (int)(k[0] & 7u));
   s.have = true;
@@ -389,14 +498,16 @@ __device__ __forceinline__ bool closest_visit(const DevPiece& pc, ClosestTrav& s
 }
 
 // Visits one node or one leaf; true when the traversal has finished.
-__device__ __forceinline__ bool closest_step(const DevPiece& pc, ClosestTrav& s, uint2* stack, uint32_t* status) {
+template <class ST>
+__device__ __forceinline__ bool closest_step(const DevPiece& pc, ClosestTrav& s, ST& stack, uint32_t* status) {
   if (!closest_next(s, stack)) return true;
   return !closest_visit(pc, s, stack, status);
 }
 
 __device__ __noinline__ TraceHit trace_closest(const DevPiece& pc, V3 o, V3 d, float t_max, uint32_t* status) {
   ClosestTrav s;
-  uint2 stack[ARGENT_STACK_SIZE];
+  uint2 arr[ARGENT_STACK_SIZE];
+  LocalStack<uint2> stack{arr};
   if (closest_begin(pc, s, o, d, t_max))
     while (!closest_step(pc, s, stack, status)) {
     }
@@ -429,7 +540,8 @@ __device__ __forceinline__ bool piece_may_occlude(const DevPiece& pc, V3 o, V3 d
 
 // Returns ARGENT_ANY_RUNNING, or ARGENT_ANY_CLEAR when the ray misses the
 // piece outright.
-__device__ __forceinline__ int any_begin(const DevPiece& pc, AnyTrav& s, uint32_t* stack, V3 o, V3 d, float t_max) {
+template <class ST>
+__device__ __forceinline__ int any_begin(const DevPiece& pc, AnyTrav& s, ST& stack, V3 o, V3 d, float t_max) {
   s.o = o;
   s.d = d;
   s.t_max = t_max;
@@ -440,22 +552,24 @@ __device__ __forceinline__ int any_begin(const DevPiece& pc, AnyTrav& s, uint32_
   if (pc.num_tris == 0) return ARGENT_ANY_CLEAR;
   s.rq = make_rayq(o, d);
   if (!node_box_hit(pc.nodes, 0u, s.rq, t_max)) return ARGENT_ANY_CLEAR;
-  stack[s.sp++] = 0u;
+  stack.push(s.sp, 0u);
   return ARGENT_ANY_RUNNING;
 }
 
 // Pops the next node or leaf into s.ref; false when none is left.
-__device__ __forceinline__ bool any_next(AnyTrav& s, const uint32_t* stack) {
+template <class ST>
+__device__ __forceinline__ bool any_next(AnyTrav& s, ST& stack) {
   if (s.have) return true;
   if (s.sp == 0) return false;
-  s.ref = stack[--s.sp];
+  s.ref = stack.pop(s.sp);
   s.have = true;
   return true;
 }
 
 // Visits s.ref: ARGENT_ANY_HIT, or ARGENT_ANY_RUNNING / ARGENT_ANY_CLEAR by
 // whether entries remain.
-__device__ __forceinline__ int any_visit(const DevPiece& pc, AnyTrav& s, uint32_t* stack, uint32_t* status) {
+template <class ST>
+__device__ __forceinline__ int any_visit(const DevPiece& pc, AnyTrav& s, ST& stack, uint32_t* status) {
   s.have = false;
   uint32_t ref = s.ref;
   if (ref & ARGENT_LEAF_BIT) {
@@ -487,20 +601,22 @@ __device__ __forceinline__ int any_visit(const DevPiece& pc, AnyTrav& s, uint32_
   while (hitmask) {
     int c = __ffs(hitmask) - 1;
     hitmask &= hitmask - 1u;
-    stack[s.sp++] = child_ref(n, c);
+    stack.push(s.sp, child_ref(n, c));
   }
   return s.sp == 0 ? ARGENT_ANY_CLEAR : ARGENT_ANY_RUNNING;
 }
 
 // Visits one node or one leaf.
-__device__ __forceinline__ int any_step(const DevPiece& pc, AnyTrav& s, uint32_t* stack, uint32_t* status) {
+template <class ST>
+__device__ __forceinline__ int any_step(const DevPiece& pc, AnyTrav& s, ST& stack, uint32_t* status) {
   if (!any_next(s, stack)) return ARGENT_ANY_CLEAR;
   return any_visit(pc, s, stack, status);
 }
 
 __device__ __noinline__ bool trace_any(const DevPiece& pc, V3 o, V3 d, float t_max, uint32_t* status) {
   AnyTrav s;
-  uint32_t stack[ARGENT_STACK_SIZE];
+  uint32_t arr[ARGENT_STACK_SIZE];
+  LocalStack<uint32_t> stack{arr};
   int r = any_begin(pc, s, stack, o, d, t_max);
   while (r == ARGENT_ANY_RUNNING) r = any_step(pc, s, stack, status);
   count_visits(3, s.n_nodes, s.n_tris);

@@ -24,6 +24,10 @@
 // sixteenth of the budget finishes in this step, and every active request
 // advances by at least one sample, so none starves.
 //
+// Bound: with max_pending set, a submit that finds that many requests
+// queued or active is refused with ARGENT_E_BUSY (argent's queue refuses a
+// job when 24 are waiting, serve/queue.rs:28,364-366).
+//
 // Threads: submit, poll and cancel lock the queue and may be called from
 // any thread.  step and read drive the context and belong to the thread
 // that owns it (a context is single-stream and not thread-safe).
@@ -77,7 +81,7 @@ struct ArgentServe {
   std::map<std::tuple<uint32_t, uint32_t, uint32_t>, std::vector<ArgentFilm*>> pool;
   uint64_t pool_bytes = 0;
   std::chrono::steady_clock::time_point t0;
-  uint64_t steps = 0, path_samples = 0;
+  uint64_t steps = 0, path_samples = 0, rejected = 0;
   // Batches in flight, oldest first: completion event and (ticket, samples).
   struct Batch {
     cudaEvent_t done;
@@ -236,6 +240,17 @@ int argent_serve_submit(ArgentServe* s, const ArgentServeRequest* req, uint64_t*
   uint64_t fb = film_bytes(req->width, req->height, req->film_flags);
   if (fb > s->cfg.film_budget) return ARGENT_E_BUSY;
   std::lock_guard<std::mutex> g(s->mu);
+  if (s->cfg.max_pending) {
+    // A bounded queue, as argent's (queue.rs:364-366): refuse rather than
+    // let the wait of every admitted request grow without bound.
+    uint32_t n = 0;
+    for (auto& kv : s->reqs)
+      if (kv.second.state == ARGENT_REQ_QUEUED || kv.second.state == ARGENT_REQ_ACTIVE) ++n;
+    if (n >= s->cfg.max_pending) {
+      ++s->rejected;
+      return ARGENT_E_BUSY;
+    }
+  }
   Request q;
   std::memset(&q, 0, sizeof(q));
   q.ticket = s->next_ticket++;

@@ -165,6 +165,9 @@ struct ArgentCtx {
   bool graphs_on = true;
   int num_sms = 148;
   int lanes = 8;
+  // Launch tuning (argent_ctx_set_tuning / argent_autotune); 0 = default.
+  int trace_bpsm = 0;
+  int shade_bpsm[5] = {0, 0, 0, 0, 0};
   bool counting = false;  // traversal instrumentation on (argent_ctx_set_counting)
   ArgentLimits limits{};
   std::string err;
@@ -187,6 +190,7 @@ struct ArgentPiece {
   uint64_t bytes = 0;
   uint32_t nv = 0, nt = 0, depth = 0, max_material = 0;
   float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  int tri_test = 0;  // ARGENT_TRI_MOLLER_TRUMBORE or ARGENT_TRI_WATERTIGHT
 };
 
 struct ArgentScene {

@@ -409,11 +409,41 @@ __device__ __forceinline__ uint32_t lane_refill(bool idle, bool* first, bool* mo
 // kernel of its hit's material class.  Persistent lanes step their BVH
 // traversals one node or leaf at a time and take a new path as soon as
 // theirs is done.
+// Rows of the traversal kernels' shared-memory stack rings (ShortStack);
+// 0 keeps the whole stack in local memory.  The kernels run 128 threads per
+// block.
+#ifndef ARGENT_SHORT_STACK
+#define ARGENT_SHORT_STACK 16
+#endif
+#ifndef ARGENT_SHORT_STACK_ANY
+#define ARGENT_SHORT_STACK_ANY 16
+#endif
+#if ARGENT_SHORT_STACK > 0
+#define ARGENT_CLOSEST_STACK(name)                                             \
+  __shared__ uint2 name##_ring[ARGENT_SHORT_STACK * 128];                      \
+  uint2 name##_spill[ARGENT_STACK_SIZE];                                       \
+  ShortStack<uint2, ARGENT_SHORT_STACK, 128> name{name##_ring + threadIdx.x, name##_spill}
+#else
+#define ARGENT_CLOSEST_STACK(name)   \
+  uint2 name##_arr[ARGENT_STACK_SIZE]; \
+  LocalStack<uint2> name { name##_arr }
+#endif
+#if ARGENT_SHORT_STACK_ANY > 0
+#define ARGENT_ANY_STACK(name)                                                     \
+  __shared__ uint32_t name##_ring[ARGENT_SHORT_STACK_ANY * 128];                   \
+  uint32_t name##_spill[ARGENT_STACK_SIZE];                                        \
+  ShortStack<uint32_t, ARGENT_SHORT_STACK_ANY, 128> name{name##_ring + threadIdx.x, name##_spill}
+#else
+#define ARGENT_ANY_STACK(name)          \
+  uint32_t name##_arr[ARGENT_STACK_SIZE]; \
+  LocalStack<uint32_t> name { name##_arr }
+#endif
+
 template <bool U>
 __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_intersect(WaveArgs a, int depth) {
   const uint32_t count = a.counters[CNT_ACT(depth)];
   uint32_t* work = a.counters + CNT_WORK(CNT_ACT(depth));
-  uint2 stack[ARGENT_STACK_SIZE];
+  ARGENT_CLOSEST_STACK(stack);
   ClosestTrav s;
   const DevScene* sc = U ? a.uscene : nullptr;
   uint32_t slot = 0;
@@ -913,7 +943,7 @@ template <bool U>
 __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_shadow(WaveArgs a, int depth) {
   const uint32_t count = a.counters[CNT_SH(depth)];
   uint32_t* work = a.counters + CNT_WORK(CNT_SH(depth));
-  uint32_t stack[ARGENT_STACK_SIZE];
+  ARGENT_ANY_STACK(stack);
   AnyTrav s;
   const DevScene* sc = nullptr;
   uint32_t idx = 0;

@@ -75,6 +75,23 @@ class Context:
         self.check(self.lib.argent_ctx_config(self.h, ctypes.byref(lanes), ctypes.byref(wave)))
         return lanes.value, wave.value
 
+    def tuning(self):
+        """The launch tuning in use, as a dict (argent_ctx_tuning)."""
+        t = N.ArgentTuning()
+        self.check(self.lib.argent_ctx_tuning(self.h, ctypes.byref(t)))
+        return {"lanes": t.lanes, "wave_paths": t.wave_paths, "trace_blocks_per_sm": t.trace_blocks_per_sm,
+                "shade_blocks_per_sm": list(t.shade_blocks_per_sm)}
+
+    def set_tuning(self, tuning):
+        """argent_ctx_set_tuning from a dict as `tuning()` returns it."""
+        t = N.ArgentTuning()
+        t.lanes = int(tuning["lanes"])
+        t.wave_paths = int(tuning["wave_paths"])
+        t.trace_blocks_per_sm = int(tuning.get("trace_blocks_per_sm", 0))
+        for i, v in enumerate(tuning.get("shade_blocks_per_sm", [0] * 5)):
+            t.shade_blocks_per_sm[i] = int(v)
+        self.check(self.lib.argent_ctx_set_tuning(self.h, ctypes.byref(t)))
+
     def set_config(self, lanes, wave_paths):
         """argent_ctx_set_config: lanes and wave size of the next calls."""
         self.check(self.lib.argent_ctx_set_config(self.h, int(lanes), int(wave_paths)))
@@ -167,6 +184,11 @@ class Piece:
             self.ctx.h, self.h, _p(m.positions, fp), _p(m.normals, fp), len(m.positions), _p(m.tris, N.c_u32_p),
             len(m.tris), ctypes.byref(s), _p(out, fp)))
         return out
+
+    def set_triangle_test(self, test):
+        """argent_piece_set_triangle_test: N.TRI_MOLLER_TRUMBORE (argent's,
+        bit-exact hits; the default) or N.TRI_WATERTIGHT."""
+        self.ctx.check(self.ctx.lib.argent_piece_set_triangle_test(self.ctx.h, self.h, int(test)))
 
     def trace_closest(self, rays: np.ndarray) -> np.ndarray:
         """rays: (n, 8) float32 [ox oy oz tmax dx dy dz pad] -> hits (n, 4)
@@ -293,10 +315,10 @@ class Serve:
     the thread that owns the context."""
 
     def __init__(self, ctx: Context, film_budget=0, max_active=0, step_path_samples=0, aging_ms=0,
-                 step_path_samples_max=0, overlap=False):
+                 step_path_samples_max=0, overlap=False, max_pending=0):
         self.ctx = ctx
         cfg = N.ArgentServeConfig(int(film_budget), int(max_active), int(aging_ms), int(step_path_samples),
-                                  int(step_path_samples_max), 1 if overlap else 0, 0)
+                                  int(step_path_samples_max), 1 if overlap else 0, int(max_pending))
         h = ctypes.c_void_p()
         ctx.check(ctx.lib.argent_serve_create(ctx.h, ctypes.byref(cfg), ctypes.byref(h)))
         self.h = h
@@ -311,6 +333,8 @@ class Serve:
         self.close()
 
     def submit(self, scene: Scene, cam, settings, width, height, spp, seed=7, priority=0, flags=N.FILM_KAHAN):
+        """A ticket, or N.ArgentError with code E_BUSY when the serve is at
+        its max_pending bound (or the film cannot fit its budget)."""
         r = N.ArgentServeRequest()
         r.scene = scene.h
         r.camera = cam

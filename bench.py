@@ -774,6 +774,7 @@ def run_serve(args, world, rank, device):
     arrival); latency = completion - submission per request class."""
     import torch
 
+    from argent_b200 import _native as N
     from argent_b200 import workloads as W
     from argent_b200.gpu import Context, Piece, Scene, Serve
 
@@ -793,7 +794,7 @@ def run_serve(args, world, rank, device):
     trace = W.serve_trace(rate, args.serve_seconds)
     srv = Serve(ctx, film_budget=32 << 30, max_active=64, step_path_samples=args.serve_step,
                 step_path_samples_max=args.serve_step_max, aging_ms=args.serve_aging_ms,
-                overlap=not args.serve_no_overlap)
+                overlap=not args.serve_no_overlap, max_pending=args.serve_max_pending)
 
     def submit(cname, i, j):
         _, w, h, spp, prio = W.SERVE_CLASSES[cname]
@@ -812,12 +813,20 @@ def run_serve(args, world, rank, device):
     done = threading.Event()
     t_origin = srv.now()
 
+    rejected = {c: 0 for c in W.SERVE_CLASSES}
+
     def driver():
         for (ta, cname, i, j) in trace:
             dt = t_origin + ta - srv.now()
             if dt > 0:
                 time.sleep(dt)
-            t = submit(cname, i, j)
+            try:
+                t = submit(cname, i, j)
+            except N.ArgentError as e:
+                if e.code != N.E_BUSY:
+                    raise
+                rejected[cname] += 1
+                continue
             reqs[t] = (i, j)
             tickets[t] = cname
         done.set()
@@ -864,12 +873,14 @@ def run_serve(args, world, rank, device):
     # The same stream through argent's own discipline (one job at a time).
     plain = None
     if not args.no_plain:
-        pv, plat = serve_plain(ctx, trace, scenes, cams, ps)
+        pv, plat, prej = serve_plain(ctx, trace, scenes, cams, ps, args.serve_max_pending)
         plain = {"value": pv, "unit": "path-samples/s",
                  "latency_s": {c: {"n": len(v), "p50": pct(v, 50), "p99": pct(v, 99), "max": max(v) if v else None}
                                for c, v in list(plat.items()) + [("all", sum(plat.values(), []))]},
+                 "rejected": prej,
                  "discipline": "one job at a time in arrival order, render_pass in chunks of 2..64 spp sized to "
-                               "about 1.5 s (serve/queue.rs:599-617), film read to host"}
+                               "about 1.5 s (serve/queue.rs:599-617), film read to host; a job arriving while "
+                               f"{max(args.serve_max_pending - 1, 0)} wait is refused (queue.rs:364-366)"}
 
     # Error of each class's first served film against the FP64 oracle (an
     # FP64-accumulated 65,536-spp render of ORACLE_ROWS rows at mid-frame
@@ -877,7 +888,6 @@ def run_serve(args, world, rank, device):
     # so the channels are camera RGB.
     acc = {}
     if not args.no_oracle:
-        from argent_b200 import _native as N
         from argent_b200.gpu import Film, render_pass
 
         for cname, ((i, j), c) in kept.items():
@@ -904,11 +914,13 @@ def run_serve(args, world, rank, device):
                        "offered_path_samples_per_s": offered, "step_path_samples": args.serve_step,
                        "step_path_samples_max": args.serve_step_max or 2 * args.serve_step,
                        "aging_ms": args.serve_aging_ms or 250, "overlap": not args.serve_no_overlap,
+                       "max_pending": args.serve_max_pending,
                        "parallelism": f"replicas{world}",
                        "timing": "wall clock of the serve loop (latency is a wall-clock quantity); each step "
                                  "synchronises its batch"},
             "latency_s": {c: {"n": len(v), "p50": pct(v, 50), "p99": pct(v, 99), "max": max(v) if v else None}
                           for c, v in list(lat.items()) + [("all", sum(lat.values(), []))]},
+            "rejected": rejected,
             "clocks": ck,
             "e2e": {"value": value, "unit": "path-samples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": d2h / max(1, len(finished)), "note": "per request: films read to host"},
@@ -921,13 +933,14 @@ def run_serve(args, world, rank, device):
         print(json.dumps(out), flush=True)
 
 
-def serve_plain(ctx, trace, scenes, cams, ps):
+def serve_plain(ctx, trace, scenes, cams, ps, max_pending=0):
     """argent's own serve discipline on the GPU, for comparison with the
     continuous-batching scheduler on the same request stream: one job at a
     time in arrival order, each rendered by render_pass in chunks that start
     at 2 spp and adapt to about 1.5 s each (capped at 64 spp), then read to
-    host memory (serve/queue.rs:599-617).  Returns (path-samples/s,
-    {class: latencies})."""
+    host memory (serve/queue.rs:599-617); with max_pending, a job that
+    arrives while max_pending - 1 wait is refused (queue.rs:364-366).
+    Returns (path-samples/s, {class: latencies}, {class: refused})."""
     import queue
 
     from argent_b200 import workloads as W
@@ -935,12 +948,16 @@ def serve_plain(ctx, trace, scenes, cams, ps):
 
     q = queue.Queue()
     t0 = time.perf_counter()
+    rejected = {c: 0 for c in W.SERVE_CLASSES}
 
     def driver():
         for (ta, cname, i, j) in trace:
             dt = t0 + ta - time.perf_counter()
             if dt > 0:
                 time.sleep(dt)
+            if max_pending and q.qsize() >= max_pending - 1:
+                rejected[cname] += 1
+                continue
             q.put((time.perf_counter(), cname, i, j))
         q.put(None)
 
@@ -975,7 +992,7 @@ def serve_plain(ctx, trace, scenes, cams, ps):
     th.join()
     for f in films.values():
         f.close()
-    return served / (t_last - t0), lat
+    return served / (t_last - t0), lat, rejected
 
 
 PATH_STATE_BYTES = 244  # per path slot per lane
@@ -1009,6 +1026,8 @@ def main():
     ap.add_argument("--serve-step-max", type=int, default=0, help="serve_trace: most path-samples per step")
     ap.add_argument("--serve-aging-ms", type=int, default=0, help="serve_trace: aging period (0 = default)")
     ap.add_argument("--serve-no-overlap", action="store_true", help="serve_trace: wait for each step's batch")
+    ap.add_argument("--serve-max-pending", type=int, default=25,
+                    help="serve_trace: requests waiting or rendering at most, both forms (argent: 24 waiting + 1)")
     args = ap.parse_args()
     if args.impl == "reference":
         # CPU only: rank 0 measures, the other ranks have nothing to do.

@@ -252,6 +252,18 @@ void argent_piece_destroy(ArgentPiece* piece);
 int argent_piece_upload_device_bvh(ArgentCtx* ctx, const float* positions, uint32_t nv, const float* normals,
                                    const uint32_t* tris, uint32_t nt, const uint16_t* tri_material,
                                    const float* cavity, ArgentPiece** out);
+/*
+ * The ray-triangle test of a piece's traversals.  ARGENT_TRI_MOLLER_TRUMBORE
+ * (the default) is argent's `tri_intersect` (bvh.rs:391-410) in argent's
+ * operation order, which gives bit-exact closest hits.  ARGENT_TRI_WATERTIGHT
+ * is Woop, Benthin and Wald's watertight test (JCGT 2013): no ray passes
+ * between two triangles that share an edge, at the price of hits that can
+ * differ from argent's at edges and in the last bits of t.  Rewrites the
+ * piece's triangle records on the device after the context's work is done;
+ * scenes built on the piece use the new test from their next render.
+ */
+enum { ARGENT_TRI_MOLLER_TRUMBORE = 0, ARGENT_TRI_WATERTIGHT = 1 };
+int argent_piece_set_triangle_test(ArgentCtx* ctx, ArgentPiece* piece, int test);
 /* Root bounds, as `Piece::bounds` (scene.rs:34-37). */
 int argent_piece_bounds(const ArgentPiece* piece, float lo[3], float hi[3]);
 /* Bytes the piece holds on the device. */
@@ -371,14 +383,37 @@ typedef struct ArgentTuneResult {
 /*
  * Times `count` samples of the given frame (after one warm-up pass) for each
  * lane count in {2, 4, 8, 12, 16} and wave size in {2^21 .. 2^25} whose path
- * state fits in half of the free device memory, keeps the fastest as the
- * context's configuration, and frees the path state of unused lanes.
- * results (may be NULL when max_results is 0) receives up to max_results
- * measurements; *n_results the number taken.  Renders into a scratch film.
+ * state fits in half of the free device memory and keeps the fastest; then,
+ * at that lane count and wave size, searches one knob at a time: blocks per
+ * SM of each shading class the scene uses ({2, 3, 4, 5, 6, 8}) and of the
+ * traversals ({4, 6, 8}), keeping a value only when it is faster.  The best
+ * tuning becomes the context's (argent_ctx_tuning reads it) and the path
+ * state of unused lanes is freed.  results (may be NULL when max_results is
+ * 0) receives up to max_results lane/wave measurements; *n_results the
+ * number taken.  Renders into a scratch film.
  */
 int argent_autotune(ArgentCtx* ctx, ArgentScene* scene, const ArgentCamera* camera,
                     const ArgentPathSettings* settings, uint32_t width, uint32_t height, uint32_t count,
                     ArgentTuneResult* results, uint32_t max_results, uint32_t* n_results);
+/*
+ * Launch configuration of a context's renders: what argent_autotune
+ * searches.  Grid sizes change only how work is spread over the SMs, never
+ * a film (every kernel takes its work from a queue counter, and film sums
+ * are added in wave order).
+ */
+typedef struct ArgentTuning {
+  uint32_t lanes;                  /* concurrent waves, 1..16 */
+  uint32_t trace_blocks_per_sm;    /* blocks of 128 per SM launched for the closest-hit and shadow
+                                      traversals; 0 = as many as are resident */
+  uint64_t wave_paths;             /* path slots per wave, 2^16..2^30 */
+  uint32_t shade_blocks_per_sm[5]; /* per material class (misses and panels, metal, coated,
+                                      dielectric, other); 0 = the built-in default */
+  uint32_t reserved;
+} ArgentTuning;
+int argent_ctx_tuning(const ArgentCtx* ctx, ArgentTuning* out);
+/* Applies a tuning (e.g. one argent_autotune found for the same kind of
+ * render earlier); waits for the context stream first. */
+int argent_ctx_set_tuning(ArgentCtx* ctx, const ArgentTuning* tuning);
 /* The context's current lanes and wave size. */
 int argent_ctx_config(const ArgentCtx* ctx, uint32_t* lanes, uint64_t* wave_paths);
 /*
@@ -531,7 +566,9 @@ typedef struct ArgentServeConfig {
   uint64_t step_path_samples_max; /* a step takes a quarter of the pending work, up to this;
                                      0 = 2 x step_path_samples */
   uint32_t overlap;           /* 1 = keep the next batch in flight while one runs */
-  uint32_t reserved;
+  uint32_t max_pending;       /* requests queued or active at most: a submit beyond it returns
+                                 ARGENT_E_BUSY (argent refuses a job when 24 wait, queue.rs:28,364);
+                                 0 = no bound */
 } ArgentServeConfig;
 
 typedef struct ArgentServeRequest {

@@ -189,3 +189,18 @@ def test_sobol_nets():
         cx = np.floor(pts[:, 0] * (1 << a)).astype(int)
         cy = np.floor(pts[:, 1] * (1 << b)).astype(int)
         assert len(np.unique(cx * (1 << b) + cy)) == n, (a, b)
+
+
+def test_tuning_size_class_keys():
+    """The tuning cache key buckets triangles and path-samples by powers of
+    two and names the scene's material kinds and env-map flag (CPU)."""
+    from types import SimpleNamespace
+
+    from argent_b200 import tuning as T
+    from argent_b200 import workloads as W
+
+    wl = W.ring_still()
+    scene = SimpleNamespace(piece=SimpleNamespace(mesh=wl.mesh), desc=wl.desc)
+    k = T.size_class(scene, 256, 256, 16)
+    assert k.startswith("t16_p20_") and k.endswith("_e0")
+    assert T.size_class(scene, 1920, 1080, 256) != k

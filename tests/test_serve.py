@@ -153,3 +153,25 @@ def test_submission_refuses_foreign_scenes_and_deep_paths(ring_setup):
     assert srv.poll(t).state == N.REQ_DONE
     srv.release(t)
     srv.close()
+
+
+def test_bounded_queue_refuses_beyond_max_pending(ring_setup):
+    """With max_pending = 3, a fourth request waiting or rendering is
+    refused with E_BUSY (argent's queue refuses a job once 24 wait,
+    queue.rs:364-366); once one finishes, a new submit is accepted."""
+    from argent_b200.gpu import Serve
+
+    ctx, _, scenes, wl = ring_setup
+    srv = Serve(ctx, max_pending=3)
+    cam = _cam(wl, 32, 32)
+    tickets = [srv.submit(scenes["sterling"], cam, W.settings(8), 32, 32, 2, 7, 0) for _ in range(3)]
+    with pytest.raises(N.ArgentError) as e:
+        srv.submit(scenes["sterling"], cam, W.settings(8), 32, 32, 2, 7, 0)
+    assert e.value.code == N.E_BUSY
+    srv.run()
+    for t in tickets:
+        assert srv.poll(t).state == N.REQ_DONE
+        srv.read(t)
+    t = srv.submit(scenes["gold14k"], cam, W.settings(8), 32, 32, 2, 7, 0)
+    srv.run()
+    assert srv.poll(t).state == N.REQ_DONE
