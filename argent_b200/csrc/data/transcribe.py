@@ -12,7 +12,7 @@ This script parses the numeric literals of those files and writes
 argent sources; the generated header is committed, so nothing at build or run
 time needs the argent tree.
 
-Usage:  python argent_b200/csrc/data/transcribe.py /root/reference
+Usage:  python argent_b200/csrc/data/transcribe.py <argent checkout>
 """
 
 import os
@@ -114,4 +114,6 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: transcribe.py <argent checkout (the directory holding crates/)>")
+    main(sys.argv[1])

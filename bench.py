@@ -662,6 +662,11 @@ def run_gpu(args, world, rank, device):
     if plan.renders > 1 and args.steps > 0:
         from argent_b200.gpu import render_pass
 
+        # (a) device time of the same renders issued one render_pass each;
+        # (b) end to end as argent's render_reel loop runs them
+        # (jobs.rs:689-707): each frame's render_image returns its image
+        # before the next frame starts, so every render is followed by its
+        # film read to host memory.  (b) is compared with the batch's e2e.
         barrier(world, device)
         ctx.sync()
         p0 = torch.cuda.Event(enable_timing=True)
@@ -674,9 +679,26 @@ def run_gpu(args, world, rank, device):
         p1.record(stream)
         p1.synchronize()
         pms = max_over_ranks(p0.elapsed_time(p1), world, device)
+        fp = ctypes.POINTER(ctypes.c_float)
+        rbuf = [tuple(np.zeros((f.height, f.width, 3), np.float32) for _ in range(3)) for f in plan.films]
+        steps_e2e = max(args.e2e_steps, 1)
+        barrier(world, device)
+        ctx.sync()
+        t0 = time.perf_counter()
+        for i in range(steps_e2e):
+            for it, (c, a, nrm) in zip(plan.items(i), rbuf):
+                it[2].clear()
+                render_pass(ctx, *it)
+                ctx.check(ctx.lib.argent_film_read(it[2].h, c.ctypes.data_as(fp), a.ctypes.data_as(fp),
+                                                   nrm.ctypes.data_as(fp)))
+        pe = max_over_ranks(time.perf_counter() - t0, world, device)
         plain = {"value": world * samples_per_step * args.steps / (pms / 1000.0), "unit": "path-samples/s",
                  "ms_per_step": pms / args.steps,
-                 "form": f"the same {plan.renders} renders per step, one render_pass each"}
+                 "e2e": {"value": world * samples_per_step * steps_e2e / pe, "unit": "path-samples/s",
+                         "ms_per_step": 1e3 * pe / steps_e2e,
+                         "form": "render_reel's loop: each render's render_pass, then its film read to host, "
+                                 "before the next render"},
+                 "form": f"the same {plan.renders} renders per step, one render_pass each (device time)"}
 
     # End-to-end through the C ABI with host buffers.
     e2e_value, e2e_split = None, None
