@@ -308,10 +308,12 @@ _host = None
 
 
 def gpu():
-    """The CUDA library (raises if it is not built)."""
+    """The CUDA library (raises if it is not built).  ARGENT_GPU_LIB names
+    another build of it to load instead, e.g. one compiled with other
+    build-time launch constants (`python -m argent_b200.build --variant`)."""
     global _gpu
     if _gpu is None:
-        _gpu = _bind(GPU_SO, GPU_FUNCS)
+        _gpu = _bind(os.environ.get("ARGENT_GPU_LIB") or GPU_SO, GPU_FUNCS)
     return _gpu
 
 

@@ -9,6 +9,7 @@ every multiply and add separately, and the closest-hit parity gate compares
 ray/triangle distances bit for bit.
 
 Usage: python -m argent_b200.build [--force]
+       python -m argent_b200.build --variant OUT.so NAME=VALUE ...   (a CUDA library with other constants)
 """
 
 import os
@@ -62,18 +63,22 @@ def _host_cxx():
     return "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 
-def build_gpu(force=False, verbose=False):
-    os.makedirs(LIB, exist_ok=True)
-    if not force and not _stale(GPU_SO, _deps()):
-        return GPU_SO
+def build_gpu(force=False, verbose=False, out=None, defines=()):
+    """The CUDA library; `out` and `defines` (e.g. ["ARGENT_SHORT_STACK=8"])
+    build a variant with other build-time constants at another path, which
+    ARGENT_GPU_LIB then selects."""
+    out = out or GPU_SO
+    os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
+    if not force and not defines and not _stale(out, _deps()):
+        return out
     cmd = ["nvcc", *ARCH, "-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-ccbin", _host_cxx(),
-           "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-shared", "-o", GPU_SO + ".tmp",
-           *GPU_SOURCES, "-lcudart"]
+           "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-shared", "-o", out + ".tmp",
+           *[f"-D{d}" for d in defines], *GPU_SOURCES, "-lcudart"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     subprocess.run(cmd, check=True)
-    os.replace(GPU_SO + ".tmp", GPU_SO)
-    return GPU_SO
+    os.replace(out + ".tmp", out)
+    return out
 
 
 def build_host(force=False):
@@ -108,4 +113,9 @@ def build_all(force=False, verbose=False):
 
 
 if __name__ == "__main__":
-    build_all(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    if "--variant" in sys.argv:
+        # python -m argent_b200.build --variant OUT.so NAME=VALUE ...
+        i = sys.argv.index("--variant")
+        build_gpu(force=True, out=sys.argv[i + 1], defines=sys.argv[i + 2:])
+    else:
+        build_all(force="--force" in sys.argv, verbose="-v" in sys.argv)

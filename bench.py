@@ -351,12 +351,17 @@ def run_reference(args, world, rank):
 class StillPlan:
     """One still per step: film cleared, one render_pass."""
 
-    def __init__(self, ctx, name):
+    def __init__(self, ctx, name, tri_test="mt"):
         from argent_b200.gpu import Film, Piece, Scene
 
         self.mesh = build_mesh(name)
         self.piece = Piece(ctx, self.mesh)
         self.wl = build_workload(name, self.mesh, self.piece)
+        self.tri_test = tri_test
+        if tri_test == "watertight":
+            from argent_b200 import _native as N
+
+            self.piece.set_triangle_test(N.TRI_WATERTIGHT)
         self.scene = Scene(ctx, self.piece, self.wl.desc)
         self.films = [Film(ctx, self.wl.width, self.wl.height)]
         self.cpu_wl = self.wl
@@ -382,8 +387,11 @@ class StillPlan:
 
     def config(self):
         wl = self.wl
-        return {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp,
-                "triangles": self.triangles, "max_depth": int(wl.settings.max_depth)}
+        out = {"workload": wl.name, "width": wl.width, "height": wl.height, "spp": wl.spp,
+               "triangles": self.triangles, "max_depth": int(wl.settings.max_depth)}
+        if self.tri_test != "mt":
+            out["triangle_test"] = self.tri_test
+        return out
 
     def accuracy_target(self, ctx):
         """(workload, scene, film holding its render at the workload's spp)."""
@@ -552,7 +560,7 @@ def run_gpu(args, world, rank, device):
 
     torch.cuda.set_device(device)
     ctx = Context(device, wave_paths=args.wave_paths or STILL_WAVE_PATHS, lanes=args.lanes)
-    plan = ReelPlan(ctx) if args.workload == "reel_batch" else StillPlan(ctx, args.workload)
+    plan = ReelPlan(ctx) if args.workload == "reel_batch" else StillPlan(ctx, args.workload, args.tri_test)
     if args.spp:
         plan.set_spp(args.spp)  # profiling runs only: the bench line uses the workload's spp
     stream = torch.cuda.ExternalStream(ctx.stream)
@@ -1039,6 +1047,8 @@ def main():
     ap.add_argument("--no-oracle", action="store_true", help="skip the FP64 65,536-spp error measurement")
     ap.add_argument("--no-plain", action="store_true", help="serve_trace: skip the one-job-at-a-time comparison")
     ap.add_argument("--spp", type=int, default=0, help="override spp (short profiling runs)")
+    ap.add_argument("--tri-test", default="mt", choices=["mt", "watertight"],
+                    help="stills: argent's Moller-Trumbore (default, bit-exact) or the watertight test")
     ap.add_argument("--lanes", type=int, default=0, help="concurrent waves (0 = the library default)")
     ap.add_argument("--wave-paths", type=int, default=0,
                     help="path slots per wave (0 = 2^25 for stills and batches, 2^23 for the serve trace)")

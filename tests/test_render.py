@@ -369,3 +369,23 @@ def test_graph_keys_keep_map_and_gradient_waves_apart():
             for got, ref in zip(render(b), w):
                 assert np.array_equal(got, ref)
     assert not np.array_equal(want[0][0], want[1][0])
+
+
+@pytest.mark.gpu
+def test_fp64_oracle_film_matches_cpu_restatement_at_c1():
+    """The FP64 oracle the benchmark scores renders against runs on the
+    device; cross-check it against argent's algorithm on the host: the small
+    plain workload at full size (256 x 256, depth 8) at 256 spp through an
+    FP64 film, against the CPU restatement's FP64 sums of the same sample
+    streams.  Both accumulate in double, so what is left is the
+    transcendental functions' last bits flipping a rare path."""
+    import oracle as O
+    from argent_b200 import _native as N
+
+    wl = W.ring_still()
+    xyz_gpu, _, _ = _gpu_render(wl, 256, flags=N.FILM_FP64)
+    sc = O.Scene(wl.mesh, wl.desc.c)
+    _, _, _, xyz = sc.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, 256, wl.seed)
+    e = rel_rmse(xyz_gpu, xyz / 256)
+    print("FP64 film, ring 256x256x256 relRMSE XYZ vs CPU restatement:", e)
+    assert np.all(e <= 2e-3), e
