@@ -19,10 +19,12 @@
 //
 // Chunks: the step's budget of path-samples grows with the work pending
 // (a quarter of it, between step_path_samples and step_path_samples_max), so a
-// deep queue runs in larger, more efficient batches.  Active requests take
-// chunks in urgency order; a request whose remaining work is under a
-// sixteenth of the budget finishes in this step, and every active request
-// advances by at least one sample, so none starves.
+// deep queue runs in larger, more efficient batches.  Requests whose
+// remaining work is under a sixteenth of the budget finish in this step (up
+// to half the budget); the rest goes to the other active requests strictly
+// in urgency order, so large requests render one or two at a time at the
+// device's full rate, near first come first served, instead of all sharing
+// it.  Aging keeps any request from waiting for ever.
 //
 // Bound: with max_pending set, a submit that finds that many requests
 // queued or active is refused with ARGENT_E_BUSY (argent's queue refuses a
@@ -338,13 +340,44 @@ int argent_serve_step(ArgentServe* s, uint32_t* pending) {
         pending_work += remaining(&kv.second);
     const uint64_t budget =
         std::min(s->cfg.step_path_samples_max, std::max(s->cfg.step_path_samples, pending_work / 4));
+    // Small requests (at most a sixteenth of the budget left) finish in
+    // this step, in urgency order, up to half the budget; the rest of the
+    // budget goes to the other requests strictly in urgency order, so the
+    // most urgent large request renders at the device's full rate instead
+    // of sharing it with every other one (which would make each large
+    // request wait for all of them).  A request reached with no budget left
+    // waits for a later step; its urgency grows while it waits.
+    std::vector<std::pair<Request*, uint32_t>> take;
     uint64_t left = budget;
+    const uint64_t small_cap = budget / 2;
+    uint64_t small_used = 0;
     for (Request* q : active) {
       if (q->cancel || q->scheduled >= q->req.spp) continue;
+      uint64_t r = remaining(q);
+      if (r <= budget / 16 && small_used + r <= small_cap) {
+        take.emplace_back(q, q->req.spp - q->scheduled);
+        small_used += r;
+      }
+    }
+    left -= small_used;
+    for (Request* q : active) {
+      if (q->cancel || q->scheduled >= q->req.spp) continue;
+      bool taken = false;
+      for (auto& t : take) taken = taken || t.first == q;
+      if (taken) continue;
       uint64_t px = (uint64_t)q->req.width * q->req.height;
       uint64_t want = q->req.spp - q->scheduled;
-      uint64_t n = remaining(q) <= budget / 16 ? want : std::min<uint64_t>(want, left / px);
-      if (n == 0) n = 1;
+      uint64_t n = std::min<uint64_t>(want, left / px);
+      // A request larger than the whole budget still advances when it is
+      // the first one this step reaches.
+      if (n == 0 && take.empty()) n = 1;
+      if (n == 0) continue;
+      take.emplace_back(q, (uint32_t)n);
+      left = n * px >= left ? 0 : left - n * px;
+    }
+    for (auto& t : take) {
+      Request* q = t.first;
+      uint64_t n = t.second;
       ArgentBatchItem it;
       std::memset(&it, 0, sizeof(it));
       it.scene = q->req.scene;
@@ -356,7 +389,6 @@ int argent_serve_step(ArgentServe* s, uint32_t* pending) {
       items.push_back(it);
       in_batch.push_back(q);
       chunk.push_back((uint32_t)n);
-      left = n * px >= left ? 0 : left - n * px;
     }
   }
   if (!items.empty()) {

@@ -27,9 +27,28 @@ class Context:
         h = ctypes.c_void_p()
         N.check(self.lib.argent_ctx_create(device, ctypes.byref(lim), ctypes.byref(h)))
         self.h = h
+        # Native objects made on this context (handle -> kind).  The context
+        # destroys those still alive before itself: the garbage collector
+        # finalises a reference cycle in any order, and a piece, scene, film
+        # or serve must never outlive the context it was made on.
+        self._owned = {}
+
+    def _own(self, kind, h):
+        self._owned[h.value] = kind
+
+    def _release(self, kind, h):
+        """Destroys a child's native object unless the context already has."""
+        if getattr(self, "h", None) is not None and self._owned.pop(h.value, None) is not None:
+            getattr(self.lib, f"argent_{kind}_destroy")(h)
 
     def close(self):
         if getattr(self, "h", None):
+            owned = getattr(self, "_owned", {})
+            for kind in ("serve", "film", "scene", "piece"):  # dependents first
+                for hv, k in list(owned.items()):
+                    if k == kind:
+                        del owned[hv]
+                        getattr(self.lib, f"argent_{kind}_destroy")(ctypes.c_void_p(hv))
             self.lib.argent_ctx_destroy(self.h)
             self.h = None
 
@@ -143,10 +162,11 @@ class Piece:
             ctx.h, _p(mesh.positions, fp), len(mesh.positions), _p(mesh.normals, fp), _p(mesh.tris, N.c_u32_p),
             len(mesh.tris), _p(mesh.tri_material, N.c_u16_p), _p(mesh.cavity, fp), ctypes.byref(h)))
         self.h = h
+        ctx._own("piece", h)
 
     def close(self):
         if getattr(self, "h", None):
-            self.ctx.lib.argent_piece_destroy(self.h)
+            self.ctx._release("piece", self.h)
             self.h = None
 
     def __del__(self):
@@ -215,10 +235,11 @@ class Scene:
         h = ctypes.c_void_p()
         ctx.check(ctx.lib.argent_scene_upload(ctx.h, piece.h, ctypes.byref(desc.c), ctypes.byref(h)))
         self.h = h
+        ctx._own("scene", h)
 
     def close(self):
         if getattr(self, "h", None):
-            self.ctx.lib.argent_scene_destroy(self.h)
+            self.ctx._release("scene", self.h)
             self.h = None
 
     def __del__(self):
@@ -237,10 +258,11 @@ class Film:
         h = ctypes.c_void_p()
         ctx.check(ctx.lib.argent_film_create(ctx.h, width, height, flags, ctypes.byref(h)))
         self.h = h
+        ctx._own("film", h)
 
     def close(self):
         if getattr(self, "h", None):
-            self.ctx.lib.argent_film_destroy(self.h)
+            self.ctx._release("film", self.h)
             self.h = None
 
     def __del__(self):
@@ -322,11 +344,12 @@ class Serve:
         h = ctypes.c_void_p()
         ctx.check(ctx.lib.argent_serve_create(ctx.h, ctypes.byref(cfg), ctypes.byref(h)))
         self.h = h
+        ctx._own("serve", h)
         self._scenes = {}  # ticket -> scene, kept alive while the request is
 
     def close(self):
         if getattr(self, "h", None):
-            self.ctx.lib.argent_serve_destroy(self.h)
+            self.ctx._release("serve", self.h)
             self.h = None
 
     def __del__(self):

@@ -397,6 +397,9 @@ class StillPlan:
         """(workload, scene, film holding its render at the workload's spp)."""
         return self.wl, self.scene, self.films[0]
 
+    def tuning_target(self):
+        return self.wl, self.scene, self.films[0]
+
 
 class ReelPlan:
     """The batched workload: step k renders turntable frame k (mod 36) of
@@ -451,6 +454,11 @@ class ReelPlan:
                 "env": "2048x1024 synthetic HDRI + noir panels (env_pick 0.5)",
                 "subset": f"each step is one turntable frame of all {self.renders} piece x alloy renders; "
                           f"steps walk the {self.W.REEL_FRAMES} frames"}
+
+    def tuning_target(self):
+        """The 1.1M-triangle render: the batch's middle piece."""
+        i = self.wls.index(self.cpu_wl)
+        return self.wls[i], self.scenes[i], self.films[i]
 
     def accuracy_target(self, ctx):
         """The 1.1M-triangle render of turntable frame 0, rendered afresh."""
@@ -552,6 +560,31 @@ def accuracy(ctx, plan, cpu_scene, threads, gpu_rate=None, cpu_rate=None):
     return out
 
 
+def tune_wanted(args):
+    """Launch tuning (argent_autotune, cached per size class by
+    argent_b200.tuning): on by default for the batched and served workloads,
+    whose contexts run many kinds of render; --tune / --no-tune override."""
+    if args.no_tune:
+        return False
+    return args.tune or args.workload in ("reel_batch", "serve_trace")
+
+
+def apply_tuning(ctx, scene, wl, count, keep_shape):
+    """Applies the cached tuning of `wl`'s size class (searching and caching
+    it on a miss).  keep_shape keeps the context's lanes and wave size (the
+    serve context chooses those for latency) and takes only the grids."""
+    from argent_b200 import tuning as T
+
+    shape = ctx.config()
+    t0 = time.perf_counter()
+    key, t, cached = T.tuned(ctx, scene, wl.camera, wl.settings, wl.width, wl.height, count)
+    if keep_shape:
+        t = dict(t, lanes=shape[0], wave_paths=shape[1])
+        ctx.set_tuning(t)
+    return {"size_class": key, "tuning": ctx.tuning(), "from_cache": cached,
+            "search_s": round(time.perf_counter() - t0, 1), "render": f"{wl.width}x{wl.height}x{count}spp"}
+
+
 def run_gpu(args, world, rank, device):
     import torch
 
@@ -564,6 +597,10 @@ def run_gpu(args, world, rank, device):
     if args.spp:
         plan.set_spp(args.spp)  # profiling runs only: the bench line uses the workload's spp
     stream = torch.cuda.ExternalStream(ctx.stream)
+    tune_info = None
+    if tune_wanted(args):
+        wl, scene, _ = plan.tuning_target()
+        tune_info = apply_tuning(ctx, scene, wl, wl.spp, keep_shape=False)
 
     for i in range(args.warmup):
         run_plan(ctx, plan, i)
@@ -763,6 +800,7 @@ def run_gpu(args, world, rank, device):
                     f"{ctx_wave_mb(args)} MB per wave x {args.lanes or 8} lanes + BVH/triangles "
                     f"{plan.device_bytes / 1e6:.0f} MB)",
                     "context": {"lanes": ctx.config()[0], "wave_paths": ctx.config()[1]},
+                    "tuning": tune_info,
                     "vs_baseline_ref": "README.md:5-6 ~17.7M path-samples/s on 32 CPU cores"})
         out = {
             "metric": "path-samples/s", "value": value, "unit": "path-samples/s", "n_gpus": world,
@@ -794,7 +832,8 @@ def run_gpu(args, world, rank, device):
             "plain_form": plain,
             "error_vs_fp64_oracle": acc,
         }
-        print(json.dumps(out), flush=True)
+        return out
+    return None
 
 
 def run_serve(args, world, rank, device):
@@ -822,6 +861,13 @@ def run_serve(args, world, rank, device):
     ps = W.settings(12)
     rate = args.serve_rate
     trace = W.serve_trace(rate, args.serve_seconds)
+    tune_info = None
+    if tune_wanted(args):
+        # A listing of the 1.0M-triangle piece at 16 spp: about one step's
+        # worth of work (2^26 path-samples).
+        _, lw, lh, _, _ = W.SERVE_CLASSES["listing"]
+        twl = W.Workload("serve_tuning", meshes[4], None, cams[(4, "listing")], lw, lh, 16, ps, 7)
+        tune_info = apply_tuning(ctx, scenes[(4, 1)], twl, 16, keep_shape=True)
     srv = Serve(ctx, film_budget=32 << 30, max_active=64, step_path_samples=args.serve_step,
                 step_path_samples_max=args.serve_step_max, aging_ms=args.serve_aging_ms,
                 overlap=not args.serve_no_overlap, max_pending=args.serve_max_pending)
@@ -944,7 +990,7 @@ def run_serve(args, world, rank, device):
                        "offered_path_samples_per_s": offered, "step_path_samples": args.serve_step,
                        "step_path_samples_max": args.serve_step_max or 2 * args.serve_step,
                        "aging_ms": args.serve_aging_ms or 250, "overlap": not args.serve_no_overlap,
-                       "max_pending": args.serve_max_pending,
+                       "max_pending": args.serve_max_pending, "tuning": tune_info,
                        "parallelism": f"replicas{world}",
                        "timing": "wall clock of the serve loop (latency is a wall-clock quantity); each step "
                                  "synchronises its batch"},
@@ -960,7 +1006,8 @@ def run_serve(args, world, rank, device):
                                                f"request, FP64 film, {ORACLE_SPP} spp on the device",
                                      "classes": acc} if acc else None,
         }
-        print(json.dumps(out), flush=True)
+        return out
+    return None
 
 
 def serve_plain(ctx, trace, scenes, cams, ps, max_pending=0):
@@ -1034,6 +1081,70 @@ def ctx_wave_mb(args):
     return PATH_STATE_BYTES * (args.wave_paths or STILL_WAVE_PATHS) // 10 ** 6
 
 
+def reel_compare(args, device, steps=2):
+    """The batched form against the plain single-render path on one frame
+    of the batched workload (12 renders: 3 pieces x 4 alloys), both end to
+    end with host buffers: the batch is one render_batch and then every
+    film's read; the plain path is render_reel's loop (jobs.rs:689-707), one
+    render_pass and its film read per render."""
+    from argent_b200.gpu import Context, render_pass
+
+    ctx = Context(device, wave_paths=STILL_WAVE_PATHS)
+    plan = ReelPlan(ctx)
+    fp = ctypes.POINTER(ctypes.c_float)
+    bufs = [tuple(np.zeros((f.height, f.width, 3), np.float32) for _ in range(3)) for f in plan.films]
+
+    def read(f, b):
+        c, a, n = b
+        ctx.check(ctx.lib.argent_film_read(f.h, c.ctypes.data_as(fp), a.ctypes.data_as(fp), n.ctypes.data_as(fp)))
+
+    def batched(k):
+        run_plan(ctx, plan, k)
+        for f, b in zip(plan.films, bufs):
+            read(f, b)
+
+    def plain(k):
+        for it, b in zip(plan.items(k), bufs):
+            it[2].clear()
+            render_pass(ctx, *it)
+            read(it[2], b)
+
+    out = {}
+    for name, fn in (("batched", batched), ("plain", plain)):
+        fn(0)  # warm-up (graphs captured, buffers grown)
+        ctx.sync()
+        t0 = time.perf_counter()
+        for k in range(steps):
+            fn(1 + k)
+        dt = time.perf_counter() - t0
+        out[name] = {"e2e_path_samples_per_s": plan.path_samples * steps / dt, "s_per_frame": dt / steps}
+    out["workload"] = plan.name
+    out["renders_per_frame"] = plan.renders
+    out["timing"] = f"wall clock, {steps} turntable frames each, films read to host memory"
+    return out
+
+
+def north_star_extras(args, device):
+    """Short legs of the north-star comparison carried in the default line:
+    the batched reel against the plain single-render path, and a served
+    Poisson trace against argent's one-job-at-a-time queue at a rate near
+    the device's capacity."""
+    out = {"reel": reel_compare(args, device)}
+    import gc
+
+    gc.collect()
+    sargs = argparse.Namespace(**vars(args))
+    sargs.serve_rate = args.extras_serve_rate
+    sargs.serve_seconds = args.extras_serve_seconds
+    sargs.no_oracle = True
+    sargs.wave_paths = 0
+    sargs.warmup = 3
+    srv = run_serve(sargs, 1, 0, device)
+    keep = ("value", "latency_s", "rejected", "plain_form", "config")
+    out["serve"] = {k: srv[k] for k in keep if k in srv}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1047,6 +1158,12 @@ def main():
     ap.add_argument("--no-oracle", action="store_true", help="skip the FP64 65,536-spp error measurement")
     ap.add_argument("--no-plain", action="store_true", help="serve_trace: skip the one-job-at-a-time comparison")
     ap.add_argument("--spp", type=int, default=0, help="override spp (short profiling runs)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="signet_still: skip the short batched-vs-plain reel and served-vs-plain trace legs")
+    ap.add_argument("--extras-serve-rate", type=float, default=8.0)
+    ap.add_argument("--extras-serve-seconds", type=float, default=30.0)
+    ap.add_argument("--tune", action="store_true", help="apply (search and cache) a launch tuning")
+    ap.add_argument("--no-tune", action="store_true", help="no launch tuning, also for reel and serve")
     ap.add_argument("--tri-test", default="mt", choices=["mt", "watertight"],
                     help="stills: argent's Moller-Trumbore (default, bit-exact) or the watertight test")
     ap.add_argument("--lanes", type=int, default=0, help="concurrent waves (0 = the library default)")
@@ -1068,12 +1185,17 @@ def main():
         return
     world, rank, local = dist_setup(args.gpus)
     try:
-        if args.impl == "reference":
-            run_reference(args, world, rank)
-        elif args.workload == "serve_trace":
-            run_serve(args, world, rank, local)
+        if args.workload == "serve_trace":
+            out = run_serve(args, world, rank, local)
         else:
-            run_gpu(args, world, rank, local)
+            out = run_gpu(args, world, rank, local)
+        if out is not None and rank == 0:
+            if args.workload == "signet_still" and world == 1 and not args.no_extras:
+                import gc
+
+                gc.collect()  # the still's context and its path state go before the extras' contexts
+                out["north_star"] = north_star_extras(args, local)
+            print(json.dumps(out), flush=True)
     finally:
         if world > 1:
             import torch.distributed as td

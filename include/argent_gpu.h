@@ -530,15 +530,17 @@ int argent_mesh_smooth(const float* positions, uint32_t nv, const uint32_t* tris
  * Replaces serve's job loop for stills (argent/src/serve/queue.rs:599-617:
  * one job at a time, render_pass in chunks sized for ~1.5 s, seed 7, a
  * cancel check between chunks) and its progressive live passes
- * (serve/live.rs:747, 767).  Here all requests in flight advance together:
- * each argent_serve_step issues one batch (as argent_render_batch) in which
- * the active requests, most urgent first, take whole samples of their frame
- * up to the step's budget.  Urgency is the priority value minus the time
- * waited over aging_ms (lower first; ties in submission order).  The budget
- * is a quarter of the pending work, between step_path_samples and
- * step_path_samples_max; a request whose remaining work is under a sixteenth
- * of it finishes in that batch, and every active request advances by at
- * least one sample.  Chunks continue each film's sample indices, so a
+ * (serve/live.rs:747, 767).  Here requests in flight share batches: each
+ * argent_serve_step issues one batch (as argent_render_batch) of chunks,
+ * whole samples of the requests' frames, up to the step's budget.  The
+ * budget is a quarter of the pending work, between step_path_samples and
+ * step_path_samples_max.  Requests whose remaining work is under a
+ * sixteenth of it finish in that batch (together up to half the budget);
+ * the rest of the budget goes to the other active requests strictly in
+ * urgency order (a request reached with no budget left waits; the first
+ * one reached always takes at least one sample).  Urgency is the priority
+ * value minus the time waited over aging_ms (lower first; ties in
+ * submission order).  Chunks continue each film's sample indices, so a
  * finished film holds what one argent_render_pass of `spp` samples with the
  * same seed gives (up to the order of the FP32 sums).
  *

@@ -138,7 +138,7 @@ def test_patina_render_matches_oracle():
     e = rel_rmse(got, ref)
     print("patina relRMSE XYZ vs oracle:", e, "patina vs polished", rel_rmse(ref, plain))
     assert np.all(e <= RELRMSE_TOL), e
-    assert np.all(rel_rmse(ref, plain) > 5 * RELRMSE_TOL)  # the patina is visible
+    assert np.all(rel_rmse(ref, plain) > 2 * RELRMSE_TOL)  # the patina is visible
 
 
 @pytest.mark.gpu
