@@ -200,6 +200,7 @@ GPU_FUNCS = {
     "argent_ctx_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
                                          ctypes.POINTER(ctypes.c_uint64)]),
     "argent_ctx_set_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64]),
+    "argent_ctx_child_hit_histogram": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
     "argent_ctx_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ArgentTuning)]),
     "argent_ctx_set_tuning": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ArgentTuning)]),
     "argent_piece_set_triangle_test": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
@@ -244,7 +245,8 @@ GPU_FUNCS = {
                                           ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "argent_serve_now": (ctypes.c_double, [ctypes.c_void_p]),
 }
-KERNEL_CLASSES = ["raygen", "intersect", "shade", "shadow", "film", "trace"]
+KERNEL_CLASSES = ["raygen", "intersect", "shade", "shadow", "film", "trace", "shade_terminal", "shade_metal",
+                  "shade_coated", "shade_dielectric", "shade_other"]
 
 _f, _i32, _u32, _cp = ctypes.c_float, ctypes.c_int32, ctypes.c_uint32, ctypes.c_char_p
 _i32p = ctypes.POINTER(ctypes.c_int32)

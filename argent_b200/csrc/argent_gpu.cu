@@ -1301,12 +1301,28 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
             dev::k_intersect<false><<<g_int[0], 128, 0, st>>>(a, (int)depth);
         }
         {
-          ProfScope ps(ctx, KC_SHADE, st);
-          if (classes & (1u << CLS_TERMINAL)) launch_shade<CLS_TERMINAL>(map, g_sh[CLS_TERMINAL], st, a, (int)depth);
-          if (classes & (1u << CLS_METAL)) launch_shade<CLS_METAL>(map, g_sh[CLS_METAL], st, a, (int)depth);
-          if (classes & (1u << CLS_COATED)) launch_shade<CLS_COATED>(map, g_sh[CLS_COATED], st, a, (int)depth);
-          if (classes & (1u << CLS_DIELECTRIC)) launch_shade<CLS_DIELECTRIC>(map, g_sh[CLS_DIELECTRIC], st, a, (int)depth);
-          if (classes & (1u << CLS_OTHER)) launch_shade<CLS_OTHER>(map, g_sh[CLS_OTHER], st, a, (int)depth);
+          // One timing scope per class launch (profiling only); the shade
+          // total is their sum.
+          if (classes & (1u << CLS_TERMINAL)) {
+            ProfScope ps(ctx, KC_SHADE_CLS0 + CLS_TERMINAL, st);
+            launch_shade<CLS_TERMINAL>(map, g_sh[CLS_TERMINAL], st, a, (int)depth);
+          }
+          if (classes & (1u << CLS_METAL)) {
+            ProfScope ps(ctx, KC_SHADE_CLS0 + CLS_METAL, st);
+            launch_shade<CLS_METAL>(map, g_sh[CLS_METAL], st, a, (int)depth);
+          }
+          if (classes & (1u << CLS_COATED)) {
+            ProfScope ps(ctx, KC_SHADE_CLS0 + CLS_COATED, st);
+            launch_shade<CLS_COATED>(map, g_sh[CLS_COATED], st, a, (int)depth);
+          }
+          if (classes & (1u << CLS_DIELECTRIC)) {
+            ProfScope ps(ctx, KC_SHADE_CLS0 + CLS_DIELECTRIC, st);
+            launch_shade<CLS_DIELECTRIC>(map, g_sh[CLS_DIELECTRIC], st, a, (int)depth);
+          }
+          if (classes & (1u << CLS_OTHER)) {
+            ProfScope ps(ctx, KC_SHADE_CLS0 + CLS_OTHER, st);
+            launch_shade<CLS_OTHER>(map, g_sh[CLS_OTHER], st, a, (int)depth);
+          }
           *kernels += __builtin_popcount(classes);
         }
         {
@@ -2192,6 +2208,12 @@ int argent_ctx_kernel_times(ArgentCtx* ctx, double* ms, uint64_t* launches) {
     ms[k] = ctx->prof.ms[k];
     launches[k] = ctx->prof.n[k];
   }
+  ms[KC_SHADE] = 0.0;
+  launches[KC_SHADE] = 0;
+  for (int c = 0; c < 5; ++c) {
+    ms[KC_SHADE] += ctx->prof.ms[KC_SHADE_CLS0 + c];
+    launches[KC_SHADE] += ctx->prof.n[KC_SHADE_CLS0 + c];
+  }
   return ARGENT_OK;
 }
 
@@ -2218,6 +2240,8 @@ int argent_ctx_set_counting(ArgentCtx* ctx, int on) {
   ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_trav_counts, z, 6 * sizeof(unsigned long long)));
   ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_trav_hist, z, sizeof(z)));
   ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_trav_max, zm, sizeof(zm)));
+  unsigned long long zc[18] = {};
+  ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_trav_child_hits, zc, sizeof(zc)));
   std::vector<unsigned long long> zb(2 * ARGENT_MAX_DEPTH, 0ull);
   ARGENT_CK(ctx, cudaMemcpyToSymbol(dev::d_bounce_counts, zb.data(), zb.size() * sizeof(unsigned long long)));
   ctx->counting = on != 0;
@@ -2245,6 +2269,16 @@ int argent_ctx_traversal_histogram(ArgentCtx* ctx, uint64_t* out18) {
   for (int i = 0; i < 16; ++i) out18[i] = h[i];
   out18[16] = m[0];
   out18[17] = m[1];
+  return ARGENT_OK;
+}
+
+int argent_ctx_child_hit_histogram(ArgentCtx* ctx, uint64_t* out18) {
+  if (!ctx || !out18) return set_error(ctx, ARGENT_E_INVALID, "NULL argument");
+  ARGENT_CK(ctx, cudaSetDevice(ctx->device));
+  ARGENT_CK(ctx, cudaStreamSynchronize(ctx->stream));
+  unsigned long long h[18];
+  ARGENT_CK(ctx, cudaMemcpyFromSymbol(h, dev::d_trav_child_hits, sizeof(h)));
+  for (int i = 0; i < 18; ++i) out18[i] = h[i];
   return ARGENT_OK;
 }
 

@@ -24,6 +24,9 @@ __device__ unsigned long long d_trav_counts[6];
 // closest-hit then any-hit, and the largest visit count of each kind.
 __device__ unsigned long long d_trav_hist[16];
 __device__ unsigned int d_trav_max[2];
+// Node visits by the number of children whose box the ray enters (0..8),
+// closest-hit then any-hit.
+__device__ unsigned long long d_trav_child_hits[18];
 // Paths entering each bounce and shadow rays queued at each bounce (64
 // bounces, the path depth limit), summed over the waves run while counting
 // is on.

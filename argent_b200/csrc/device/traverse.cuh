@@ -481,6 +481,7 @@ __device__ __forceinline__ bool closest_visit(const DevPiece& pc, ClosestTrav& s
     k[c] = h ? ((__float_as_uint(tc) & ~7u) | (uint32_t)c) : 0xFFFFFFFFu;
     nh += h ? 1 : 0;
   }
+  if (d_trav_counting) atomicAdd(&d_trav_child_hits[nh], 1ull);
   if (nh == 0) return s.sp > 0;
   if (s.sp + nh - 1 > ARGENT_STACK_SIZE) {
     atomicOr(status, ARGENT_STATUS_STACK_OVERFLOW);
@@ -593,6 +594,7 @@ __device__ __forceinline__ int any_visit(const DevPiece& pc, AnyTrav& s, ST& sta
     if (child_q(nq, c, s.t_max, &tmin)) hitmask |= 1u << c;
   }
   hitmask &= n.present;
+  if (d_trav_counting) atomicAdd(&d_trav_child_hits[9 + __popc(hitmask)], 1ull);
   if (s.sp + __popc(hitmask) > ARGENT_STACK_SIZE) {
     atomicOr(status, ARGENT_STATUS_STACK_OVERFLOW);
     s.sp = 0;

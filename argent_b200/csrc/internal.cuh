@@ -118,13 +118,13 @@ struct WaveBuffers {
 };
 
 // Per-kernel-class CUDA event pairs recorded while profiling is on.
-enum { KC_RAYGEN = 0, KC_INTERSECT, KC_SHADE, KC_SHADOW, KC_FILM, KC_TRACE, KC_COUNT };
+enum { KC_RAYGEN = 0, KC_INTERSECT, KC_SHADE, KC_SHADOW, KC_FILM, KC_TRACE, KC_SHADE_CLS0, KC_COUNT = KC_SHADE_CLS0 + 5 };
 struct KernelProfile {
   bool on = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[KC_COUNT];
   std::vector<cudaEvent_t> pool;
-  double ms[KC_COUNT] = {0, 0, 0, 0, 0, 0};
-  uint64_t n[KC_COUNT] = {0, 0, 0, 0, 0, 0};
+  double ms[KC_COUNT] = {};
+  uint64_t n[KC_COUNT] = {};
 };
 
 // Waves rotate over `lanes` lanes (default 8, at most ARGENT_LANES), each

@@ -74,8 +74,8 @@ class Context:
 
     def kernel_times(self):
         """{class: (total_ms, launches)} since the last set_profiling."""
-        ms = (ctypes.c_double * 6)()
-        n = (ctypes.c_uint64 * 6)()
+        ms = (ctypes.c_double * len(N.KERNEL_CLASSES))()
+        n = (ctypes.c_uint64 * len(N.KERNEL_CLASSES))()
         self.check(self.lib.argent_ctx_kernel_times(self.h, ms, n))
         return {k: (ms[i], int(n[i])) for i, k in enumerate(N.KERNEL_CLASSES)}
 
@@ -127,6 +127,14 @@ class Context:
         self.check(self.lib.argent_ctx_traversal_counts(self.h, out))
         k = ["closest_rays", "closest_nodes", "closest_tris", "any_rays", "any_nodes", "any_tris"]
         return dict(zip(k, [int(x) for x in out]))
+
+    def child_hit_histogram(self):
+        """Interior node visits by children entered (0..8): {"closest": [...],
+        "any": [...]} since counting was turned on."""
+        out = (ctypes.c_uint64 * 18)()
+        self.check(self.lib.argent_ctx_child_hit_histogram(self.h, out))
+        v = [int(x) for x in out]
+        return {"closest": v[0:9], "any": v[9:18]}
 
     def bounce_counts(self):
         """(paths entering each bounce, shadow rays queued at each bounce),

@@ -613,6 +613,7 @@ def run_gpu(args, world, rank, device):
     counts = ctx.traversal_counts()
     bounce_act, bounce_sh = ctx.bounce_counts()
     hist = ctx.traversal_histogram()
+    child_hits = ctx.child_hit_histogram()
     ctx.set_counting(False)
     for f in cfilms:
         f.close()
@@ -660,7 +661,8 @@ def run_gpu(args, world, rank, device):
     kt = ctx.kernel_times()
     ctx.set_profiling(False)
     ctx.set_config(lanes_cfg, wave_cfg)
-    serial_total = sum(v[0] for v in kt.values()) or 1.0
+    # "shade" is the sum of the per-class "shade_*" entries
+    serial_total = sum(v[0] for k, v in kt.items() if not k.startswith("shade_")) or 1.0
 
     # Dominant kernel: the single kernel with the largest share of serialised
     # device time (closest-hit traversal here; "shade" totals the five
@@ -826,6 +828,7 @@ def run_gpu(args, world, rank, device):
             "kernel_share_alone": {k: round(v[0] / serial_total, 4) for k, v in kt.items()},
             "traversal_per_path_sample": {k: v / px for k, v in counts.items()},
             "traversal_nodes_per_ray_histogram": hist,
+            "traversal_children_entered_per_node_visit": child_hits,
             "rays_per_path_sample_by_bounce": {"closest": [round(x / px, 4) for x in bounce_act],
                                                "shadow": [round(x / px, 4) for x in bounce_sh]},
             "cpu_baseline": cpu,

@@ -639,7 +639,13 @@ enum {
   ARGENT_KC_SHADOW = 3,
   ARGENT_KC_FILM = 4,
   ARGENT_KC_TRACE = 5,
-  ARGENT_KC_COUNT = 6
+  /* The shading kernel of each material class; ARGENT_KC_SHADE is their sum. */
+  ARGENT_KC_SHADE_TERMINAL = 6,
+  ARGENT_KC_SHADE_METAL = 7,
+  ARGENT_KC_SHADE_COATED = 8,
+  ARGENT_KC_SHADE_DIELECTRIC = 9,
+  ARGENT_KC_SHADE_OTHER = 10,
+  ARGENT_KC_COUNT = 11
 };
 /* While on, every launch is bracketed by CUDA events on the context stream;
  * turning it on or off resets the totals. */
@@ -661,6 +667,10 @@ int argent_ctx_traversal_counts(ArgentCtx* ctx, uint64_t* out);
  * count of a closest-hit ray and of an any-hit ray, since the last
  * argent_ctx_set_counting. */
 int argent_ctx_traversal_histogram(ArgentCtx* ctx, uint64_t* out);
+/* out[18]: interior node visits by the number of children whose box the ray
+ * enters, 0..8 (closest hit out[0..8], any hit out[9..17]), since the last
+ * argent_ctx_set_counting. */
+int argent_ctx_child_hit_histogram(ArgentCtx* ctx, uint64_t* out);
 /* out[128]: paths entering bounce d (out[d]) and shadow rays queued at
  * bounce d (out[64 + d]), d < 64, summed over the waves run since the last
  * argent_ctx_set_counting that turned counting on. */
