@@ -106,7 +106,8 @@ class ArgentBatchItem(ctypes.Structure):
 class ArgentServeConfig(ctypes.Structure):
     _fields_ = [("film_budget", ctypes.c_uint64), ("max_active", ctypes.c_uint32), ("aging_ms", ctypes.c_uint32),
                 ("step_path_samples", ctypes.c_uint64), ("step_path_samples_max", ctypes.c_uint64),
-                ("overlap", ctypes.c_uint32), ("max_pending", ctypes.c_uint32)]
+                ("overlap", ctypes.c_uint32), ("max_pending", ctypes.c_uint32),
+                ("max_pending_path_samples", ctypes.c_uint64)]
 
 
 class ArgentServeRequest(ctypes.Structure):

@@ -1263,10 +1263,24 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
 
   // Issues the batch: fork from the context stream, each wave's kernels on
   // its lane, join.  Counts the kernels it launches.
+  // The step of the issue that failed first, for the error text.
+  const char* stage = "fork";
   auto issue = [&](uint64_t* kernels) -> cudaError_t {
+    // Launch errors are reported by cudaPeekAtLastError right after the
+    // launch that caused them, so the failing step is named.
+    auto launched = [&](cudaError_t& e, const char* what) {
+      if (e != cudaSuccess) return;
+      e = cudaPeekAtLastError();
+      if (e != cudaSuccess) stage = what;
+    };
+    // An error left by an earlier, unrelated runtime call on this thread
+    // (already reported by whichever call made it) is not this batch's.
+    cudaError_t stale = cudaGetLastError();
+    if (stale != cudaSuccess) ctx->stale_errors++;
     cudaError_t e = cudaEventRecord(ctx->fork_ev, ctx->stream);
     for (int k = 0; k < used && e == cudaSuccess; ++k)
       e = cudaStreamWaitEvent(ctx->lane_stream[(start + k) % nlanes], ctx->fork_ev, 0);
+    if (e == cudaSuccess) stage = "waves";
     int prev_film = chain_first ? ctx->last_film_lane : -1;
     for (size_t wi = 0; wi < waves.size() && e == cudaSuccess; ++wi) {
       const dev::WaveDesc& w = waves[wi];
@@ -1289,6 +1303,7 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
         ProfScope ps(ctx, KC_RAYGEN, st);
         dev::k_raygen<<<g_ray, 256, 0, st>>>(a, w);
       }
+      launched(e, "k_raygen");
       ++*kernels;
       for (uint32_t depth = 0; depth < depths[wi] && depth < ARGENT_MAX_DEPTH; ++depth) {
         a.q_in = (depth & 1) ? wb.q1 : wb.q0;
@@ -1300,6 +1315,7 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
           else
             dev::k_intersect<false><<<g_int[0], 128, 0, st>>>(a, (int)depth);
         }
+        launched(e, "k_intersect");
         {
           // One timing scope per class launch (profiling only); the shade
           // total is their sum.
@@ -1325,6 +1341,7 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
           }
           *kernels += __builtin_popcount(classes);
         }
+        launched(e, "k_shade");
         {
           ProfScope ps(ctx, KC_SHADOW, st);
           if (uni)
@@ -1332,6 +1349,7 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
           else
             dev::k_shadow<false><<<g_any[0], 128, 0, st>>>(a, (int)depth);
         }
+        launched(e, "k_shadow");
         *kernels += 2;
       }
       if (ctx->counting) {
@@ -1340,15 +1358,20 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
         ++*kernels;
       }
       // Films accumulate in wave order: wait for the previous wave's film pass.
-      if (prev_film >= 0 && prev_film != lane) e = cudaStreamWaitEvent(st, ctx->film_ev[prev_film], 0);
+      if (e == cudaSuccess && prev_film >= 0 && prev_film != lane) {
+        e = cudaStreamWaitEvent(st, ctx->film_ev[prev_film], 0);
+        if (e != cudaSuccess) stage = "film chain";
+      }
       {
         ProfScope ps(ctx, KC_FILM, st);
         dev::k_film<<<g_film, 256, 0, st>>>(a, w);
       }
+      launched(e, "k_film");
       if (e == cudaSuccess) e = cudaEventRecord(ctx->film_ev[lane], st);
       prev_film = lane;
       ++*kernels;
     }
+    if (e == cudaSuccess) stage = "join";
     for (int k = 0; k < used && e == cudaSuccess; ++k) {
       e = cudaEventRecord(ctx->join_ev, ctx->lane_stream[(start + k) % nlanes]);
       if (e == cudaSuccess) e = cudaStreamWaitEvent(join, ctx->join_ev, 0);
@@ -1438,7 +1461,8 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
     if (e == cudaSuccess) e = cudaEventRecord(done, join);
     ctx->overlapped_pending = true;
   }
-  if (e != cudaSuccess) return set_error(ctx, ARGENT_E_CUDA, std::string("render launch: ") + cudaGetErrorString(e));
+  if (e != cudaSuccess)
+    return set_error(ctx, ARGENT_E_CUDA, std::string("render launch (") + stage + "): " + cudaGetErrorString(e));
   return ARGENT_OK;
 }
 

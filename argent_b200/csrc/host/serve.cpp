@@ -28,7 +28,10 @@
 //
 // Bound: with max_pending set, a submit that finds that many requests
 // queued or active is refused with ARGENT_E_BUSY (argent's queue refuses a
-// job when 24 are waiting, serve/queue.rs:28,364-366).
+// job when 24 are waiting, serve/queue.rs:28,364-366); with
+// max_pending_path_samples, one that would take the work still to render
+// past that bound is refused too, which bounds every admitted request's wait
+// when requests arrive faster than the device renders them.
 //
 // Threads: submit, poll and cancel lock the queue and may be called from
 // any thread.  step and read drive the context and belong to the thread
@@ -242,13 +245,21 @@ int argent_serve_submit(ArgentServe* s, const ArgentServeRequest* req, uint64_t*
   uint64_t fb = film_bytes(req->width, req->height, req->film_flags);
   if (fb > s->cfg.film_budget) return ARGENT_E_BUSY;
   std::lock_guard<std::mutex> g(s->mu);
-  if (s->cfg.max_pending) {
+  if (s->cfg.max_pending || s->cfg.max_pending_path_samples) {
     // A bounded queue, as argent's (queue.rs:364-366): refuse rather than
-    // let the wait of every admitted request grow without bound.
+    // let the wait of every admitted request grow without bound.  The bound
+    // counts requests, or the work they still need, or both.
     uint32_t n = 0;
+    uint64_t work = 0;
     for (auto& kv : s->reqs)
-      if (kv.second.state == ARGENT_REQ_QUEUED || kv.second.state == ARGENT_REQ_ACTIVE) ++n;
-    if (n >= s->cfg.max_pending) {
+      if (kv.second.state == ARGENT_REQ_QUEUED || kv.second.state == ARGENT_REQ_ACTIVE) {
+        ++n;
+        work += remaining(&kv.second);
+      }
+    uint64_t mine = (uint64_t)req->spp * req->width * req->height;
+    bool busy = (s->cfg.max_pending && n >= s->cfg.max_pending) ||
+                (s->cfg.max_pending_path_samples && n > 0 && work + mine > s->cfg.max_pending_path_samples);
+    if (busy) {
       ++s->rejected;
       return ARGENT_E_BUSY;
     }

@@ -181,6 +181,9 @@ struct ArgentCtx {
   // Device address of the allocation-free entry point's static array,
   // looked up by this context's first call of it.
   void* noalloc_addr = nullptr;
+  // Runtime errors found pending (from earlier calls) when a batch was
+  // issued; cleared there, counted for diagnosis.
+  uint64_t stale_errors = 0;
 };
 
 struct ArgentPiece {

@@ -411,12 +411,16 @@ __device__ __forceinline__ uint32_t lane_refill(bool idle, bool* first, bool* mo
 // theirs is done.
 // Rows of the traversal kernels' shared-memory stack rings (ShortStack);
 // 0 keeps the whole stack in local memory.  The kernels run 128 threads per
-// block.
+// block.  Measured on B200 (signet still, eight lanes): local stacks 1.756 G
+// path-samples/s, rings of 8 rows 1.727 G, of 16 rows 1.722 G -- the rings'
+// shared memory (8-16 KB per block) costs the other lanes' kernels L1 and
+// co-residency more than the stack traffic it saves (the local stack hits
+// in L1), so the default is 0.
 #ifndef ARGENT_SHORT_STACK
-#define ARGENT_SHORT_STACK 16
+#define ARGENT_SHORT_STACK 0
 #endif
 #ifndef ARGENT_SHORT_STACK_ANY
-#define ARGENT_SHORT_STACK_ANY 16
+#define ARGENT_SHORT_STACK_ANY 0
 #endif
 #if ARGENT_SHORT_STACK > 0
 #define ARGENT_CLOSEST_STACK(name)                                             \

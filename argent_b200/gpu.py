@@ -345,10 +345,11 @@ class Serve:
     the thread that owns the context."""
 
     def __init__(self, ctx: Context, film_budget=0, max_active=0, step_path_samples=0, aging_ms=0,
-                 step_path_samples_max=0, overlap=False, max_pending=0):
+                 step_path_samples_max=0, overlap=False, max_pending=0, max_pending_path_samples=0):
         self.ctx = ctx
         cfg = N.ArgentServeConfig(int(film_budget), int(max_active), int(aging_ms), int(step_path_samples),
-                                  int(step_path_samples_max), 1 if overlap else 0, int(max_pending))
+                                  int(step_path_samples_max), 1 if overlap else 0, int(max_pending),
+                                  int(max_pending_path_samples))
         h = ctypes.c_void_p()
         ctx.check(ctx.lib.argent_serve_create(ctx.h, ctypes.byref(cfg), ctypes.byref(h)))
         self.h = h

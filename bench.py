@@ -873,7 +873,8 @@ def run_serve(args, world, rank, device):
         tune_info = apply_tuning(ctx, scenes[(4, 1)], twl, 16, keep_shape=True)
     srv = Serve(ctx, film_budget=32 << 30, max_active=64, step_path_samples=args.serve_step,
                 step_path_samples_max=args.serve_step_max, aging_ms=args.serve_aging_ms,
-                overlap=not args.serve_no_overlap, max_pending=args.serve_max_pending)
+                overlap=not args.serve_no_overlap, max_pending=args.serve_max_pending,
+                max_pending_path_samples=int(args.serve_max_pending_work * W.mean_request_path_samples()))
 
     def submit(cname, i, j):
         _, w, h, spp, prio = W.SERVE_CLASSES[cname]
@@ -993,7 +994,9 @@ def run_serve(args, world, rank, device):
                        "offered_path_samples_per_s": offered, "step_path_samples": args.serve_step,
                        "step_path_samples_max": args.serve_step_max or 2 * args.serve_step,
                        "aging_ms": args.serve_aging_ms or 250, "overlap": not args.serve_no_overlap,
-                       "max_pending": args.serve_max_pending, "tuning": tune_info,
+                       "max_pending": args.serve_max_pending,
+                       "max_pending_path_samples": int(args.serve_max_pending_work * W.mean_request_path_samples()),
+                       "tuning": tune_info,
                        "parallelism": f"replicas{world}",
                        "timing": "wall clock of the serve loop (latency is a wall-clock quantity); each step "
                                  "synchronises its batch"},
@@ -1180,6 +1183,9 @@ def main():
     ap.add_argument("--serve-no-overlap", action="store_true", help="serve_trace: wait for each step's batch")
     ap.add_argument("--serve-max-pending", type=int, default=25,
                     help="serve_trace: requests waiting or rendering at most, both forms (argent: 24 waiting + 1)")
+    ap.add_argument("--serve-max-pending-work", type=float, default=25.0,
+                    help="serve_trace, served form: pending work bound in mean requests' path-samples "
+                         "(0 = none); 25 is the work argent's 25-job bound holds on average")
     args = ap.parse_args()
     if args.impl == "reference":
         # CPU only: rank 0 measures, the other ranks have nothing to do.

@@ -571,6 +571,11 @@ typedef struct ArgentServeConfig {
   uint32_t max_pending;       /* requests queued or active at most: a submit beyond it returns
                                  ARGENT_E_BUSY (argent refuses a job when 24 wait, queue.rs:28,364);
                                  0 = no bound */
+  uint64_t max_pending_path_samples; /* work not yet rendered, at most: a submit that would take the
+                                        path-samples still to render of the queued and active requests
+                                        past it returns ARGENT_E_BUSY (a request finding nothing
+                                        pending is always taken); bounds the wait of every admitted
+                                        request under overload; 0 = no bound */
 } ArgentServeConfig;
 
 typedef struct ArgentServeRequest {

@@ -46,7 +46,7 @@ def test_struct_sizes_match_c():
     assert ctypes.sizeof(N.ArgentMaterial) == 13 * 4 + 2 * 95 * 4 + 3 * 471 * 4
     assert ctypes.sizeof(N.ArgentCamera) == 4 * (12 + 4 + 2)
     assert ctypes.sizeof(N.ArgentTuning) == 40
-    assert ctypes.sizeof(N.ArgentServeConfig) == 40
+    assert ctypes.sizeof(N.ArgentServeConfig) == 48
 
 
 def test_error_path_without_device():

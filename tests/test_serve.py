@@ -175,3 +175,47 @@ def test_bounded_queue_refuses_beyond_max_pending(ring_setup):
     t = srv.submit(scenes["gold14k"], cam, W.settings(8), 32, 32, 2, 7, 0)
     srv.run()
     assert srv.poll(t).state == N.REQ_DONE
+
+
+def test_serve_after_autotune():
+    """argent_autotune renders on the context with other lane counts and
+    wave sizes and frees the lanes it does not keep; a serve on the same
+    context afterwards (overlapped batches) renders every request."""
+    from argent_b200.gpu import Context, Piece, Scene, Serve
+
+    wl = W.ring_still()
+    ctx = Context(0)
+    scene = Scene(ctx, Piece(ctx, wl.mesh), wl.desc)
+    ctx.autotune(scene, wl.camera, wl.settings, 256, 256, 4)
+    t = ctx.tuning()
+    ctx.set_tuning(dict(t, lanes=8, wave_paths=1 << 22))
+    srv = Serve(ctx, overlap=True, step_path_samples=1 << 17)
+    ts = [srv.submit(scene, _cam(wl, w, h), W.settings(8), w, h, spp, 7, prio)
+          for w, h, spp, prio in ((64, 64, 4, 0), (256, 256, 16, 1), (128, 96, 8, 2))]
+    srv.run()
+    for t in ts:
+        assert srv.poll(t).state == N.REQ_DONE
+        srv.read(t)
+
+
+def test_work_bound_refuses_beyond_max_pending_path_samples(ring_setup):
+    """max_pending_path_samples bounds the work not yet rendered: a request
+    that would take it past the bound is refused; one arriving when nothing
+    is pending is taken whatever its size."""
+    from argent_b200.gpu import Serve
+
+    ctx, _, scenes, wl = ring_setup
+    cam = _cam(wl, 64, 64)
+    srv = Serve(ctx, max_pending_path_samples=64 * 64 * 12)
+    big = srv.submit(scenes["sterling"], cam, W.settings(8), 64, 64, 32, 7, 0)  # above the bound, nothing pending
+    with pytest.raises(N.ArgentError) as e:
+        srv.submit(scenes["sterling"], cam, W.settings(8), 64, 64, 1, 7, 0)
+    assert e.value.code == N.E_BUSY
+    srv.run()
+    srv.read(big)
+    a = srv.submit(scenes["sterling"], cam, W.settings(8), 64, 64, 8, 7, 0)
+    b = srv.submit(scenes["gold14k"], cam, W.settings(8), 64, 64, 4, 7, 0)  # 12 samples of work in all: fits
+    with pytest.raises(N.ArgentError):
+        srv.submit(scenes["gold14k"], cam, W.settings(8), 64, 64, 1, 7, 0)
+    srv.run()
+    assert srv.poll(a).state == N.REQ_DONE and srv.poll(b).state == N.REQ_DONE
