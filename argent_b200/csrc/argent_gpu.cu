@@ -1255,9 +1255,13 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
     wmap[wi] = map;
     wone[wi] = one;
   }
-  // The first film pass waits for the last one before this batch unless the
-  // context stream already orders it (a joined batch after joined ones).
-  const bool chain_first = !joined || ctx->overlapped_pending;
+  // The first film pass waits for the last one before this batch only while
+  // an overlapped batch may still be adding to films.  After a joined batch
+  // the context stream already orders it: this batch forks from that stream
+  // once the joined batch's lanes have joined it.  (A joined batch may have
+  // been captured as a graph, and an event recorded during a capture is no
+  // event to wait on outside it.)
+  const bool chain_first = ctx->overlapped_pending;
   const int last_lane = (int)((start + waves.size() - 1) % nlanes);
   cudaStream_t join = joined ? ctx->stream : ctx->aux_stream;
 
@@ -1460,6 +1464,11 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
     cudaFreeAsync(d_jobs, join);
     if (e == cudaSuccess) e = cudaEventRecord(done, join);
     ctx->overlapped_pending = true;
+  } else {
+    // This batch's first film pass waited for the overlapped batches' last
+    // one and its lanes joined the context stream, so work issued after it
+    // is ordered after every film pass so far.
+    ctx->overlapped_pending = false;
   }
   if (e != cudaSuccess)
     return set_error(ctx, ARGENT_E_CUDA, std::string("render launch (") + stage + "): " + cudaGetErrorString(e));

@@ -378,14 +378,22 @@ __device__ __forceinline__ void sort8(uint32_t k[8]) {
 }
 #undef ARGENT_CX
 
+// Children's push order: 1 = all entered children sorted by entry distance
+// (the nearest popped first), 0 = the nearest entered at once and the rest
+// pushed in slot order.  Hits do not depend on it (see below).
+#ifndef ARGENT_SORTED_PUSH
+#define ARGENT_SORTED_PUSH 0
+#endif
+
 // Closest hit with t in (1e-7, t_max).  Ties at equal t go to the lower
 // original triangle index.
 //
-// Order of visits: the children a node's slab test keeps are sorted by
-// entry distance and the nearest is entered at once; the others are pushed
-// far-to-near.  The sort key is the entry distance with its 3 low mantissa
-// bits replaced by the child slot; the truncated distance is what the stack
-// keeps for pruning, which can only keep more nodes than the exact value.
+// Order of visits: of the children a node's slab test keeps, the nearest
+// by entry distance is entered at once; the others are pushed with their
+// entry distances (ARGENT_SORTED_PUSH: far-to-near).  The key is the entry
+// distance with its 3 low mantissa bits replaced by the child slot; the
+// truncated distance is what the stack keeps for pruning, which can only
+// keep more nodes than the exact value.
 // The visit order changes how much is pruned, never the result: a triangle
 // whose hit is the final best has box entry <= that distance <= the running
 // best at every point, so its box is always entered.
@@ -474,12 +482,14 @@ __device__ __forceinline__ bool closest_visit(const DevPiece& pc, ClosestTrav& s
   NodeQ nq = node_ray(n, s.rq);
   uint32_t k[8];
   int nh = 0;
+  uint32_t hm = 0;
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
     float tc;
     bool h = child_q(nq, c, s.best.t, &tc) && ((n.present >> c) & 1u);
     k[c] = h ? ((__float_as_uint(tc) & ~7u) | (uint32_t)c) : 0xFFFFFFFFu;
     nh += h ? 1 : 0;
+    hm |= h ? (1u << c) : 0u;
   }
   if (d_trav_counting) atomicAdd(&d_trav_child_hits[nh], 1ull);
   if (nh == 0) return s.sp > 0;
@@ -488,12 +498,32 @@ __device__ __forceinline__ bool closest_visit(const DevPiece& pc, ClosestTrav& s
     s.sp = 0;
     return false;
   }
+#if ARGENT_SORTED_PUSH
   sort8(k);
 #pragma unroll
   for (int j = 7; j >= 1; --j) {
     if (j < nh) stack.push(s.sp, make_uint2(child_ref(n, (int)(k[j] & 7u)), k[j] & ~7u));
   }
   s.ref = child_ref(n, (int)(k[0] & 7u));
+#else
+  // Descend into the nearest child; push the others (nh - 1: none in three
+  // visits of four, and at most one in more than nine of ten) in slot order
+  // with their entry distances, so popping still prunes them against the
+  // running best.  The loop runs as many times as the lane has children to
+  // push, where a full sort of eight keys would cost 19 compare-exchanges
+  // and eight guarded pushes on every visit.
+  uint32_t kmin = min(min(min(k[0], k[1]), min(k[2], k[3])), min(min(k[4], k[5]), min(k[6], k[7])));
+  uint32_t near = kmin & 7u;
+  uint32_t rest = hm & ~(1u << near);
+  while (rest) {
+    int c = __ffs(rest) - 1;
+    rest &= rest - 1u;
+    uint32_t kc = c == 0 ? k[0] : c == 1 ? k[1] : c == 2 ? k[2] : c == 3 ? k[3]
+                : c == 4 ? k[4] : c == 5 ? k[5] : c == 6 ? k[6] : k[7];
+    stack.push(s.sp, make_uint2(child_ref(n, c), kc & ~7u));
+  }
+  s.ref = child_ref(n, (int)near);
+#endif
   s.have = true;
   return true;
 }

@@ -141,12 +141,14 @@ struct ArgentCtx {
   cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   cudaEvent_t film_ev[ARGENT_LANES] = {};
   // Waves rotate over the lanes across calls: the next call starts at
-  // next_lane, and its first film pass waits for the film pass of the last
-  // wave before it (on last_film_lane), so films accumulate in wave order
-  // also when batches overlap.
+  // next_lane, and, while an overlapped batch may still run, its first film
+  // pass waits for the film pass of the last wave before it (on
+  // last_film_lane), so films accumulate in wave order also when batches
+  // overlap.
   int next_lane = 0, last_film_lane = -1;
   // Completion stream of batches that do not join the context stream, and
-  // whether one may still run (cleared by argent_ctx_sync).
+  // whether one may still run (cleared by argent_ctx_sync and by a joined
+  // batch, which orders everything after it).
   cudaStream_t aux_stream = nullptr;
   bool overlapped_pending = false;
   // Job records of joined batches (kept, so captured graphs can point at it).
