@@ -101,6 +101,12 @@ __device__ __forceinline__ bool wt_hit(float4 a, float4 b, float4 c, V3 o, V3 d,
 // 0 for argent's Moller-Trumbore (record = v0, e1, e2) and
 // ARGENT_TRI_REC_WATERTIGHT for the watertight test (record = v0, v1, v2).
 #define ARGENT_TRI_REC_WATERTIGHT 1u
+// 0 compiles the watertight branch out of the leaf test (pieces can then
+// only use Moller-Trumbore; argent_piece_set_triangle_test still rewrites
+// the records, which such a build would misread).
+#ifndef ARGENT_WATERTIGHT_OPTION
+#define ARGENT_WATERTIGHT_OPTION 1
+#endif
 
 // Moller-Trumbore, bvh.rs:391-410 (or the watertight test, by the
 // record's marker).  True on a hit with t in (1e-7, t_max).
@@ -109,11 +115,13 @@ __device__ __forceinline__ bool mt_hit(const float4* tri, V3 o, V3 d, float t_ma
   float4 a = __ldg(tri);
   float4 b = __ldg(tri + 1);
   float4 c = __ldg(tri + 2);
+#if ARGENT_WATERTIGHT_OPTION
   if (__float_as_uint(b.w) == ARGENT_TRI_REC_WATERTIGHT) {
     if (!wt_hit(a, b, c, o, d, t_max, t_out, u_out, v_out)) return false;
     *prim_out = __float_as_uint(a.w);
     return true;
   }
+#endif
   V3 v0{a.x, a.y, a.z}, e1{b.x, b.y, b.z}, e2{c.x, c.y, c.z};
   V3 p = cross(d, e2);
   float det = dot(e1, p);
