@@ -388,9 +388,12 @@ __device__ __forceinline__ void sort8(uint32_t k[8]) {
 
 // Children's push order: 1 = all entered children sorted by entry distance
 // (the nearest popped first), 0 = the nearest entered at once and the rest
-// pushed in slot order.  Hits do not depend on it (see below).
+// pushed in slot order.  Hits do not depend on it (see below).  Measured on
+// B200 with eight lanes: sorted 1.752 G path-samples/s on the signet still
+// and 1.17 G on the gems, nearest-first 1.737 G and 1.144 G (it visits a
+// few more nodes, and needs a few more registers), so sorting stays.
 #ifndef ARGENT_SORTED_PUSH
-#define ARGENT_SORTED_PUSH 0
+#define ARGENT_SORTED_PUSH 1
 #endif
 
 // Closest hit with t in (1e-7, t_max).  Ties at equal t go to the lower
@@ -518,8 +521,8 @@ __device__ __forceinline__ bool closest_visit(const DevPiece& pc, ClosestTrav& s
   // visits of four, and at most one in more than nine of ten) in slot order
   // with their entry distances, so popping still prunes them against the
   // running best.  The loop runs as many times as the lane has children to
-  // push, where a full sort of eight keys would cost 19 compare-exchanges
-  // and eight guarded pushes on every visit.
+  // push, where the sort costs 19 compare-exchanges and eight guarded
+  // pushes on every visit.
   uint32_t kmin = min(min(min(k[0], k[1]), min(k[2], k[3])), min(min(k[4], k[5]), min(k[6], k[7])));
   uint32_t near = kmin & 7u;
   uint32_t rest = hm & ~(1u << near);

@@ -30,8 +30,9 @@
 // queued or active is refused with ARGENT_E_BUSY (argent's queue refuses a
 // job when 24 are waiting, serve/queue.rs:28,364-366); with
 // max_pending_path_samples, one that would take the work still to render
-// past that bound is refused too, which bounds every admitted request's wait
-// when requests arrive faster than the device renders them.
+// past that bound is refused too (unless nothing of its priority is
+// pending), which bounds every admitted request's wait when requests arrive
+// faster than the device renders them.
 //
 // Threads: submit, poll and cancel lock the queue and may be called from
 // any thread.  step and read drive the context and belong to the thread
@@ -249,16 +250,21 @@ int argent_serve_submit(ArgentServe* s, const ArgentServeRequest* req, uint64_t*
     // A bounded queue, as argent's (queue.rs:364-366): refuse rather than
     // let the wait of every admitted request grow without bound.  The bound
     // counts requests, or the work they still need, or both.
-    uint32_t n = 0;
+    uint32_t n = 0, same = 0;
     uint64_t work = 0;
     for (auto& kv : s->reqs)
       if (kv.second.state == ARGENT_REQ_QUEUED || kv.second.state == ARGENT_REQ_ACTIVE) {
         ++n;
         work += remaining(&kv.second);
+        if (kv.second.req.priority == req->priority) ++same;
       }
     uint64_t mine = (uint64_t)req->spp * req->width * req->height;
+    // The work bound spares a request whose priority level has nothing
+    // pending, so the largest requests are never all refused while the
+    // small ones keep the pending work near the bound.
     bool busy = (s->cfg.max_pending && n >= s->cfg.max_pending) ||
-                (s->cfg.max_pending_path_samples && n > 0 && work + mine > s->cfg.max_pending_path_samples);
+                (s->cfg.max_pending_path_samples && same > 0 &&
+                 work + mine > s->cfg.max_pending_path_samples);
     if (busy) {
       ++s->rejected;
       return ARGENT_E_BUSY;

@@ -573,9 +573,9 @@ typedef struct ArgentServeConfig {
                                  0 = no bound */
   uint64_t max_pending_path_samples; /* work not yet rendered, at most: a submit that would take the
                                         path-samples still to render of the queued and active requests
-                                        past it returns ARGENT_E_BUSY (a request finding nothing
-                                        pending is always taken); bounds the wait of every admitted
-                                        request under overload; 0 = no bound */
+                                        past it returns ARGENT_E_BUSY, unless no request of its
+                                        priority is pending (so no class is shut out); bounds the
+                                        wait of every admitted request under overload; 0 = no bound */
 } ArgentServeConfig;
 
 typedef struct ArgentServeRequest {

@@ -200,8 +200,8 @@ def test_serve_after_autotune():
 
 def test_work_bound_refuses_beyond_max_pending_path_samples(ring_setup):
     """max_pending_path_samples bounds the work not yet rendered: a request
-    that would take it past the bound is refused; one arriving when nothing
-    is pending is taken whatever its size."""
+    that would take it past the bound is refused; one whose priority level
+    has nothing pending is taken whatever its size."""
     from argent_b200.gpu import Serve
 
     ctx, _, scenes, wl = ring_setup
@@ -217,5 +217,9 @@ def test_work_bound_refuses_beyond_max_pending_path_samples(ring_setup):
     b = srv.submit(scenes["gold14k"], cam, W.settings(8), 64, 64, 4, 7, 0)  # 12 samples of work in all: fits
     with pytest.raises(N.ArgentError):
         srv.submit(scenes["gold14k"], cam, W.settings(8), 64, 64, 1, 7, 0)
+    # another priority level with nothing pending is taken past the bound
+    c = srv.submit(scenes["gold14k"], cam, W.settings(8), 64, 64, 16, 7, 2)
+    with pytest.raises(N.ArgentError):
+        srv.submit(scenes["gold14k"], cam, W.settings(8), 64, 64, 1, 7, 2)
     srv.run()
-    assert srv.poll(a).state == N.REQ_DONE and srv.poll(b).state == N.REQ_DONE
+    assert all(srv.poll(t).state == N.REQ_DONE for t in (a, b, c))
