@@ -308,7 +308,7 @@ def run_reference(args, world, rank):
     t0 = time.perf_counter()
     band(0, 1)
     dt = time.perf_counter() - t0
-    rows = int(max(1, min(wls[0].height // 8, args.ref_seconds / max(dt, 1e-3))))
+    rows = int(max(1, min(wls[0].height // 8, args.ref_step_seconds / max(dt, 1e-3))))
     times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
@@ -1159,7 +1159,9 @@ def main():
     ap.add_argument("--impl", default="argent", choices=["argent", "reference"])
     ap.add_argument("--workload", default="signet_still", choices=list(WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--ref-seconds", type=float, default=8.0)
+    ap.add_argument("--ref-seconds", type=float, default=8.0, help="CPU work of the cpu_baseline sample (GPU arm)")
+    ap.add_argument("--ref-step-seconds", type=float, default=3.0,
+                    help="--impl reference: CPU work of each step's sample (warm-up and timed steps alike)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-oracle", action="store_true", help="skip the FP64 65,536-spp error measurement")
     ap.add_argument("--no-plain", action="store_true", help="serve_trace: skip the one-job-at-a-time comparison")

@@ -12,7 +12,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def test_reference_arm_prints_one_contract_line():
     cmd = [sys.executable, "bench.py", "--impl", "reference", "--workload", "ring_still", "--steps", "2",
-           "--warmup", "1", "--ref-seconds", "0.5"]
+           "--warmup", "1", "--ref-step-seconds", "0.5"]
     out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
