@@ -337,14 +337,19 @@ __global__ void __launch_bounds__(256) k_raygen(WaveArgs a, WaveDesc w) {
     float sy = 1.0f - (((float)y + 0.5f + jy) * aspect_sy);
     V3 o, d;
     camera_ray(job.cam, sx, sy, lu, lv, &o, &d);
+    // The throughput (1 at bounce 0) and the guides are not stored here: the
+    // bounce-0 shading takes beta = 1 and writes every path's guides (zero
+    // where it has none), so ray generation writes 48 B less per path.  A
+    // job without bounces zeroes its guides here, for the film pass.
     a.o[slot] = make_float4(o.x, o.y, o.z, 0.0f);
     a.d[slot] = make_float4(d.x, d.y, d.z, 1.0f);  // w = prev_pdf
-    a.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
     a.L[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     a.lambda[slot] = make_float4(wl.lambda[0], wl.lambda[1], wl.lambda[2], wl.lambda[3]);
     a.pdf[slot] = make_float4(wl.pdf[0], wl.pdf[1], wl.pdf[2], wl.pdf[3]);
-    a.albedo[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    a.normal[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (job.max_depth == 0) {
+      a.albedo[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      a.normal[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
     // flags: bit0 specular, bit1 rough_seen, bits 8..15 medium (material+1), bits 16..31 job
     a.meta[slot] = make_uint4(pix, si, pix_seed, 1u | (sg.job << 16));
     a.rng[slot] = s.rng;
@@ -570,7 +575,8 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
   float4 of = a.o[slot], df = a.d[slot], hf = a.hit[slot];
   V3 ro{of.x, of.y, of.z}, rd{df.x, df.y, df.z};
   float prev_pdf = df.w;
-  Spec beta = spec4(a.beta[slot]);
+  Spec beta = depth == 0 ? spec(1.0f) : spec4(a.beta[slot]);
+  bool guided = false;  // bounce 0: this path's guides are written
   // Radiance changes here only for terminal hits and floor fade misses, and
   // the wavelength pdfs only when a dispersive refraction terminates the
   // secondaries: the other classes read and write them only where they do.
@@ -714,6 +720,7 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
       guide_rgb(mat, cavity, g);
       a.albedo[slot] = make_float4(g[0], g[1], g[2], 0.0f);
       a.normal[slot] = make_float4(nsu.x, nsu.y, nsu.z, 0.0f);
+      guided = true;
     }
 
     // Next-event estimation (integrator.rs:130-178).
@@ -868,6 +875,12 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
   }
   }
   if constexpr (CLS == CLS_TERMINAL) a.L[slot] = to_f4(L);
+  if (depth == 0 && !guided) {
+    // A camera ray that ends at its first hit (miss, panel, faded floor)
+    // has no guides: the film adds zeros.
+    a.albedo[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    a.normal[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  }
   return out;
 }
 
