@@ -53,7 +53,19 @@ struct BNode {
   Box box;
   int32_t left = -1, right = -1;
   uint32_t start = 0, count = 0;  // leaf when count > 0
+  uint32_t span = 0;              // triangles of the subtree, at ref[start ..)
 };
+
+// Subtrees of at most this many triangles become one leaf of the wide tree
+// (the binary build's triangles of a subtree are contiguous in `ref`).  A
+// node visit costs several times a triangle test, so a wide node whose
+// children are two leaves of two triangles is better as one leaf of four.
+// Leaves hold at most 16 triangles (a 4-bit count).  0 keeps the binary
+// tree's leaves.
+#ifndef ARGENT_LEAF_MERGE
+#define ARGENT_LEAF_MERGE 0
+#endif
+static_assert(ARGENT_LEAF_MERGE <= 16, "wide-tree leaves hold at most 16 triangles");
 
 const int BINS = 16;
 const uint32_t MAX_LEAF = 4;
@@ -79,6 +91,7 @@ struct Builder {
     n.box = b;
     n.start = begin;
     n.count = end - begin;
+    n.span = end - begin;
   }
 
   // Returns the split position or `begin` when the range should be a leaf.
@@ -168,6 +181,8 @@ struct Builder {
     nodes[id].left = (int32_t)l;
     nodes[id].right = (int32_t)r;
     nodes[id].count = 0;
+    nodes[id].start = begin;
+    nodes[id].span = end - begin;
     if (end - begin >= PARALLEL_MIN && threads_left.fetch_sub(1) > 1) {
       std::thread t([&, l, begin, m, depth] { build(l, begin, m, depth + 1); });
       build(r, m, end, depth + 1);
@@ -229,11 +244,19 @@ struct Collapser {
     return r;
   }
 
+  // A binary node the wide tree stores as one leaf: a leaf, or a subtree
+  // small enough to merge.  The collapse first opens binary nodes (largest
+  // half-area first) until a wide node has eight children, so wide nodes
+  // stay full; an interior child still left then becomes a leaf if it is
+  // small enough, instead of a wide node of two or three small leaves.
+  static bool as_leaf(const BNode& n) { return n.count > 0 || n.span <= (uint32_t)ARGENT_LEAF_MERGE; }
+  static uint32_t leaf_count(const BNode& n) { return n.count > 0 ? n.count : n.span; }
+
   // Fills wide node `me` from binary node `root`; returns the depth below.
   uint32_t fill(uint32_t me, uint32_t root) {
     std::vector<uint32_t> kids;
     const BNode& r = bn[root];
-    if (r.count > 0)
+    if (as_leaf(r))
       kids.push_back(root);
     else {
       kids.push_back((uint32_t)r.left);
@@ -291,7 +314,7 @@ struct Collapser {
     w.ez = e[2];
     uint32_t n_interior = 0;
     for (uint32_t k : kids)
-      if (bn[k].count == 0) ++n_interior;
+      if (!as_leaf(bn[k])) ++n_interior;
     uint32_t child_base = (uint32_t)out.nodes.size();
     out.nodes.resize(out.nodes.size() + n_interior);
     w.child_base = child_base;
@@ -305,10 +328,11 @@ struct Collapser {
         if (!quant_hi(w.origin[a], k.box.hi[a], e[a], &qh)) throw std::runtime_error("quantisation failed");
         w.qhi[a][c] = qh;
       }
-      if (k.count > 0) {
-        if (k.count > 16) throw std::runtime_error("leaf larger than 16 triangles");
-        w.leaf_counts |= (k.count - 1) << (4 * c);
-        for (uint32_t i = k.start; i < k.start + k.count; ++i) out.tris.push_back(make_tri(ref[i]));
+      if (as_leaf(k)) {
+        uint32_t cnt = leaf_count(k);
+        if (cnt > 16) throw std::runtime_error("leaf larger than 16 triangles");
+        w.leaf_counts |= (cnt - 1) << (4 * c);
+        for (uint32_t i = k.start; i < k.start + cnt; ++i) out.tris.push_back(make_tri(ref[i]));
       } else {
         w.imask |= (uint8_t)(1u << c);
       }
@@ -316,7 +340,7 @@ struct Collapser {
     out.nodes[me] = w;
     uint32_t depth = 1, slot = 0;
     for (size_t c = 0; c < kids.size(); ++c) {
-      if (bn[kids[c]].count == 0) {
+      if (!as_leaf(bn[kids[c]])) {
         uint32_t d = 1 + fill(child_base + slot, kids[c]);
         depth = std::max(depth, d);
         ++slot;
