@@ -1130,8 +1130,9 @@ def reel_compare(args, device, steps=2):
     return out
 
 
-def north_star_extras(args, device):
-    """Short legs of the north-star comparison carried in the default line:
+def form_comparisons(args, device):
+    """Short legs comparing the batched and served forms with the plain
+    single-render path, carried in the default line:
     the batched reel against the plain single-render path, and a served
     Poisson trace against argent's one-job-at-a-time queue at a rate near
     the device's capacity."""
@@ -1205,7 +1206,7 @@ def main():
                 import gc
 
                 gc.collect()  # the still's context and its path state go before the extras' contexts
-                out["north_star"] = north_star_extras(args, local)
+                out["forms"] = form_comparisons(args, local)
             print(json.dumps(out), flush=True)
     finally:
         if world > 1:
