@@ -1087,7 +1087,7 @@ def ctx_wave_mb(args):
     return PATH_STATE_BYTES * (args.wave_paths or STILL_WAVE_PATHS) // 10 ** 6
 
 
-def reel_compare(args, device, steps=2):
+def reel_compare(args, device, steps=4):
     """The batched form against the plain single-render path on one frame
     of the batched workload (12 renders: 3 pieces x 4 alloys), both end to
     end with host buffers: the batch is one render_batch and then every
@@ -1115,18 +1115,24 @@ def reel_compare(args, device, steps=2):
             render_pass(ctx, *it)
             read(it[2], b)
 
-    out = {}
-    for name, fn in (("batched", batched), ("plain", plain)):
+    forms = (("batched", batched), ("plain", plain))
+    for _, fn in forms:
         fn(0)  # warm-up (graphs captured, buffers grown)
-        ctx.sync()
-        t0 = time.perf_counter()
-        for k in range(steps):
+    ctx.sync()
+    # The two forms alternate frame by frame, so a drift of the device's
+    # speed during the leg falls on both.
+    spent = {name: 0.0 for name, _ in forms}
+    for k in range(steps):
+        for name, fn in forms:
+            t0 = time.perf_counter()
             fn(1 + k)
-        dt = time.perf_counter() - t0
-        out[name] = {"e2e_path_samples_per_s": plan.path_samples * steps / dt, "s_per_frame": dt / steps}
+            spent[name] += time.perf_counter() - t0
+    out = {name: {"e2e_path_samples_per_s": plan.path_samples * steps / dt, "s_per_frame": dt / steps}
+           for name, dt in spent.items()}
     out["workload"] = plan.name
     out["renders_per_frame"] = plan.renders
-    out["timing"] = f"wall clock, {steps} turntable frames each, films read to host memory"
+    out["timing"] = (f"wall clock, {steps} turntable frames each, the forms alternating frame by frame, "
+                     f"films read to host memory")
     return out
 
 
@@ -1136,7 +1142,7 @@ def form_comparisons(args, device):
     the batched reel against the plain single-render path, and a served
     Poisson trace against argent's one-job-at-a-time queue at a rate near
     the device's capacity."""
-    out = {"reel": reel_compare(args, device)}
+    out = {"reel": reel_compare(args, device, args.extras_reel_frames)}
     import gc
 
     gc.collect()
@@ -1169,6 +1175,7 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="override spp (short profiling runs)")
     ap.add_argument("--no-extras", action="store_true",
                     help="signet_still: skip the short batched-vs-plain reel and served-vs-plain trace legs")
+    ap.add_argument("--extras-reel-frames", type=int, default=4)
     ap.add_argument("--extras-serve-rate", type=float, default=8.0)
     ap.add_argument("--extras-serve-seconds", type=float, default=30.0)
     ap.add_argument("--tune", action="store_true", help="apply (search and cache) a launch tuning")
