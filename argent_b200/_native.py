@@ -211,6 +211,7 @@ GPU_FUNCS = {
     "argent_ctx_kernel_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                                ctypes.POINTER(ctypes.c_uint64)]),
     "argent_ctx_set_graphs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "argent_ctx_set_ray_sharing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "argent_ctx_set_counting": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "argent_ctx_traversal_counts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
     "argent_ctx_bounce_counts": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),

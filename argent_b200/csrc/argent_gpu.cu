@@ -286,6 +286,8 @@ void argent_ctx_destroy(ArgentCtx* ctx) {
   prof_collect(ctx);
   for (cudaEvent_t e : ctx->prof.pool) cudaEventDestroy(e);
   for (int l = 0; l < ARGENT_LANES; ++l) ctx->wave[l].release();
+  for (auto& b : ctx->blobs) cudaFree(b.dev);
+  ctx->blobs.clear();
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->resolve) cudaFree(ctx->resolve);
   if (ctx->d_jobs_buf) cudaFree(ctx->d_jobs_buf);
@@ -1052,18 +1054,105 @@ static int ensure_wave(ArgentCtx* ctx, int lane, uint64_t cap) {
   return ARGENT_OK;
 }
 
+// Grows lane `lane`'s ray-sharing buffers to at least `cap` slots.
+static int ensure_share(ArgentCtx* ctx, int lane, uint64_t cap) {
+  WaveBuffers& w = ctx->wave[lane];
+  if (w.share_cap >= cap) return ARGENT_OK;
+  if (w.share_cap > 0) ARGENT_CK(ctx, cudaStreamSynchronize(ctx->lane_stream[lane]));
+  w.release_share();
+  auto alloc = [&](void** p, size_t bytes) -> bool {
+    if (cudaMalloc(p, bytes) != cudaSuccess) return false;
+    w.share_allocs.push_back(*p);
+    w.share_bytes += bytes;
+    w.bytes += bytes;
+    return true;
+  };
+  bool ok = alloc((void**)&w.lead, cap * sizeof(uint32_t)) && alloc((void**)&w.mark, cap * sizeof(uint32_t)) &&
+            alloc((void**)&w.shrec, cap * sizeof(uint2)) && alloc((void**)&w.vis, cap * sizeof(uint8_t)) &&
+            alloc((void**)&w.qt, cap * sizeof(uint32_t)) && alloc((void**)&w.qx, cap * sizeof(uint32_t)) &&
+            alloc((void**)&w.qst, cap * sizeof(uint32_t)) && alloc((void**)&w.qsx, cap * sizeof(uint32_t));
+  if (!ok) {
+    w.release_share();
+    return set_error(ctx, ARGENT_E_OOM, "ray-sharing buffers: out of device memory");
+  }
+  w.share_cap = cap;
+  return ARGENT_OK;
+}
+
 // ------------------------------------------------------------------ wave driver
 
 namespace {
 
-struct Chunk {
-  uint32_t job, p0, pn, s0, sn;
-};
+// True when two scenes give every ray the same closest hit and the same
+// visibility: the same piece (its BVH and triangle records), the same
+// turntable rotation, the same panels (as k_intersect tests them) and the
+// same floor plane.  Materials, lights' emission and the environment may
+// differ.
+bool same_geometry(const ArgentScene* a, const ArgentScene* b) {
+  if (a == b) return true;
+  const dev::DevScene &x = a->host, &y = b->host;
+  auto bits = [](float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, sizeof(u));
+    return u;
+  };
+  if (a->piece != b->piece || x.has_turn != y.has_turn) return false;
+  if (x.has_turn && (bits(x.to_obj_s) != bits(y.to_obj_s) || bits(x.to_obj_c) != bits(y.to_obj_c))) return false;
+  if (x.num_panels != y.num_panels || x.floor_enabled != y.floor_enabled) return false;
+  if (x.floor_enabled && bits(x.floor_y) != bits(y.floor_y)) return false;
+  for (int p = 0; p < x.num_panels; ++p) {
+    const dev::DevPanel &u = x.panels[p], &v = y.panels[p];
+    if (std::memcmp(u.c, v.c, sizeof(u.c)) || std::memcmp(u.hu, v.hu, sizeof(u.hu)) ||
+        std::memcmp(u.hv, v.hv, sizeof(u.hv)) || std::memcmp(u.n, v.n, sizeof(u.n)) ||
+        bits(u.hu_l2) != bits(v.hu_l2) || bits(u.hv_l2) != bits(v.hv_l2) || u.camera_visible != v.camera_visible)
+      return false;
+  }
+  return true;
+}
 
-// Splits every job into (pixel range, sample range) chunks of at most
-// `cap` paths and packs them, in order, into waves.
+// True when the traversal kernels may take scene `b`'s paths as `a`'s: the
+// same geometry and the same shading class for every material slot and the
+// floor (what k_intersect reads from a wave's one scene).
+bool same_traversal(const ArgentScene* a, const ArgentScene* b) {
+  return a == b || (same_geometry(a, b) && a->host.floor_class == b->host.floor_class &&
+                    std::memcmp(a->host.mat_class, b->host.mat_class, sizeof(a->host.mat_class)) == 0);
+}
+
+// Groups of jobs that trace the same rays: the same film size, samples,
+// seed and camera over the same geometry.  With sharing off, or for a job
+// with no partner, a group is the job alone.  Groups are listed in the order
+// of their first jobs, at most 16 jobs each.
+std::vector<std::vector<uint32_t>> plan_groups(bool share, const std::vector<dev::DevJob>& jobs,
+                                               const std::vector<uint32_t>& counts,
+                                               const std::vector<const ArgentScene*>& scenes) {
+  std::vector<std::vector<uint32_t>> groups;
+  std::vector<bool> taken(jobs.size(), false);
+  for (uint32_t j = 0; j < jobs.size(); ++j) {
+    if (taken[j]) continue;
+    taken[j] = true;
+    groups.push_back({j});
+    if (!share) continue;
+    const dev::DevJob& a = jobs[j];
+    for (uint32_t i = j + 1; i < jobs.size() && groups.back().size() < 16; ++i) {
+      const dev::DevJob& b = jobs[i];
+      if (taken[i] || b.w != a.w || b.h != a.h || b.first != a.first || b.seed_h != a.seed_h ||
+          counts[i] != counts[j] || std::memcmp(&a.cam, &b.cam, sizeof(a.cam)) != 0 ||
+          !same_geometry(scenes[j], scenes[i]))
+        continue;
+      taken[i] = true;
+      groups.back().push_back(i);
+    }
+  }
+  return groups;
+}
+
+// Splits every group of jobs into (pixel range, sample range) chunks of at
+// most `cap` paths and packs them, in order, into waves.  A group of k jobs
+// takes k segments with the same pixels and samples per chunk, side by side,
+// the first leading the others.
 std::vector<dev::WaveDesc> plan_waves(const std::vector<dev::DevJob>& jobs, const std::vector<uint32_t>& counts,
-                                      uint64_t cap, std::vector<uint32_t>* wave_depth) {
+                                      const std::vector<std::vector<uint32_t>>& groups, uint64_t cap,
+                                      std::vector<uint32_t>* wave_depth) {
   std::vector<dev::WaveDesc> waves;
   dev::WaveDesc cur{};
   uint32_t cur_depth = 0;
@@ -1075,30 +1164,38 @@ std::vector<dev::WaveDesc> plan_waves(const std::vector<dev::DevJob>& jobs, cons
     cur = dev::WaveDesc{};
     cur_depth = 0;
   };
-  for (uint32_t j = 0; j < jobs.size(); ++j) {
-    uint32_t P = jobs[j].w * jobs[j].h;
-    uint32_t count = counts[j];
+  for (const std::vector<uint32_t>& g : groups) {
+    const uint32_t j0 = g[0];
+    const uint64_t k = g.size();
+    uint32_t P = jobs[j0].w * jobs[j0].h;
+    uint32_t count = counts[j0];
     if (P == 0 || count == 0) continue;
-    uint32_t pn_max = (uint32_t)std::min<uint64_t>(P, cap);
+    uint32_t depth = 0;
+    for (uint32_t j : g) depth = std::max(depth, jobs[j].max_depth);
+    uint32_t pn_max = (uint32_t)std::min<uint64_t>(P, cap / k);
     for (uint32_t p0 = 0; p0 < P; p0 += pn_max) {
       uint32_t pn = std::min(pn_max, P - p0);
       uint32_t s0 = 0;
       while (s0 < count) {
         uint64_t room = cap - cur.num_slots;
-        if (room < pn || cur.num_segments == ARGENT_MAX_SEGMENTS) {
+        if (room < k * pn || cur.num_segments + k > ARGENT_MAX_SEGMENTS) {
           flush();
           room = cap;
         }
-        uint32_t sn = (uint32_t)std::min<uint64_t>(count - s0, room / pn);
-        dev::DevSegment& sg = cur.seg[cur.num_segments++];
-        sg.slot_begin = cur.num_slots;
-        sg.job = j;
-        sg.p0 = p0;
-        sg.pn = pn;
-        sg.s0 = s0;
-        sg.sn = sn;
-        cur.num_slots += pn * sn;
-        cur_depth = std::max(cur_depth, jobs[j].max_depth);
+        uint32_t sn = (uint32_t)std::min<uint64_t>(count - s0, room / (k * pn));
+        const uint32_t lead = cur.num_slots;
+        for (uint64_t m = 0; m < k; ++m) {
+          dev::DevSegment& sg = cur.seg[cur.num_segments++];
+          sg.slot_begin = cur.num_slots;
+          sg.job = g[m];
+          sg.p0 = p0;
+          sg.pn = pn;
+          sg.s0 = s0;
+          sg.sn = sn;
+          sg.lead = m == 0 ? ~0u : lead;
+          cur.num_slots += pn * sn;
+        }
+        cur_depth = std::max(cur_depth, depth);
         s0 += sn;
       }
     }
@@ -1166,7 +1263,8 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   for (size_t j = 0; j < jobs.size(); ++j) total += (uint64_t)jobs[j].w * jobs[j].h * counts[j];
   uint32_t cap = (uint32_t)std::min<uint64_t>(ctx->limits.wave_paths, std::max<uint64_t>(total, 1u << 16));
   std::vector<uint32_t> depths;
-  std::vector<dev::WaveDesc> waves = plan_waves(jobs, counts, cap, &depths);
+  std::vector<dev::WaveDesc> waves =
+      plan_waves(jobs, counts, plan_groups(ctx->share_rays, jobs, counts, job_scenes), cap, &depths);
   if (waves.empty()) return ARGENT_OK;
   rc = ensure_lane_streams(ctx, ctx->lanes);
   if (rc != ARGENT_OK) return rc;
@@ -1176,6 +1274,16 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   for (int k = 0; k < used; ++k) {
     rc = ensure_wave(ctx, (start + k) % nlanes, cap);
     if (rc != ARGENT_OK) return rc;
+  }
+  // Waves whose segments share rays, and their lanes' sharing buffers.
+  std::vector<uint8_t> wshare(waves.size(), 0);
+  for (size_t wi = 0; wi < waves.size(); ++wi) {
+    for (uint32_t sgi = 0; sgi < waves[wi].num_segments; ++sgi)
+      if (waves[wi].seg[sgi].lead != ~0u) wshare[wi] = 1;
+    if (wshare[wi]) {
+      rc = ensure_share(ctx, (int)((start + wi) % nlanes), cap);
+      if (rc != ARGENT_OK) return rc;
+    }
   }
   // Joined batches (done == null) read their job records from a buffer the
   // context keeps; overlapped ones from their own, freed when they finish.
@@ -1236,9 +1344,11 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   int g_any[2] = {tuned_grid(grid_for(ctx, (const void*)dev::k_shadow<false>, 128, cap), ctx->trace_bpsm),
                   tuned_grid(grid_for(ctx, (const void*)dev::k_shadow<true>, 128, cap), ctx->trace_bpsm)};
   int g_film = grid_for(ctx, (const void*)dev::k_film, 256, cap);
+  int g_split = grid_for(ctx, (const void*)dev::k_share_split, 256, cap);
   // Per wave: its classes, whether any of its scenes has an env map (the
-  // shading kernels without one leave the map code out) and, for a one-scene
-  // wave, that scene.
+  // shading kernels without one leave the map code out) and, when its scenes
+  // all trace alike (one scene, or metal variants of one: same_traversal),
+  // the first of them for the traversal kernels' uniform form.
   std::vector<uint32_t> wclasses(waves.size()), wmap(waves.size());
   std::vector<const ArgentScene*> wone(waves.size());
   for (size_t wi = 0; wi < waves.size(); ++wi) {
@@ -1249,7 +1359,7 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
       const ArgentScene* sc = job_scenes[w.seg[sgi].job];
       classes |= sc->host.class_mask;
       if (sc->host.env_is_map) map = 1;
-      if (sc != one) one = nullptr;
+      if (one && !same_traversal(one, sc)) one = nullptr;
     }
     wclasses[wi] = classes;
     wmap[wi] = map;
@@ -1303,6 +1413,15 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
       a.u_to_obj_c = one ? one->host.to_obj_c : 1.0f;
       a.q_in = wb.q0;
       a.q_out = wb.q1;
+      const bool shared = wshare[wi] != 0;
+      a.lead = shared ? wb.lead : nullptr;
+      a.mark = shared ? wb.mark : nullptr;
+      a.shrec = shared ? wb.shrec : nullptr;
+      a.vis = shared ? wb.vis : nullptr;
+      a.qt = shared ? wb.qt : nullptr;
+      a.qx = shared ? wb.qx : nullptr;
+      a.qst = shared ? wb.qst : nullptr;
+      a.qsx = shared ? wb.qsx : nullptr;
       {
         ProfScope ps(ctx, KC_RAYGEN, st);
         dev::k_raygen<<<g_ray, 256, 0, st>>>(a, w);
@@ -1314,10 +1433,21 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
         a.q_out = (depth & 1) ? wb.q0 : wb.q1;
         {
           ProfScope ps(ctx, KC_INTERSECT, st);
+          if (shared) {
+            dev::k_share_split<<<g_split, 256, 0, st>>>(a, (int)depth);
+            ++*kernels;
+          }
           if (uni)
             dev::k_intersect<true><<<g_int[1], 128, 0, st>>>(a, (int)depth);
           else
             dev::k_intersect<false><<<g_int[0], 128, 0, st>>>(a, (int)depth);
+          if (shared) {
+            if (uni)
+              dev::k_hit_copy<true><<<g_split, 256, 0, st>>>(a, (int)depth);
+            else
+              dev::k_hit_copy<false><<<g_split, 256, 0, st>>>(a, (int)depth);
+            ++*kernels;
+          }
         }
         launched(e, "k_intersect");
         {
@@ -1348,10 +1478,18 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
         launched(e, "k_shade");
         {
           ProfScope ps(ctx, KC_SHADOW, st);
+          if (shared) {
+            dev::k_shadow_split<<<g_split, 256, 0, st>>>(a, (int)depth);
+            ++*kernels;
+          }
           if (uni)
             dev::k_shadow<true><<<g_any[1], 128, 0, st>>>(a, (int)depth);
           else
             dev::k_shadow<false><<<g_any[0], 128, 0, st>>>(a, (int)depth);
+          if (shared) {
+            dev::k_shadow_copy<<<g_split, 256, 0, st>>>(a, (int)depth);
+            ++*kernels;
+          }
         }
         launched(e, "k_shadow");
         *kernels += 2;
@@ -1403,7 +1541,12 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
     put(g_any, sizeof(g_any));
     put(g_sh, sizeof(g_sh));
     put(&d_jobs, sizeof(d_jobs));
-    for (int k = 0; k < used; ++k) put(&args[(start + k) % nlanes], sizeof(dev::WaveArgs));
+    for (int k = 0; k < used; ++k) {
+      put(&args[(start + k) % nlanes], sizeof(dev::WaveArgs));
+      const WaveBuffers& wb = ctx->wave[(start + k) % nlanes];
+      const void* sp[8] = {wb.lead, wb.mark, wb.shrec, wb.vis, wb.qt, wb.qx, wb.qst, wb.qsx};
+      put(sp, sizeof(sp));
+    }
     for (size_t wi = 0; wi < waves.size(); ++wi) {
       const dev::WaveDesc& w = waves[wi];
       put(&w.num_segments, sizeof(w.num_segments));
@@ -1479,11 +1622,65 @@ extern "C" {
 
 // ------------------------------------------------------------------ scene
 
+// 64-bit hash of a byte string, eight bytes at a time (a multiply-xorshift
+// mix per word); equal hashes are confirmed by comparing the bytes.
+static uint64_t blob_hash(const void* src, size_t bytes) {
+  const uint8_t* p = (const uint8_t*)src;
+  uint64_t h = 0x9e3779b97f4a7c15ull ^ bytes;
+  size_t i = 0;
+  for (; i + 8 <= bytes; i += 8) {
+    uint64_t w;
+    std::memcpy(&w, p + i, 8);
+    h = (h ^ w) * 0xff51afd7ed558ccdull;
+    h ^= h >> 32;
+  }
+  for (; i < bytes; ++i) h = (h ^ p[i]) * 0x100000001b3ull;
+  return h;
+}
+
+// The device copy of `bytes` bytes equal to `src`: an existing blob of the
+// same content gains a holder, or a new one is uploaded.  The pointer is
+// added to `held`; null when the device is out of memory.
+static void* intern_blob(ArgentCtx* ctx, const void* src, size_t bytes, std::vector<void*>* held) {
+  uint64_t h = blob_hash(src, bytes);
+  for (auto& b : ctx->blobs) {
+    if (b.hash == h && b.host.size() == bytes && std::memcmp(b.host.data(), src, bytes) == 0) {
+      ++b.refs;
+      held->push_back(b.dev);
+      return b.dev;
+    }
+  }
+  ArgentCtx::SharedBlob b;
+  if (cudaMalloc(&b.dev, bytes) != cudaSuccess) return nullptr;
+  if (cudaMemcpy(b.dev, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(b.dev);
+    return nullptr;
+  }
+  b.hash = h;
+  b.host.assign((const uint8_t*)src, (const uint8_t*)src + bytes);
+  b.refs = 1;
+  ctx->blobs.push_back(std::move(b));
+  held->push_back(ctx->blobs.back().dev);
+  return ctx->blobs.back().dev;
+}
+
+static void release_blob(ArgentCtx* ctx, void* dev) {
+  for (size_t i = 0; i < ctx->blobs.size(); ++i) {
+    if (ctx->blobs[i].dev != dev) continue;
+    if (--ctx->blobs[i].refs == 0) {
+      cudaFree(dev);
+      ctx->blobs.erase(ctx->blobs.begin() + (long)i);
+    }
+    return;
+  }
+}
+
 void argent_scene_destroy(ArgentScene* s) {
   if (!s) return;
   cudaSetDevice(s->ctx->device);
   cudaStreamSynchronize(s->ctx->stream);
   for (void* a : s->allocs) cudaFree(a);
+  for (void* b : s->shared) release_blob(s->ctx, b);
   if (s->staged) cudaFreeHost(s->staged);
   if (s->staged_ev) cudaEventDestroy(s->staged_ev);
   delete s;
@@ -1539,6 +1736,8 @@ int argent_scene_upload(ArgentCtx* ctx, ArgentPiece* piece, const ArgentSceneDes
     if (cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
     return d;
   };
+  // Data that other scenes of the context may hold too: one device copy.
+  auto share = [&](const void* src, size_t bytes) -> void* { return intern_blob(ctx, src, bytes, &s->shared); };
   bool ok = true;
   h.mats = (const ArgentMaterial*)up(desc->materials, sizeof(ArgentMaterial) * desc->num_materials);
   ok = ok && h.mats;
@@ -1556,7 +1755,7 @@ int argent_scene_upload(ArgentCtx* ctx, ArgentPiece* piece, const ArgentSceneDes
     dp.feather = p.feather;
     dp.emits = p.emits ? 1 : 0;
     dp.camera_visible = p.camera_visible ? 1 : 0;
-    dp.emission = p.emits ? (const float*)up(p.emission, sizeof(float) * ARGENT_SPEC_LEN) : nullptr;
+    dp.emission = p.emits ? (const float*)share(p.emission, sizeof(float) * ARGENT_SPEC_LEN) : nullptr;
     ok = ok && (!p.emits || dp.emission);
   }
   argent::LightTable lt = argent::build_lights(*desc);
@@ -1574,10 +1773,10 @@ int argent_scene_upload(ArgentCtx* ctx, ArgentPiece* piece, const ArgentSceneDes
     h.env_is_map = 1;
     h.map_w = env->width;
     h.map_h = env->height;
-    h.map_weights = (const float*)up(et.weights.data(), et.weights.size() * sizeof(float));
-    h.map_cond = (const float*)up(et.conditional.data(), et.conditional.size() * sizeof(float));
-    h.map_marg = (const float*)up(et.marginal.data(), et.marginal.size() * sizeof(float));
-    h.lin_basis = (const float*)up(basis, sizeof(basis));
+    h.map_weights = (const float*)share(et.weights.data(), et.weights.size() * sizeof(float));
+    h.map_cond = (const float*)share(et.conditional.data(), et.conditional.size() * sizeof(float));
+    h.map_marg = (const float*)share(et.marginal.data(), et.marginal.size() * sizeof(float));
+    h.lin_basis = (const float*)share(basis, sizeof(basis));
     ok = ok && h.map_weights && h.map_cond && h.map_marg && h.lin_basis;
     float r_l = (-env->rotation_deg) * (3.14159265358979323846f / 180.0f);
     float r_w = env->rotation_deg * (3.14159265358979323846f / 180.0f);
@@ -1588,9 +1787,9 @@ int argent_scene_upload(ArgentCtx* ctx, ArgentPiece* piece, const ArgentSceneDes
   } else {
     h.env_is_map = 0;
     h.env_power = env ? env->power : 1.0f;
-    h.env_top = (const float*)up(env ? env->top : zeros, sizeof(float) * ARGENT_SPEC_LEN);
-    h.env_horizon = (const float*)up(env ? env->horizon : zeros, sizeof(float) * ARGENT_SPEC_LEN);
-    h.env_bottom = (const float*)up(env ? env->bottom : zeros, sizeof(float) * ARGENT_SPEC_LEN);
+    h.env_top = (const float*)share(env ? env->top : zeros, sizeof(float) * ARGENT_SPEC_LEN);
+    h.env_horizon = (const float*)share(env ? env->horizon : zeros, sizeof(float) * ARGENT_SPEC_LEN);
+    h.env_bottom = (const float*)share(env ? env->bottom : zeros, sizeof(float) * ARGENT_SPEC_LEN);
     ok = ok && h.env_top && h.env_horizon && h.env_bottom;
   }
   h.floor_enabled = desc->floor.enabled ? 1 : 0;
@@ -2259,6 +2458,12 @@ int argent_ctx_set_graphs(ArgentCtx* ctx, int on) {
     for (auto& g : ctx->graph_cache) cudaGraphExecDestroy(g.exec);
     ctx->graph_cache.clear();
   }
+  return ARGENT_OK;
+}
+
+int argent_ctx_set_ray_sharing(ArgentCtx* ctx, int on) {
+  if (!ctx) return set_error(nullptr, ARGENT_E_INVALID, "ctx is NULL");
+  ctx->share_rays = on != 0;
   return ARGENT_OK;
 }
 

@@ -84,8 +84,13 @@ struct DevJob {
 
 // A contiguous run of path slots in a wave: pixels [p0, p0+pn) of job
 // `job`, samples first+s0 .. first+s0+sn-1; slot = slot_begin + k*pn + p.
+// With ray sharing, the segments of jobs that trace the same rays (same
+// piece, camera, seed and samples; other materials) follow each other with
+// the same pixels and samples, and `lead` is the first such segment's
+// slot_begin (the slot of the same pixel-sample there is lead + k*pn + p);
+// ~0u when the segment leads or shares nothing.
 struct DevSegment {
-  uint32_t slot_begin, job, p0, pn, s0, sn;
+  uint32_t slot_begin, job, p0, pn, s0, sn, lead;
 };
 
 #define ARGENT_MAX_SEGMENTS 64
@@ -109,9 +114,31 @@ struct WaveBuffers {
   uint32_t* counters = nullptr;
   std::vector<void*> allocs;
   uint64_t bytes = 0;
+  // Ray sharing (allocated on the first wave that shares rays): per slot its
+  // leader's slot, the depth + 1 it is alive at, and its shadow record of
+  // the current depth (position, depth + 1); per shadow record whether it
+  // reached its light; the queues of rays to trace and of rays that take
+  // their leader's result, for closest hits and for shadow rays.
+  uint64_t share_cap = 0, share_bytes = 0;
+  uint32_t *lead = nullptr, *mark = nullptr;
+  uint2* shrec = nullptr;
+  uint8_t* vis = nullptr;
+  uint32_t *qt = nullptr, *qx = nullptr, *qst = nullptr, *qsx = nullptr;
+  std::vector<void*> share_allocs;
+  void release_share() {
+    for (void* a : share_allocs) cudaFree(a);
+    share_allocs.clear();
+    lead = mark = qt = qx = qst = qsx = nullptr;
+    shrec = nullptr;
+    vis = nullptr;
+    share_cap = 0;
+    bytes -= share_bytes;
+    share_bytes = 0;
+  }
   void release() {
     for (void* a : allocs) cudaFree(a);
     allocs.clear();
+    release_share();
     cap = 0;
     bytes = 0;
   }
@@ -165,6 +192,21 @@ struct ArgentCtx {
   std::vector<GraphEntry> graph_cache;
   uint64_t graph_clock = 0;
   bool graphs_on = true;
+  // Batches trace the rays that renders have in common once
+  // (argent_ctx_set_ray_sharing).
+  bool share_rays = false;
+  // Scene data uploaded once per distinct content (environment maps and
+  // their sampling tables, emission and sky spectra), shared by the scenes
+  // that hold it and freed with the last of them: metal variants of one
+  // studio then read one copy, which keeps one map in L2 instead of one per
+  // scene.
+  struct SharedBlob {
+    uint64_t hash = 0;
+    std::vector<uint8_t> host;
+    void* dev = nullptr;
+    int refs = 0;
+  };
+  std::vector<SharedBlob> blobs;
   int num_sms = 148;
   int lanes = 8;
   // Launch tuning (argent_ctx_set_tuning / argent_autotune); 0 = default.
@@ -204,6 +246,7 @@ struct ArgentScene {
   dev::DevScene host{};           // host copy of the device descriptor
   dev::DevScene* d_scene = nullptr;
   std::vector<void*> allocs;
+  std::vector<void*> shared;  // blobs held in ctx->blobs
   uint64_t bytes = 0;
   float cam_m[9];
   // Pinned staging copy for stream-ordered descriptor updates (turntable),

@@ -258,6 +258,16 @@ struct WaveArgs {
   DevPiece upiece;
   int32_t u_has_turn;
   float u_to_obj_s, u_to_obj_c;
+  // Ray sharing, for a wave whose segments share rays (null otherwise): per
+  // slot its leader's slot (~0u for none) and the depth + 1 it is alive at;
+  // per slot its shadow record of the current depth (position, depth + 1);
+  // per shadow record whether it reached its light; the queues of closest
+  // rays to trace (qt) and to take from their leader (qx), and the same for
+  // shadow records (qst, qsx).
+  uint32_t *lead, *mark;
+  uint2* shrec;
+  uint8_t* vis;
+  uint32_t *qt, *qx, *qst, *qsx;
 };
 
 // Queue counters of one wave: active paths per bounce, shade-queue lengths
@@ -266,7 +276,13 @@ struct WaveArgs {
 #define CNT_ACT(d) (d)
 #define CNT_CLS(d, c) ((ARGENT_MAX_DEPTH + 2) + (d) * NUM_CLS + (c))
 #define CNT_SH(d) ((ARGENT_MAX_DEPTH + 2) * (1 + NUM_CLS) + (d))
-#define CNT_QUEUES ((ARGENT_MAX_DEPTH + 2) * (2 + NUM_CLS))
+// Ray sharing: closest rays to trace and to take from their leaders, shadow
+// records to trace and to take from their leaders.
+#define CNT_TR(d) ((ARGENT_MAX_DEPTH + 2) * (2 + NUM_CLS) + (d))
+#define CNT_CP(d) ((ARGENT_MAX_DEPTH + 2) * (3 + NUM_CLS) + (d))
+#define CNT_STR(d) ((ARGENT_MAX_DEPTH + 2) * (4 + NUM_CLS) + (d))
+#define CNT_SCP(d) ((ARGENT_MAX_DEPTH + 2) * (5 + NUM_CLS) + (d))
+#define CNT_QUEUES ((ARGENT_MAX_DEPTH + 2) * (6 + NUM_CLS))
 #define CNT_WORK(q) (CNT_QUEUES + (q))
 #define CNT_TOTAL (2 * CNT_QUEUES)
 
@@ -323,6 +339,11 @@ __global__ void __launch_bounds__(256) k_raygen(WaveArgs a, WaveDesc w) {
     uint32_t pix = sg.p0 + k % sg.pn;
     uint32_t si = job.first + sg.s0 + k / sg.pn;
     uint32_t x = pix % job.w, y = pix / job.w;
+    if (a.lead) {
+      a.lead[slot] = sg.lead == ~0u ? ~0u : sg.lead + k;
+      a.mark[slot] = 1u;  // alive at depth 0
+      a.shrec[slot] = make_uint2(0u, 0u);  // no shadow record yet
+    }
     uint32_t pix_seed = hash32((y * job.w + x) ^ job.seed_h);
     Sampler s;
     s.init(pix_seed, si);
@@ -383,7 +404,8 @@ __device__ __forceinline__ void warp_append(bool pred, uint32_t value, uint32_t*
 // own).  The record is written where it is built, so its twelve values are
 // not held through the continuation sample.  The order of the records in the
 // queue does not matter: each adds to its own path's radiance.
-__device__ __forceinline__ void push_shadow(const WaveArgs& a, int depth, float4 o, float4 d, float4 c) {
+__device__ __forceinline__ void push_shadow(const WaveArgs& a, int depth, uint32_t slot, float4 o, float4 d,
+                                            float4 c) {
   unsigned m = __activemask();
   int lane = threadIdx.x & 31;
   int leader = __ffs(m) - 1;
@@ -395,6 +417,7 @@ __device__ __forceinline__ void push_shadow(const WaveArgs& a, int depth, float4
     a.sh_o[pos] = o;
     a.sh_d[pos] = d;
     a.sh_c[pos] = c;
+    if (a.shrec) a.shrec[slot] = make_uint2(pos, (uint32_t)depth + 1u);
   } else {
     atomicOr(a.status, ARGENT_STATUS_QUEUE_OVERFLOW);
   }
@@ -473,8 +496,12 @@ __device__ __forceinline__ uint32_t lane_refill(bool idle, bool* first, bool* mo
 
 template <bool U>
 __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_intersect(WaveArgs a, int depth) {
-  const uint32_t count = a.counters[CNT_ACT(depth)];
-  uint32_t* work = a.counters + CNT_WORK(CNT_ACT(depth));
+  // With ray sharing, the rays that take their leader's hit are left out
+  // (k_share_split) and the rest come from the trace queue.
+  const uint32_t cq = a.lead ? CNT_TR(depth) : CNT_ACT(depth);
+  const uint32_t count = a.counters[cq];
+  uint32_t* work = a.counters + CNT_WORK(cq);
+  const uint32_t* qin = a.lead ? a.qt : a.q_in;
   ARGENT_CLOSEST_STACK(stack);
   ClosestTrav s;
   const DevScene* sc = U ? a.uscene : nullptr;
@@ -483,7 +510,7 @@ __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_intersect(WaveArgs 
   for (;;) {
     uint32_t j = lane_refill(!active, &first, &more, count, work);
     if (j != ~0u) {
-      slot = a.q_in[j];
+      slot = qin[j];
       if (!U) sc = a.jobs[a.meta[slot].w >> 16].scene;
       float4 of = a.o[slot], df = a.d[slot];
       V3 oo{of.x, of.y, of.z}, od{df.x, df.y, df.z};
@@ -849,7 +876,7 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
               float4 so = make_float4(oo.x, oo.y, oo.z, t_max);
               float4 sd = make_float4(od.x, od.y, od.z, __uint_as_float(slot));
               if constexpr (InlineShadow<CLS>::value) {
-                push_shadow(a, depth, so, sd, to_f4(c));
+                push_shadow(a, depth, slot, so, sd, to_f4(c));
               } else {
                 out.shadow = true;
                 out.sh_o = so;
@@ -969,6 +996,7 @@ __global__ void __launch_bounds__(128, CLS == CLS_TERMINAL      ? 1
       r = shade_path<CLS, MAP>(a, slot, depth);
     }
     warp_append(r.alive, slot, next_counter, a.q_out, cap, a.status);
+    if (a.mark && r.alive) a.mark[slot] = (uint32_t)depth + 2u;  // alive at depth + 1
     if constexpr (!InlineShadow<CLS>::value) {
       // Shadow rays: the record is written at the queue position.
       unsigned m = __ballot_sync(0xffffffffu, r.shadow);
@@ -984,6 +1012,7 @@ __global__ void __launch_bounds__(128, CLS == CLS_TERMINAL      ? 1
             a.sh_o[pos] = r.sh_o;
             a.sh_d[pos] = r.sh_d;
             a.sh_c[pos] = r.sh_c;
+            if (a.shrec) a.shrec[slot] = make_uint2(pos, (uint32_t)depth + 1u);
           } else {
             atomicOr(a.status, ARGENT_STATUS_QUEUE_OVERFLOW);
           }
@@ -999,8 +1028,12 @@ __global__ void __launch_bounds__(128, CLS == CLS_TERMINAL      ? 1
 // slowest ray of its warp ends.
 template <bool U>
 __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_shadow(WaveArgs a, int depth) {
-  const uint32_t count = a.counters[CNT_SH(depth)];
-  uint32_t* work = a.counters + CNT_WORK(CNT_SH(depth));
+  // With ray sharing, the records that take their leader's visibility are
+  // left out (k_shadow_split) and the rest come through the trace queue;
+  // each traced record's visibility is kept for its followers.
+  const uint32_t cq = a.lead ? CNT_STR(depth) : CNT_SH(depth);
+  const uint32_t count = a.counters[cq];
+  uint32_t* work = a.counters + CNT_WORK(cq);
   ARGENT_ANY_STACK(stack);
   AnyTrav s;
   const DevScene* sc = nullptr;
@@ -1010,8 +1043,8 @@ __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_shadow(WaveArgs a, 
   for (;;) {
     uint32_t j = lane_refill(!active, &first, &more, count, work);
     if (j != ~0u) {
-      idx = j;
-      float4 so = __ldcs(a.sh_o + j), sd = __ldcs(a.sh_d + j);
+      idx = a.lead ? a.qst[j] : j;
+      float4 so = __ldcs(a.sh_o + idx), sd = __ldcs(a.sh_d + idx);
       if (!U) sc = a.jobs[a.meta[__float_as_uint(sd.w)].w >> 16].scene;
       state = any_begin(U ? a.upiece : sc->piece, s, stack, V3{so.x, so.y, so.z}, V3{sd.x, sd.y, sd.z}, so.w);
       active = true;
@@ -1027,6 +1060,7 @@ __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_shadow(WaveArgs a, 
     }
     if (active && state != ARGENT_ANY_RUNNING) {
       count_visits(3, s.n_nodes, s.n_tris);
+      if (a.vis) a.vis[idx] = state == ARGENT_ANY_CLEAR ? 1u : 0u;
       if (state == ARGENT_ANY_CLEAR) {
         uint32_t slot = __float_as_uint(__ldcs(a.sh_d + idx).w);
         float4 c = __ldcs(a.sh_c + idx);
@@ -1034,6 +1068,151 @@ __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_shadow(WaveArgs a, 
         a.L[slot] = make_float4(l.x + c.x, l.y + c.y, l.z + c.z, l.w + c.w);
       }
       active = false;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- ray sharing
+// Renders of one batch that differ only in their materials (metal variants
+// of a piece under the same camera, seed and samples) trace the same rays
+// until their paths part (a different sampled lobe, Russian roulette on a
+// different throughput).  Their segments sit side by side in a wave; before
+// each traversal a path whose leader (the same pixel-sample of the first
+// render) is alive with a bit-identical ray takes the leader's result, so
+// every shared ray is traced once.  Identical rays in identical geometry
+// have identical closest hits and identical visibility, so the records and
+// films equal those of tracing every ray.
+
+__device__ __forceinline__ bool same_bits3(float4 a, float4 b) {
+  return __float_as_uint(a.x) == __float_as_uint(b.x) && __float_as_uint(a.y) == __float_as_uint(b.y) &&
+         __float_as_uint(a.z) == __float_as_uint(b.z);
+}
+
+// Shading class of a hit record, for a path of scene `sc` (the classes
+// k_intersect gives: miss and panels terminal, the floor's material class,
+// the hit triangle's material class).
+__device__ __forceinline__ int hit_class(const DevScene* sc, const DevPiece& pc, float4 rec) {
+  uint32_t kind = __float_as_uint(rec.w);
+  if (kind == HIT_FLOOR) return sc->floor_class;
+  if (kind >= HIT_PANEL) return CLS_TERMINAL;
+  return sc->mat_class[__ldg(&pc.tri_idx[kind].w)];
+}
+
+// Block-aggregated queue append for the streaming passes below: one atomic
+// per block and queue instead of one per warp (a pass over tens of millions
+// of entries is otherwise bound by the atomics on one counter).  Every
+// thread of the block must call it; `sw` is the block's scratch of
+// blockDim.x / 32 + 1 words.
+__device__ __forceinline__ void block_append(bool pred, uint32_t value, uint32_t* counter, uint32_t* queue,
+                                             uint32_t cap, uint32_t* status, uint32_t* sw) {
+  const unsigned m = __ballot_sync(0xffffffffu, pred);
+  const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nw = blockDim.x >> 5;
+  if (lane == 0) sw[warp] = (uint32_t)__popc(m);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t total = 0;
+    for (unsigned w = 0; w < nw; ++w) {
+      uint32_t c = sw[w];
+      sw[w] = total;
+      total += c;
+    }
+    sw[nw] = total ? atomicAdd(counter, total) : 0u;
+  }
+  __syncthreads();
+  if (pred) {
+    uint32_t pos = sw[nw] + sw[warp] + (uint32_t)__popc(m & ((1u << lane) - 1u));
+    if (pos < cap)
+      queue[pos] = value;
+    else
+      atomicOr(status, ARGENT_STATUS_QUEUE_OVERFLOW);
+  }
+  __syncthreads();  // sw is reused by the next append
+}
+
+// Before k_intersect: splits the alive paths of `depth` into those that take
+// their leader's hit (qx) and those to trace (qt).
+__global__ void __launch_bounds__(256) k_share_split(WaveArgs a, int depth) {
+  __shared__ uint32_t sw[256 / 32 + 1];
+  const uint32_t count = min(a.counters[CNT_ACT(depth)], a.cap);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += stride) {
+    uint32_t i = base + threadIdx.x;
+    bool valid = i < count, share = false;
+    uint32_t slot = 0;
+    if (valid) {
+      slot = a.q_in[i];
+      uint32_t ld = a.lead[slot];
+      if (ld != ~0u && a.mark[ld] == (uint32_t)depth + 1u)
+        share = same_bits3(a.o[slot], a.o[ld]) && same_bits3(a.d[slot], a.d[ld]);
+    }
+    block_append(valid && share, slot, a.counters + CNT_CP(depth), a.qx, a.cap, a.status, sw);
+    block_append(valid && !share, slot, a.counters + CNT_TR(depth), a.qt, a.cap, a.status, sw);
+  }
+}
+
+// After k_intersect: the paths of qx take their leaders' hit records and
+// join the shade queue of their own material's class.
+template <bool U>
+__global__ void __launch_bounds__(256) k_hit_copy(WaveArgs a, int depth) {
+  __shared__ uint32_t sw[256 / 32 + 1];
+  const uint32_t count = min(a.counters[CNT_CP(depth)], a.cap);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += stride) {
+    uint32_t i = base + threadIdx.x;
+    int cls = -1;
+    uint32_t slot = 0;
+    if (i < count) {
+      slot = a.qx[i];
+      float4 rec = a.hit[a.lead[slot]];
+      a.hit[slot] = rec;
+      const DevScene* sc = U ? a.uscene : a.jobs[a.meta[slot].w >> 16].scene;
+      cls = hit_class(sc, U ? a.upiece : sc->piece, rec);
+    }
+    for (int c = 0; c < NUM_CLS; ++c)
+      if (__syncthreads_or(cls == c))
+        block_append(cls == c, slot, a.counters + CNT_CLS(depth, c), a.qc + (size_t)c * a.cap, a.cap, a.status,
+                     sw);
+  }
+}
+
+// Before k_shadow: a shadow record whose path's leader wrote a record at
+// this depth with the same origin, t_max and direction takes that record's
+// visibility (qsx); the others are traced (qst).
+__global__ void __launch_bounds__(256) k_shadow_split(WaveArgs a, int depth) {
+  __shared__ uint32_t sw[256 / 32 + 1];
+  const uint32_t count = min(a.counters[CNT_SH(depth)], a.cap);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += stride) {
+    uint32_t i = base + threadIdx.x;
+    bool valid = i < count, share = false;
+    if (valid) {
+      float4 so = a.sh_o[i], sd = a.sh_d[i];
+      uint32_t ld = a.lead[__float_as_uint(sd.w)];
+      if (ld != ~0u) {
+        uint2 lr = a.shrec[ld];
+        if (lr.y == (uint32_t)depth + 1u) {
+          float4 lo = a.sh_o[lr.x];
+          share = same_bits3(so, lo) && __float_as_uint(so.w) == __float_as_uint(lo.w) &&
+                  same_bits3(sd, a.sh_d[lr.x]);
+        }
+      }
+    }
+    block_append(valid && share, i, a.counters + CNT_SCP(depth), a.qsx, a.cap, a.status, sw);
+    block_append(valid && !share, i, a.counters + CNT_STR(depth), a.qst, a.cap, a.status, sw);
+  }
+}
+
+// After k_shadow: a record of qsx whose leader's record reached its light
+// adds its contribution, as k_shadow adds a clear ray's.
+__global__ void __launch_bounds__(256) k_shadow_copy(WaveArgs a, int depth) {
+  const uint32_t count = min(a.counters[CNT_SCP(depth)], a.cap);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    uint32_t r = a.qsx[i];
+    uint32_t slot = __float_as_uint(a.sh_d[r].w);
+    if (a.vis[a.shrec[a.lead[slot]].x]) {
+      float4 c = a.sh_c[r];
+      float4 l = a.L[slot];
+      a.L[slot] = make_float4(l.x + c.x, l.y + c.y, l.z + c.z, l.w + c.w);
     }
   }
 }

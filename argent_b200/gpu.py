@@ -122,6 +122,11 @@ class Context:
         """Capture and replay repeated renders as CUDA graphs (default on)."""
         self.check(self.lib.argent_ctx_set_graphs(self.h, 1 if on else 0))
 
+    def set_ray_sharing(self, on):
+        """Batches trace the rays their renders have in common once
+        (argent_ctx_set_ray_sharing; default off)."""
+        self.check(self.lib.argent_ctx_set_ray_sharing(self.h, 1 if on else 0))
+
     def traversal_counts(self):
         out = (ctypes.c_uint64 * 6)()
         self.check(self.lib.argent_ctx_traversal_counts(self.h, out))

@@ -594,6 +594,8 @@ def run_gpu(args, world, rank, device):
     torch.cuda.set_device(device)
     ctx = Context(device, wave_paths=args.wave_paths or STILL_WAVE_PATHS, lanes=args.lanes)
     plan = ReelPlan(ctx) if args.workload == "reel_batch" else StillPlan(ctx, args.workload, args.tri_test)
+    if args.share_rays:
+        ctx.set_ray_sharing(True)
     if args.spp:
         plan.set_spp(args.spp)  # profiling runs only: the bench line uses the workload's spp
     stream = torch.cuda.ExternalStream(ctx.stream)
@@ -803,6 +805,7 @@ def run_gpu(args, world, rank, device):
                     f"{plan.device_bytes / 1e6:.0f} MB)",
                     "context": {"lanes": ctx.config()[0], "wave_paths": ctx.config()[1]},
                     "tuning": tune_info,
+                    "ray_sharing": bool(args.share_rays),
                     "vs_baseline_ref": "README.md:5-6 ~17.7M path-samples/s on 32 CPU cores"})
         out = {
             "metric": "path-samples/s", "value": value, "unit": "path-samples/s", "n_gpus": world,
@@ -1089,38 +1092,50 @@ def ctx_wave_mb(args):
 
 def reel_compare(args, device, steps=4):
     """The batched form against the plain single-render path on one frame
-    of the batched workload (12 renders: 3 pieces x 4 alloys), both end to
+    of the batched workload (12 renders: 3 pieces x 4 alloys), all end to
     end with host buffers: the batch is one render_batch and then every
     film's read; the plain path is render_reel's loop (jobs.rs:689-707), one
-    render_pass and its film read per render."""
+    render_pass and its film read per render.  A third leg runs the batch
+    with ray sharing (argent_ctx_set_ray_sharing): the four alloys of a piece
+    trace their common rays once; its films are compared with the unshared
+    batch's."""
     from argent_b200.gpu import Context, render_pass
 
     ctx = Context(device, wave_paths=STILL_WAVE_PATHS)
     plan = ReelPlan(ctx)
     fp = ctypes.POINTER(ctypes.c_float)
-    bufs = [tuple(np.zeros((f.height, f.width, 3), np.float32) for _ in range(3)) for f in plan.films]
+    names = ("batched", "batched_shared_rays", "plain")
+    bufs = {n: [tuple(np.zeros((f.height, f.width, 3), np.float32) for _ in range(3)) for f in plan.films]
+            for n in names}
 
     def read(f, b):
         c, a, n = b
         ctx.check(ctx.lib.argent_film_read(f.h, c.ctypes.data_as(fp), a.ctypes.data_as(fp), n.ctypes.data_as(fp)))
 
-    def batched(k):
+    def batched(k, name="batched"):
         run_plan(ctx, plan, k)
-        for f, b in zip(plan.films, bufs):
+        for f, b in zip(plan.films, bufs[name]):
             read(f, b)
 
+    def batched_shared(k):
+        ctx.set_ray_sharing(True)
+        try:
+            batched(k, "batched_shared_rays")
+        finally:
+            ctx.set_ray_sharing(False)
+
     def plain(k):
-        for it, b in zip(plan.items(k), bufs):
+        for it, b in zip(plan.items(k), bufs["plain"]):
             it[2].clear()
             render_pass(ctx, *it)
             read(it[2], b)
 
-    forms = (("batched", batched), ("plain", plain))
+    forms = tuple(zip(names, (batched, batched_shared, plain)))
     for _, fn in forms:
         fn(0)  # warm-up (graphs captured, buffers grown)
     ctx.sync()
-    # The two forms alternate frame by frame, so a drift of the device's
-    # speed during the leg falls on both.
+    # The forms alternate frame by frame, so a drift of the device's speed
+    # during the leg falls on all of them.
     spent = {name: 0.0 for name, _ in forms}
     for k in range(steps):
         for name, fn in forms:
@@ -1129,6 +1144,12 @@ def reel_compare(args, device, steps=4):
             spent[name] += time.perf_counter() - t0
     out = {name: {"e2e_path_samples_per_s": plan.path_samples * steps / dt, "s_per_frame": dt / steps}
            for name, dt in spent.items()}
+    # The last frame's films: shared against unshared (the same samples,
+    # grouped into other waves, so equal to float rounding of the sums).
+    worst = 0.0
+    for (c1, _, _), (c2, _, _) in zip(bufs["batched_shared_rays"], bufs["batched"]):
+        worst = max(worst, float(np.abs(c1 - c2).max() / max(float(np.abs(c2).max()), 1e-30)))
+    out["batched_shared_rays"]["max_abs_diff_vs_batched_over_max"] = worst
     out["workload"] = plan.name
     out["renders_per_frame"] = plan.renders
     out["timing"] = (f"wall clock, {steps} turntable frames each, the forms alternating frame by frame, "
@@ -1180,6 +1201,8 @@ def main():
     ap.add_argument("--extras-serve-seconds", type=float, default=30.0)
     ap.add_argument("--tune", action="store_true", help="apply (search and cache) a launch tuning")
     ap.add_argument("--no-tune", action="store_true", help="no launch tuning, also for reel and serve")
+    ap.add_argument("--share-rays", action="store_true",
+                    help="batches trace the rays their renders have in common once (argent_ctx_set_ray_sharing)")
     ap.add_argument("--tri-test", default="mt", choices=["mt", "watertight"],
                     help="stills: argent's Moller-Trumbore (default, bit-exact) or the watertight test")
     ap.add_argument("--lanes", type=int, default=0, help="concurrent waves (0 = the library default)")

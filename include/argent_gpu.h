@@ -662,6 +662,19 @@ int argent_ctx_kernel_times(ArgentCtx* ctx, double* ms, uint64_t* launches);
  * graphs and replayed when the same waves come again (on by default); off
  * also frees the captured graphs. */
 int argent_ctx_set_graphs(ArgentCtx* ctx, int on);
+/* Ray sharing for batches (off by default).  argent's reel renders every
+ * metal variant of a frame on its own (jobs.rs:595-713); variants that differ
+ * only in their materials -- the same piece, turntable angle, panels, floor,
+ * camera, film size, samples and seed -- trace the same rays until their
+ * paths part.  While on, the renders of one argent_render_batch (or serve
+ * step) that match so are laid out side by side in the waves, and a ray
+ * bit-identical to the same pixel-sample's ray of the first of them takes
+ * that ray's closest hit or shadow visibility instead of being traced again.
+ * Every hit record and radiance sample equals the unshared render's; a
+ * film's sums may group its samples differently (other waves), which moves
+ * its values by float rounding only.  Costs 33 bytes per path slot per lane
+ * in use. */
+int argent_ctx_set_ray_sharing(ArgentCtx* ctx, int on);
 /* Traversal visit counters: on = count, and reset to zero. */
 int argent_ctx_set_counting(ArgentCtx* ctx, int on);
 /* out[6] = closest-hit rays, nodes, triangles; any-hit rays, nodes,
