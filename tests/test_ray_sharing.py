@@ -8,6 +8,7 @@ film sums where it groups them into other waves."""
 import numpy as np
 import pytest
 
+from argent_b200 import _native as N
 from argent_b200 import workloads as W
 
 ALLOYS = ("sterling", "gold14k", "rose14k")
@@ -138,3 +139,39 @@ def test_sharing_off_is_the_default_and_leaves_batches_unchanged():
     films_of(ctx, piece, descs, wl, 4, share=True)
     b = films_of(ctx, piece, descs, wl, 4)
     assert_films_equal(a, b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("overlap", [False, True])
+def test_served_variants_share_and_equal_their_renders_alone(overlap):
+    """Served requests for three alloys of the same piece, size, samples and
+    seed (argent's queue renders every job with seed 7, queue.rs:613) plus one
+    of another size: with sharing on they are served together, and every
+    result equals its render alone to float rounding."""
+    from argent_b200.gpu import Context, Film, Piece, Scene, Serve, render_pass
+
+    wl = W.ring_still()
+    ctx = Context(0)
+    piece = Piece(ctx, wl.mesh)
+    scenes = [Scene(ctx, piece, d) for d in variants(wl)]
+    cam = lambda w, h: W.shot(None, W.hull(wl.mesh), "hero", 100.0, 0.0, w / h)[0]  # noqa: E731
+    reqs = [(0, 96, 96, 8), (1, 96, 96, 8), (2, 96, 96, 8), (1, 64, 128, 4)]
+    ctx.set_ray_sharing(True)
+    srv = Serve(ctx, step_path_samples=1 << 20, overlap=overlap)
+    tickets = [srv.submit(scenes[i], cam(w, h), W.settings(8), w, h, spp, 7, 0) for i, w, h, spp in reqs]
+    steps = 0
+    while srv.step():
+        steps += 1
+        assert steps < 1000
+    ctx.set_ray_sharing(False)
+    for t, (i, w, h, spp) in zip(tickets, reqs):
+        st = srv.poll(t)
+        assert st.state == N.REQ_DONE and st.samples == spp
+        c, a, n = srv.read(t)
+        f = Film(ctx, w, h)
+        render_pass(ctx, scenes[i], cam(w, h), f, W.settings(8), spp, 7)
+        c0, a0, n0 = f.read()
+        assert np.allclose(c, c0, rtol=1e-5, atol=1e-7)
+        assert np.allclose(a, a0, rtol=1e-5, atol=1e-7)
+        assert np.allclose(n, n0, rtol=1e-5, atol=1e-6)
+    srv.close()
