@@ -1067,7 +1067,7 @@ static int ensure_share(ArgentCtx* ctx, int lane, uint64_t cap) {
     w.bytes += bytes;
     return true;
   };
-  bool ok = alloc((void**)&w.lead, cap * sizeof(uint32_t)) && alloc((void**)&w.mark, cap * sizeof(uint32_t)) &&
+  bool ok = alloc((void**)&w.lead, cap * sizeof(uint32_t)) &&
             alloc((void**)&w.shrec, cap * sizeof(uint2)) && alloc((void**)&w.vis, cap * sizeof(uint8_t)) &&
             alloc((void**)&w.qt, cap * sizeof(uint32_t)) && alloc((void**)&w.qx, cap * sizeof(uint32_t)) &&
             alloc((void**)&w.qst, cap * sizeof(uint32_t)) && alloc((void**)&w.qsx, cap * sizeof(uint32_t));
@@ -1415,7 +1415,6 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
       a.q_out = wb.q1;
       const bool shared = wshare[wi] != 0;
       a.lead = shared ? wb.lead : nullptr;
-      a.mark = shared ? wb.mark : nullptr;
       a.shrec = shared ? wb.shrec : nullptr;
       a.vis = shared ? wb.vis : nullptr;
       a.qt = shared ? wb.qt : nullptr;
@@ -1479,8 +1478,9 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
         {
           ProfScope ps(ctx, KC_SHADOW, st);
           if (shared) {
+            dev::k_shadow_index<<<g_split, 256, 0, st>>>(a, (int)depth);
             dev::k_shadow_split<<<g_split, 256, 0, st>>>(a, (int)depth);
-            ++*kernels;
+            *kernels += 2;
           }
           if (uni)
             dev::k_shadow<true><<<g_any[1], 128, 0, st>>>(a, (int)depth);
@@ -1544,7 +1544,7 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
     for (int k = 0; k < used; ++k) {
       put(&args[(start + k) % nlanes], sizeof(dev::WaveArgs));
       const WaveBuffers& wb = ctx->wave[(start + k) % nlanes];
-      const void* sp[8] = {wb.lead, wb.mark, wb.shrec, wb.vis, wb.qt, wb.qx, wb.qst, wb.qsx};
+      const void* sp[7] = {wb.lead, wb.shrec, wb.vis, wb.qt, wb.qx, wb.qst, wb.qsx};
       put(sp, sizeof(sp));
     }
     for (size_t wi = 0; wi < waves.size(); ++wi) {

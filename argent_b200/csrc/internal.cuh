@@ -115,12 +115,12 @@ struct WaveBuffers {
   std::vector<void*> allocs;
   uint64_t bytes = 0;
   // Ray sharing (allocated on the first wave that shares rays): per slot its
-  // leader's slot, the depth + 1 it is alive at, and its shadow record of
-  // the current depth (position, depth + 1); per shadow record whether it
-  // reached its light; the queues of rays to trace and of rays that take
-  // their leader's result, for closest hits and for shadow rays.
+  // leader's slot and its shadow record of the current depth (position,
+  // depth + 1); per shadow record whether it reached its light; the queues of
+  // rays to trace and of rays that take their leader's result, for closest
+  // hits and for shadow rays.
   uint64_t share_cap = 0, share_bytes = 0;
-  uint32_t *lead = nullptr, *mark = nullptr;
+  uint32_t* lead = nullptr;
   uint2* shrec = nullptr;
   uint8_t* vis = nullptr;
   uint32_t *qt = nullptr, *qx = nullptr, *qst = nullptr, *qsx = nullptr;
@@ -128,7 +128,7 @@ struct WaveBuffers {
   void release_share() {
     for (void* a : share_allocs) cudaFree(a);
     share_allocs.clear();
-    lead = mark = qt = qx = qst = qsx = nullptr;
+    lead = qt = qx = qst = qsx = nullptr;
     shrec = nullptr;
     vis = nullptr;
     share_cap = 0;

@@ -259,12 +259,13 @@ struct WaveArgs {
   int32_t u_has_turn;
   float u_to_obj_s, u_to_obj_c;
   // Ray sharing, for a wave whose segments share rays (null otherwise): per
-  // slot its leader's slot (~0u for none) and the depth + 1 it is alive at;
-  // per slot its shadow record of the current depth (position, depth + 1);
-  // per shadow record whether it reached its light; the queues of closest
-  // rays to trace (qt) and to take from their leader (qx), and the same for
-  // shadow records (qst, qsx).
-  uint32_t *lead, *mark;
+  // slot its leader's slot (~0u for none) and its shadow record of the
+  // current depth (position, depth + 1); per shadow record whether it
+  // reached its light; the queues of closest rays to trace (qt) and to take
+  // from their leader (qx), and the same for shadow records (qst, qsx).
+  // Whether a path is alive at a depth is in bits 2..7 of its meta.w (the
+  // depth it was last continued to).
+  uint32_t* lead;
   uint2* shrec;
   uint8_t* vis;
   uint32_t *qt, *qx, *qst, *qsx;
@@ -341,7 +342,6 @@ __global__ void __launch_bounds__(256) k_raygen(WaveArgs a, WaveDesc w) {
     uint32_t x = pix % job.w, y = pix / job.w;
     if (a.lead) {
       a.lead[slot] = sg.lead == ~0u ? ~0u : sg.lead + k;
-      a.mark[slot] = 1u;  // alive at depth 0
       a.shrec[slot] = make_uint2(0u, 0u);  // no shadow record yet
     }
     uint32_t pix_seed = hash32((y * job.w + x) ^ job.seed_h);
@@ -404,8 +404,7 @@ __device__ __forceinline__ void warp_append(bool pred, uint32_t value, uint32_t*
 // own).  The record is written where it is built, so its twelve values are
 // not held through the continuation sample.  The order of the records in the
 // queue does not matter: each adds to its own path's radiance.
-__device__ __forceinline__ void push_shadow(const WaveArgs& a, int depth, uint32_t slot, float4 o, float4 d,
-                                            float4 c) {
+__device__ __forceinline__ void push_shadow(const WaveArgs& a, int depth, float4 o, float4 d, float4 c) {
   unsigned m = __activemask();
   int lane = threadIdx.x & 31;
   int leader = __ffs(m) - 1;
@@ -417,7 +416,6 @@ __device__ __forceinline__ void push_shadow(const WaveArgs& a, int depth, uint32
     a.sh_o[pos] = o;
     a.sh_d[pos] = d;
     a.sh_c[pos] = c;
-    if (a.shrec) a.shrec[slot] = make_uint2(pos, (uint32_t)depth + 1u);
   } else {
     atomicOr(a.status, ARGENT_STATUS_QUEUE_OVERFLOW);
   }
@@ -876,7 +874,7 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
               float4 so = make_float4(oo.x, oo.y, oo.z, t_max);
               float4 sd = make_float4(od.x, od.y, od.z, __uint_as_float(slot));
               if constexpr (InlineShadow<CLS>::value) {
-                push_shadow(a, depth, slot, so, sd, to_f4(c));
+                push_shadow(a, depth, so, sd, to_f4(c));
               } else {
                 out.shadow = true;
                 out.sh_o = so;
@@ -935,7 +933,9 @@ __device__ __forceinline__ ShadeOut shade_path(const WaveArgs& a, uint32_t slot,
     if (out.alive) {
       a.o[slot] = make_float4(ro.x, ro.y, ro.z, 0.0f);
       a.d[slot] = make_float4(rd.x, rd.y, rd.z, prev_pdf);
-      uint32_t nf = (flags & 0xffff0000u) | (specular ? 1u : 0u) | (rough_seen ? 2u : 0u) | (medium << 8);
+      // Bits 2..7: the depth the path is alive at (ray sharing reads it).
+      uint32_t nf = (flags & 0xffff0000u) | (specular ? 1u : 0u) | (rough_seen ? 2u : 0u) |
+                    ((((uint32_t)depth + 1u) & 63u) << 2) | (medium << 8);
       a.meta[slot].w = nf;
       a.rng[slot] = s.rng;
     }
@@ -996,7 +996,6 @@ __global__ void __launch_bounds__(128, CLS == CLS_TERMINAL      ? 1
       r = shade_path<CLS, MAP>(a, slot, depth);
     }
     warp_append(r.alive, slot, next_counter, a.q_out, cap, a.status);
-    if (a.mark && r.alive) a.mark[slot] = (uint32_t)depth + 2u;  // alive at depth + 1
     if constexpr (!InlineShadow<CLS>::value) {
       // Shadow rays: the record is written at the queue position.
       unsigned m = __ballot_sync(0xffffffffu, r.shadow);
@@ -1012,7 +1011,6 @@ __global__ void __launch_bounds__(128, CLS == CLS_TERMINAL      ? 1
             a.sh_o[pos] = r.sh_o;
             a.sh_d[pos] = r.sh_d;
             a.sh_c[pos] = r.sh_c;
-            if (a.shrec) a.shrec[slot] = make_uint2(pos, (uint32_t)depth + 1u);
           } else {
             atomicOr(a.status, ARGENT_STATUS_QUEUE_OVERFLOW);
           }
@@ -1083,6 +1081,12 @@ __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_shadow(WaveArgs a, 
 // have identical closest hits and identical visibility, so the records and
 // films equal those of tracing every ray.
 
+// The depth path `slot` was last continued to (0 from ray generation): it is
+// alive at `depth` exactly when this equals `depth`.
+__device__ __forceinline__ uint32_t alive_depth(const WaveArgs& a, uint32_t slot) {
+  return (reinterpret_cast<const uint32_t*>(a.meta + slot)[3] >> 2) & 63u;
+}
+
 __device__ __forceinline__ bool same_bits3(float4 a, float4 b) {
   return __float_as_uint(a.x) == __float_as_uint(b.x) && __float_as_uint(a.y) == __float_as_uint(b.y) &&
          __float_as_uint(a.z) == __float_as_uint(b.z);
@@ -1142,7 +1146,7 @@ __global__ void __launch_bounds__(256) k_share_split(WaveArgs a, int depth) {
     if (valid) {
       slot = a.q_in[i];
       uint32_t ld = a.lead[slot];
-      if (ld != ~0u && a.mark[ld] == (uint32_t)depth + 1u)
+      if (ld != ~0u && alive_depth(a, ld) == (uint32_t)depth)
         share = same_bits3(a.o[slot], a.o[ld]) && same_bits3(a.d[slot], a.d[ld]);
     }
     block_append(valid && share, slot, a.counters + CNT_CP(depth), a.qx, a.cap, a.status, sw);
@@ -1173,6 +1177,14 @@ __global__ void __launch_bounds__(256) k_hit_copy(WaveArgs a, int depth) {
         block_append(cls == c, slot, a.counters + CNT_CLS(depth, c), a.qc + (size_t)c * a.cap, a.cap, a.status,
                      sw);
   }
+}
+
+// Before k_shadow_split: each path's shadow record of this depth, by slot
+// (position, depth + 1).
+__global__ void __launch_bounds__(256) k_shadow_index(WaveArgs a, int depth) {
+  const uint32_t count = min(a.counters[CNT_SH(depth)], a.cap);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    a.shrec[__float_as_uint(a.sh_d[i].w)] = make_uint2(i, (uint32_t)depth + 1u);
 }
 
 // Before k_shadow: a shadow record whose path's leader wrote a record at

@@ -672,7 +672,7 @@ int argent_ctx_set_graphs(ArgentCtx* ctx, int on);
  * that ray's closest hit or shadow visibility instead of being traced again.
  * Every hit record and radiance sample equals the unshared render's; a
  * film's sums may group its samples differently (other waves), which moves
- * its values by float rounding only.  Costs 33 bytes per path slot per lane
+ * its values by float rounding only.  Costs 29 bytes per path slot per lane
  * in use. */
 int argent_ctx_set_ray_sharing(ArgentCtx* ctx, int on);
 /* Traversal visit counters: on = count, and reset to zero. */
