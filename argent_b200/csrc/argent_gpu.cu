@@ -1070,7 +1070,8 @@ static int ensure_share(ArgentCtx* ctx, int lane, uint64_t cap) {
   bool ok = alloc((void**)&w.lead, cap * sizeof(uint32_t)) &&
             alloc((void**)&w.shrec, cap * sizeof(uint2)) && alloc((void**)&w.vis, cap * sizeof(uint8_t)) &&
             alloc((void**)&w.qt, cap * sizeof(uint32_t)) && alloc((void**)&w.qx, cap * sizeof(uint32_t)) &&
-            alloc((void**)&w.qst, cap * sizeof(uint32_t)) && alloc((void**)&w.qsx, cap * sizeof(uint32_t));
+            alloc((void**)&w.qst, cap * sizeof(uint32_t)) && alloc((void**)&w.qsx, cap * sizeof(uint32_t)) &&
+            alloc((void**)&w.qsc, cap * sizeof(uint32_t));
   if (!ok) {
     w.release_share();
     return set_error(ctx, ARGENT_E_OOM, "ray-sharing buffers: out of device memory");
@@ -1116,6 +1117,35 @@ bool same_geometry(const ArgentScene* a, const ArgentScene* b) {
 bool same_traversal(const ArgentScene* a, const ArgentScene* b) {
   return a == b || (same_geometry(a, b) && a->host.floor_class == b->host.floor_class &&
                     std::memcmp(a->host.mat_class, b->host.mat_class, sizeof(a->host.mat_class)) == 0);
+}
+
+// Sets `f`'s ray-sharing masks against its group's leader `l` (scenes ls,
+// fs): the material slots with byte-equal records and shading classes, and
+// whether the rest of what shading reads is equal (the scene descriptor but
+// for its materials, their classes and the film's camera matrix; the path
+// settings).  Environment tables and emission spectra of equal content are
+// one blob, so their pointers compare equal.
+void share_masks(const dev::DevJob& l, const ArgentScene* ls, const ArgentScene* fs, dev::DevJob* f) {
+  std::memset(f->share_mat, 0, sizeof(f->share_mat));
+  f->share_rest = 0;
+  dev::DevScene a = ls->host, b = fs->host;
+  for (dev::DevScene* x : {&a, &b}) {
+    x->mats = nullptr;
+    x->num_mats = 0;
+    std::memset(x->mat_class, 0, sizeof(x->mat_class));
+    x->floor_class = 0;
+    x->class_mask = 0;
+    std::memset(x->cam_m, 0, sizeof(x->cam_m));
+  }
+  const bool rest = std::memcmp(&a, &b, sizeof(a)) == 0 && l.max_depth == f->max_depth &&
+                    l.rr_depth == f->rr_depth && std::memcmp(&l.clamp_indirect, &f->clamp_indirect, 4) == 0;
+  if (!rest) return;
+  f->share_rest = 1;
+  const size_t n = std::min(ls->mats_host.size(), fs->mats_host.size());
+  for (size_t i = 0; i < n && i < 256; ++i)
+    if (ls->host.mat_class[i] == fs->host.mat_class[i] &&
+        std::memcmp(&ls->mats_host[i], &fs->mats_host[i], sizeof(ArgentMaterial)) == 0)
+      f->share_mat[i / 32] |= 1u << (i % 32);
 }
 
 // Groups of jobs that trace the same rays: the same film size, samples,
@@ -1263,9 +1293,19 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   for (size_t j = 0; j < jobs.size(); ++j) total += (uint64_t)jobs[j].w * jobs[j].h * counts[j];
   uint32_t cap = (uint32_t)std::min<uint64_t>(ctx->limits.wave_paths, std::max<uint64_t>(total, 1u << 16));
   std::vector<uint32_t> depths;
-  std::vector<dev::WaveDesc> waves =
-      plan_waves(jobs, counts, plan_groups(ctx->share_rays, jobs, counts, job_scenes), cap, &depths);
+  const std::vector<std::vector<uint32_t>> groups = plan_groups(ctx->share_rays, jobs, counts, job_scenes);
+  std::vector<dev::WaveDesc> waves = plan_waves(jobs, counts, groups, cap, &depths);
   if (waves.empty()) return ARGENT_OK;
+  // Followers of a group: which of their materials (and whether the rest of
+  // what shading reads) equal the leader's.
+  std::vector<dev::DevJob> shared_jobs;
+  const std::vector<dev::DevJob>* job_list = &jobs;
+  for (const auto& g : groups) {
+    if (g.size() < 2) continue;
+    if (shared_jobs.empty()) shared_jobs = jobs;
+    for (size_t m = 1; m < g.size(); ++m) share_masks(jobs[g[0]], job_scenes[g[0]], job_scenes[g[m]], &shared_jobs[g[m]]);
+    job_list = &shared_jobs;
+  }
   rc = ensure_lane_streams(ctx, ctx->lanes);
   if (rc != ARGENT_OK) return rc;
   const int nlanes = ctx->lanes;
@@ -1307,7 +1347,7 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
     ARGENT_CK(ctx, cudaMallocAsync((void**)&d_jobs, jobs.size() * sizeof(dev::DevJob), ctx->stream));
   }
   // Pageable source: the call returns once the bytes are staged.
-  ARGENT_CK(ctx, cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(dev::DevJob), cudaMemcpyHostToDevice,
+  ARGENT_CK(ctx, cudaMemcpyAsync(d_jobs, job_list->data(), jobs.size() * sizeof(dev::DevJob), cudaMemcpyHostToDevice,
                                  ctx->stream));
   dev::WaveArgs args[ARGENT_LANES];
   for (int l = 0; l < ARGENT_LANES; ++l) {
@@ -1421,6 +1461,7 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
       a.qx = shared ? wb.qx : nullptr;
       a.qst = shared ? wb.qst : nullptr;
       a.qsx = shared ? wb.qsx : nullptr;
+      a.qsc = shared ? wb.qsc : nullptr;
       {
         ProfScope ps(ctx, KC_RAYGEN, st);
         dev::k_raygen<<<g_ray, 256, 0, st>>>(a, w);
@@ -1479,8 +1520,9 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
           ProfScope ps(ctx, KC_SHADOW, st);
           if (shared) {
             dev::k_shadow_index<<<g_split, 256, 0, st>>>(a, (int)depth);
+            dev::k_shade_copy<<<g_split, 256, 0, st>>>(a, (int)depth);
             dev::k_shadow_split<<<g_split, 256, 0, st>>>(a, (int)depth);
-            *kernels += 2;
+            *kernels += 3;
           }
           if (uni)
             dev::k_shadow<true><<<g_any[1], 128, 0, st>>>(a, (int)depth);
@@ -1544,7 +1586,7 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
     for (int k = 0; k < used; ++k) {
       put(&args[(start + k) % nlanes], sizeof(dev::WaveArgs));
       const WaveBuffers& wb = ctx->wave[(start + k) % nlanes];
-      const void* sp[7] = {wb.lead, wb.shrec, wb.vis, wb.qt, wb.qx, wb.qst, wb.qsx};
+      const void* sp[8] = {wb.lead, wb.shrec, wb.vis, wb.qt, wb.qx, wb.qst, wb.qsx, wb.qsc};
       put(sp, sizeof(sp));
     }
     for (size_t wi = 0; wi < waves.size(); ++wi) {
@@ -1740,6 +1782,7 @@ int argent_scene_upload(ArgentCtx* ctx, ArgentPiece* piece, const ArgentSceneDes
   auto share = [&](const void* src, size_t bytes) -> void* { return intern_blob(ctx, src, bytes, &s->shared); };
   bool ok = true;
   h.mats = (const ArgentMaterial*)up(desc->materials, sizeof(ArgentMaterial) * desc->num_materials);
+  s->mats_host.assign(desc->materials, desc->materials + desc->num_materials);
   ok = ok && h.mats;
   h.num_mats = desc->num_materials;
   h.num_panels = desc->num_panels;

@@ -80,6 +80,14 @@ struct DevJob {
   double* film_xyz64;    // FP64 sums (or null)
   float* film_albedo;    // 3 per pixel
   float* film_normal;    // 3 per pixel
+  // Ray sharing, for a job that follows another in its group: the material
+  // slots whose records equal the leader's (bit i of share_mat[i / 32]), and
+  // whether everything else shading reads (lights, environment, floor,
+  // turntable, path settings) equals the leader's.  A bounce-0 hit on such a
+  // material is shaded exactly as the leader's, so it takes the leader's
+  // result (k_shade_copy).
+  uint32_t share_mat[8];
+  uint32_t share_rest;
 };
 
 // A contiguous run of path slots in a wave: pixels [p0, p0+pn) of job
@@ -121,6 +129,7 @@ struct WaveBuffers {
   // hits and for shadow rays.
   uint64_t share_cap = 0, share_bytes = 0;
   uint32_t* lead = nullptr;
+  uint32_t* qsc = nullptr;  // bounce-0 paths that take their leader's shading
   uint2* shrec = nullptr;
   uint8_t* vis = nullptr;
   uint32_t *qt = nullptr, *qx = nullptr, *qst = nullptr, *qsx = nullptr;
@@ -128,7 +137,7 @@ struct WaveBuffers {
   void release_share() {
     for (void* a : share_allocs) cudaFree(a);
     share_allocs.clear();
-    lead = qt = qx = qst = qsx = nullptr;
+    lead = qt = qx = qst = qsx = qsc = nullptr;
     shrec = nullptr;
     vis = nullptr;
     share_cap = 0;
@@ -247,6 +256,7 @@ struct ArgentScene {
   dev::DevScene* d_scene = nullptr;
   std::vector<void*> allocs;
   std::vector<void*> shared;  // blobs held in ctx->blobs
+  std::vector<ArgentMaterial> mats_host;  // the material records, for ray sharing's comparisons
   uint64_t bytes = 0;
   float cam_m[9];
   // Pinned staging copy for stream-ordered descriptor updates (turntable),

@@ -269,6 +269,7 @@ struct WaveArgs {
   uint2* shrec;
   uint8_t* vis;
   uint32_t *qt, *qx, *qst, *qsx;
+  uint32_t* qsc;  // bounce-0 paths that take their leader's shading
 };
 
 // Queue counters of one wave: active paths per bounce, shade-queue lengths
@@ -283,7 +284,9 @@ struct WaveArgs {
 #define CNT_CP(d) ((ARGENT_MAX_DEPTH + 2) * (3 + NUM_CLS) + (d))
 #define CNT_STR(d) ((ARGENT_MAX_DEPTH + 2) * (4 + NUM_CLS) + (d))
 #define CNT_SCP(d) ((ARGENT_MAX_DEPTH + 2) * (5 + NUM_CLS) + (d))
-#define CNT_QUEUES ((ARGENT_MAX_DEPTH + 2) * (6 + NUM_CLS))
+// Ray sharing: bounce-0 paths that take their leader's shading.
+#define CNT_SC(d) ((ARGENT_MAX_DEPTH + 2) * (6 + NUM_CLS) + (d))
+#define CNT_QUEUES ((ARGENT_MAX_DEPTH + 2) * (7 + NUM_CLS))
 #define CNT_WORK(q) (CNT_QUEUES + (q))
 #define CNT_TOTAL (2 * CNT_QUEUES)
 
@@ -1154,8 +1157,26 @@ __global__ void __launch_bounds__(256) k_share_split(WaveArgs a, int depth) {
   }
 }
 
+// True when path `slot` enters shading at `depth` (> 0) in the same state as
+// path `l`: throughput, radiance, wavelengths and their pdfs, sampler state,
+// the previous bounce's pdf and its flags (specular, rough, medium).  The
+// rays and hits are already equal.
+__device__ __forceinline__ bool same_state(const WaveArgs& a, uint32_t slot, uint32_t l) {
+  auto eq4 = [](float4 x, float4 y) { return same_bits3(x, y) && __float_as_uint(x.w) == __float_as_uint(y.w); };
+  return eq4(a.beta[slot], a.beta[l]) && eq4(a.L[slot], a.L[l]) && eq4(a.lambda[slot], a.lambda[l]) &&
+         eq4(a.pdf[slot], a.pdf[l]) && a.rng[slot] == a.rng[l] &&
+         __float_as_uint(a.d[slot].w) == __float_as_uint(a.d[l].w) &&
+         ((reinterpret_cast<const uint32_t*>(a.meta + slot)[3] ^ reinterpret_cast<const uint32_t*>(a.meta + l)[3]) &
+          0xffffu) == 0u;
+}
+
 // After k_intersect: the paths of qx take their leaders' hit records and
-// join the shade queue of their own material's class.
+// join the shade queue of their own material's class.  A path that hits a
+// surface whose material record and everything else shading reads equal the
+// leader's (the job's share masks), and enters shading in its leader's state
+// -- at bounce 0 always (the same camera sample), later while its path has
+// met only such materials -- goes to qsc instead and takes the leader's
+// shading (k_shade_copy).
 template <bool U>
 __global__ void __launch_bounds__(256) k_hit_copy(WaveArgs a, int depth) {
   __shared__ uint32_t sw[256 / 32 + 1];
@@ -1165,17 +1186,93 @@ __global__ void __launch_bounds__(256) k_hit_copy(WaveArgs a, int depth) {
     uint32_t i = base + threadIdx.x;
     int cls = -1;
     uint32_t slot = 0;
+    bool same_shading = false;
     if (i < count) {
       slot = a.qx[i];
       float4 rec = a.hit[a.lead[slot]];
       a.hit[slot] = rec;
-      const DevScene* sc = U ? a.uscene : a.jobs[a.meta[slot].w >> 16].scene;
-      cls = hit_class(sc, U ? a.upiece : sc->piece, rec);
+      const DevJob& job = a.jobs[a.meta[slot].w >> 16];
+      const DevScene* sc = U ? a.uscene : job.scene;
+      const DevPiece& pc = U ? a.upiece : sc->piece;
+      cls = hit_class(sc, pc, rec);
+      // Surface hits only: a miss or panel hit costs less to shade than to
+      // copy.
+      if (job.share_rest && cls != CLS_TERMINAL) {
+        uint32_t kind = __float_as_uint(rec.w);
+        uint32_t m = kind == HIT_FLOOR ? (uint32_t)sc->floor_material : __ldg(&pc.tri_idx[kind].w);
+        same_shading = ((job.share_mat[m >> 5] >> (m & 31u)) & 1u) && (depth == 0 || same_state(a, slot, a.lead[slot]));
+      }
+      if (same_shading) cls = -1;
     }
+    if (__syncthreads_or(same_shading))
+      block_append(same_shading, slot, a.counters + CNT_SC(depth), a.qsc, a.cap, a.status, sw);
     for (int c = 0; c < NUM_CLS; ++c)
       if (__syncthreads_or(cls == c))
         block_append(cls == c, slot, a.counters + CNT_CLS(depth, c), a.qc + (size_t)c * a.cap, a.cap, a.status,
                      sw);
+  }
+}
+
+// After the shading kernels and k_shadow_index: each path of qsc takes its
+// leader's shaded state (radiance, throughput, guides, the next ray and
+// sampler state, its flags but for its own job index), continues if the
+// leader continues, and gets a copy of the leader's shadow record.
+__global__ void __launch_bounds__(256) k_shade_copy(WaveArgs a, int depth) {
+  __shared__ uint32_t sw[256 / 32 + 1];
+  const uint32_t count = min(a.counters[CNT_SC(depth)], a.cap);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < count; base += stride) {
+    uint32_t i = base + threadIdx.x;
+    bool alive = false, shadow = false;
+    uint32_t slot = 0, rec = 0;
+    if (i < count) {
+      slot = a.qsc[i];
+      uint32_t l = a.lead[slot];
+      a.L[slot] = a.L[l];
+      a.beta[slot] = a.beta[l];
+      a.lambda[slot] = a.lambda[l];
+      a.pdf[slot] = a.pdf[l];
+      a.albedo[slot] = a.albedo[l];
+      a.normal[slot] = a.normal[l];
+      a.o[slot] = a.o[l];
+      a.d[slot] = a.d[l];
+      a.rng[slot] = a.rng[l];
+      uint32_t* mw = reinterpret_cast<uint32_t*>(a.meta + slot) + 3;
+      *mw = (reinterpret_cast<const uint32_t*>(a.meta + l)[3] & 0xffffu) | (*mw & 0xffff0000u);
+      alive = alive_depth(a, l) == (uint32_t)depth + 1u;
+      uint2 sr = a.shrec[l];
+      shadow = sr.y == (uint32_t)depth + 1u;
+      rec = sr.x;
+    }
+    block_append(alive, slot, a.counters + CNT_ACT(depth + 1), a.q_out, a.cap, a.status, sw);
+    // The shadow record: a position reserved like a queue entry, then the
+    // leader's record with this path's slot.
+    const unsigned m = __ballot_sync(0xffffffffu, shadow);
+    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nw = blockDim.x >> 5;
+    if (lane == 0) sw[warp] = (uint32_t)__popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t total = 0;
+      for (unsigned w = 0; w < nw; ++w) {
+        uint32_t c = sw[w];
+        sw[w] = total;
+        total += c;
+      }
+      sw[nw] = total ? atomicAdd(a.counters + CNT_SH(depth), total) : 0u;
+    }
+    __syncthreads();
+    if (shadow) {
+      uint32_t pos = sw[nw] + sw[warp] + (uint32_t)__popc(m & ((1u << lane) - 1u));
+      if (pos < a.cap) {
+        float4 sd = a.sh_d[rec];
+        a.sh_o[pos] = a.sh_o[rec];
+        a.sh_d[pos] = make_float4(sd.x, sd.y, sd.z, __uint_as_float(slot));
+        a.sh_c[pos] = a.sh_c[rec];
+      } else {
+        atomicOr(a.status, ARGENT_STATUS_QUEUE_OVERFLOW);
+      }
+    }
+    __syncthreads();
   }
 }
 

@@ -669,10 +669,12 @@ int argent_ctx_set_graphs(ArgentCtx* ctx, int on);
  * paths part.  While on, the renders of one argent_render_batch (or serve
  * step) that match so are laid out side by side in the waves, and a ray
  * bit-identical to the same pixel-sample's ray of the first of them takes
- * that ray's closest hit or shadow visibility instead of being traced again.
+ * that ray's closest hit or shadow visibility instead of being traced again;
+ * a first hit on a material whose record equals the first render's (the
+ * studio floor) takes that render's shading too.
  * Every hit record and radiance sample equals the unshared render's; a
  * film's sums may group its samples differently (other waves), which moves
- * its values by float rounding only.  Costs 29 bytes per path slot per lane
+ * its values by float rounding only.  Costs 33 bytes per path slot per lane
  * in use. */
 int argent_ctx_set_ray_sharing(ArgentCtx* ctx, int on);
 /* Traversal visit counters: on = count, and reset to zero. */
