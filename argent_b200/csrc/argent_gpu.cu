@@ -1303,7 +1303,8 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   for (const auto& g : groups) {
     if (g.size() < 2) continue;
     if (shared_jobs.empty()) shared_jobs = jobs;
-    for (size_t m = 1; m < g.size(); ++m) share_masks(jobs[g[0]], job_scenes[g[0]], job_scenes[g[m]], &shared_jobs[g[m]]);
+    for (size_t m = 1; m < g.size(); ++m)
+      share_masks(jobs[g[0]], job_scenes[g[0]], job_scenes[g[m]], &shared_jobs[g[m]]);
     job_list = &shared_jobs;
   }
   rc = ensure_lane_streams(ctx, ctx->lanes);

@@ -1200,7 +1200,8 @@ __global__ void __launch_bounds__(256) k_hit_copy(WaveArgs a, int depth) {
       if (job.share_rest && cls != CLS_TERMINAL) {
         uint32_t kind = __float_as_uint(rec.w);
         uint32_t m = kind == HIT_FLOOR ? (uint32_t)sc->floor_material : __ldg(&pc.tri_idx[kind].w);
-        same_shading = ((job.share_mat[m >> 5] >> (m & 31u)) & 1u) && (depth == 0 || same_state(a, slot, a.lead[slot]));
+        same_shading =
+            ((job.share_mat[m >> 5] >> (m & 31u)) & 1u) && (depth == 0 || same_state(a, slot, a.lead[slot]));
       }
       if (same_shading) cls = -1;
     }

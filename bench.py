@@ -855,6 +855,8 @@ def run_serve(args, world, rank, device):
 
     torch.cuda.set_device(device)
     ctx = Context(device, wave_paths=args.wave_paths or SERVE_WAVE_PATHS, lanes=args.lanes)
+    if getattr(args, "share_rays", False):
+        ctx.set_ray_sharing(True)
     meshes = W.serve_pieces()
     pieces = [Piece(ctx, m) for m in meshes]
     cams, scenes = {}, {}
@@ -997,6 +999,7 @@ def run_serve(args, world, rank, device):
                        "offered_path_samples_per_s": offered, "step_path_samples": args.serve_step,
                        "step_path_samples_max": args.serve_step_max or 2 * args.serve_step,
                        "aging_ms": args.serve_aging_ms or 250, "overlap": not args.serve_no_overlap,
+                       "ray_sharing": bool(getattr(args, "share_rays", False)),
                        "max_pending": args.serve_max_pending,
                        "max_pending_path_samples": int(args.serve_max_pending_work * W.mean_request_path_samples()),
                        "tuning": tune_info,
