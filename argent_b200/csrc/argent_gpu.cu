@@ -1686,6 +1686,7 @@ static uint64_t blob_hash(const void* src, size_t bytes) {
 // added to `held`; null when the device is out of memory.
 static void* intern_blob(ArgentCtx* ctx, const void* src, size_t bytes, std::vector<void*>* held) {
   uint64_t h = blob_hash(src, bytes);
+  std::lock_guard<std::mutex> lock(ctx->blob_mu);
   for (auto& b : ctx->blobs) {
     if (b.hash == h && b.host.size() == bytes && std::memcmp(b.host.data(), src, bytes) == 0) {
       ++b.refs;
@@ -1708,6 +1709,7 @@ static void* intern_blob(ArgentCtx* ctx, const void* src, size_t bytes, std::vec
 }
 
 static void release_blob(ArgentCtx* ctx, void* dev) {
+  std::lock_guard<std::mutex> lock(ctx->blob_mu);
   for (size_t i = 0; i < ctx->blobs.size(); ++i) {
     if (ctx->blobs[i].dev != dev) continue;
     if (--ctx->blobs[i].refs == 0) {

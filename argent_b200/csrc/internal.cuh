@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -216,6 +217,7 @@ struct ArgentCtx {
     int refs = 0;
   };
   std::vector<SharedBlob> blobs;
+  std::mutex blob_mu;  // scenes may be uploaded and destroyed from several threads
   int num_sms = 148;
   int lanes = 8;
   // Launch tuning (argent_ctx_set_tuning / argent_autotune); 0 = default.
