@@ -84,14 +84,16 @@ def test_shared_batch_traces_fewer_rays():
 
 
 @pytest.mark.gpu
-def test_shared_batch_over_many_waves_matches_to_rounding():
+@pytest.mark.parametrize("wave_paths", [1 << 18, 1 << 17])
+def test_shared_batch_over_many_waves_matches_to_rounding(wave_paths):
     """Waves of 2^18 paths: alone each film takes two waves of 4 samples,
-    shared the three take eight waves of one sample each, so the film sums
+    shared the three take eight waves of one sample each; waves of 2^17
+    paths also split the shared renders' pixels into chunks.  The film sums
     group the same samples differently; they agree to float rounding."""
     from argent_b200.gpu import Context, Piece
 
     wl = W.ring_still()
-    ctx = Context(0, wave_paths=1 << 18)
+    ctx = Context(0, wave_paths=wave_paths)
     piece = Piece(ctx, wl.mesh)
     descs = variants(wl)
     alone = films_of(ctx, piece, descs, wl, 8, batch=False)
@@ -175,3 +177,20 @@ def test_served_variants_share_and_equal_their_renders_alone(overlap):
         assert np.allclose(a, a0, rtol=1e-5, atol=1e-7)
         assert np.allclose(n, n0, rtol=1e-5, atol=1e-6)
     srv.close()
+
+
+@pytest.mark.gpu
+def test_groups_hold_at_most_sixteen_renders():
+    """Seventeen variants (alloys repeated) of a 64 x 64 x 2 spp shot: a group
+    of sixteen and one render alone, every film bit for bit its render
+    alone."""
+    from argent_b200.gpu import Context, Piece
+
+    wl = W.ring_still(spp=2, width=64, height=64)
+    ctx = Context(0)
+    piece = Piece(ctx, wl.mesh)
+    alloys = ("sterling", "gold14k", "rose14k", "bronze") * 4 + ("platinum",)
+    descs = variants(wl, alloys)
+    alone = films_of(ctx, piece, descs, wl, 2, batch=False)
+    shared = films_of(ctx, piece, descs, wl, 2, share=True)
+    assert_films_equal(shared, alone)
