@@ -1082,7 +1082,9 @@ __global__ void __launch_bounds__(128, ARGENT_TRAV_BLOCKS) k_shadow(WaveArgs a, 
 // render) is alive with a bit-identical ray takes the leader's result, so
 // every shared ray is traced once.  Identical rays in identical geometry
 // have identical closest hits and identical visibility, so the records and
-// films equal those of tracing every ray.
+// films equal those of tracing every ray.  Likewise a hit on a surface whose
+// material (and everything else shading reads) equals the leader's, reached
+// in the leader's path state, takes the leader's shading.
 
 // The depth path `slot` was last continued to (0 from ray generation): it is
 // alive at `depth` exactly when this equals `depth`.
