@@ -1124,7 +1124,9 @@ bool same_traversal(const ArgentScene* a, const ArgentScene* b) {
 // whether the rest of what shading reads is equal (the scene descriptor but
 // for its materials, their classes and the film's camera matrix; the path
 // settings).  Environment tables and emission spectra of equal content are
-// one blob, so their pointers compare equal.
+// one blob, so their pointers compare equal.  The descriptors are zeroed
+// before they are filled, so their padding compares equal too; a mismatch
+// could only turn sharing off.
 void share_masks(const dev::DevJob& l, const ArgentScene* ls, const ArgentScene* fs, dev::DevJob* f) {
   std::memset(f->share_mat, 0, sizeof(f->share_mat));
   f->share_rest = 0;

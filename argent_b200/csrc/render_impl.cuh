@@ -1107,13 +1107,13 @@ __device__ __forceinline__ int hit_class(const DevScene* sc, const DevPiece& pc,
   return sc->mat_class[__ldg(&pc.tri_idx[kind].w)];
 }
 
-// Block-aggregated queue append for the streaming passes below: one atomic
-// per block and queue instead of one per warp (a pass over tens of millions
-// of entries is otherwise bound by the atomics on one counter).  Every
-// thread of the block must call it; `sw` is the block's scratch of
-// blockDim.x / 32 + 1 words.
-__device__ __forceinline__ void block_append(bool pred, uint32_t value, uint32_t* counter, uint32_t* queue,
-                                             uint32_t cap, uint32_t* status, uint32_t* sw) {
+// Block-aggregated reservation for the streaming passes below: the threads
+// of the block with `pred` set take consecutive positions behind `counter`
+// with one atomic per block (a pass over tens of millions of entries is
+// otherwise bound by the atomics on one counter); returns this thread's
+// position (meaningful where `pred` is set).  Every thread of the block must
+// call it; `sw` is the block's scratch of blockDim.x / 32 + 1 words.
+__device__ __forceinline__ uint32_t block_reserve(bool pred, uint32_t* counter, uint32_t* sw) {
   const unsigned m = __ballot_sync(0xffffffffu, pred);
   const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nw = blockDim.x >> 5;
   if (lane == 0) sw[warp] = (uint32_t)__popc(m);
@@ -1128,14 +1128,21 @@ __device__ __forceinline__ void block_append(bool pred, uint32_t value, uint32_t
     sw[nw] = total ? atomicAdd(counter, total) : 0u;
   }
   __syncthreads();
+  const uint32_t pos = sw[nw] + sw[warp] + (uint32_t)__popc(m & ((1u << lane) - 1u));
+  __syncthreads();  // sw is reused by the next reservation
+  return pos;
+}
+
+// Block-aggregated queue append (block_reserve, then the entry).
+__device__ __forceinline__ void block_append(bool pred, uint32_t value, uint32_t* counter, uint32_t* queue,
+                                             uint32_t cap, uint32_t* status, uint32_t* sw) {
+  const uint32_t pos = block_reserve(pred, counter, sw);
   if (pred) {
-    uint32_t pos = sw[nw] + sw[warp] + (uint32_t)__popc(m & ((1u << lane) - 1u));
     if (pos < cap)
       queue[pos] = value;
     else
       atomicOr(status, ARGENT_STATUS_QUEUE_OVERFLOW);
   }
-  __syncthreads();  // sw is reused by the next append
 }
 
 // Before k_intersect: splits the alive paths of `depth` into those that take
@@ -1248,24 +1255,9 @@ __global__ void __launch_bounds__(256) k_shade_copy(WaveArgs a, int depth) {
       rec = sr.x;
     }
     block_append(alive, slot, a.counters + CNT_ACT(depth + 1), a.q_out, a.cap, a.status, sw);
-    // The shadow record: a position reserved like a queue entry, then the
-    // leader's record with this path's slot.
-    const unsigned m = __ballot_sync(0xffffffffu, shadow);
-    const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, nw = blockDim.x >> 5;
-    if (lane == 0) sw[warp] = (uint32_t)__popc(m);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint32_t total = 0;
-      for (unsigned w = 0; w < nw; ++w) {
-        uint32_t c = sw[w];
-        sw[w] = total;
-        total += c;
-      }
-      sw[nw] = total ? atomicAdd(a.counters + CNT_SH(depth), total) : 0u;
-    }
-    __syncthreads();
+    // The shadow record: the leader's, with this path's slot.
+    const uint32_t pos = block_reserve(shadow, a.counters + CNT_SH(depth), sw);
     if (shadow) {
-      uint32_t pos = sw[nw] + sw[warp] + (uint32_t)__popc(m & ((1u << lane) - 1u));
       if (pos < a.cap) {
         float4 sd = a.sh_d[rec];
         a.sh_o[pos] = a.sh_o[rec];
@@ -1275,7 +1267,6 @@ __global__ void __launch_bounds__(256) k_shade_copy(WaveArgs a, int depth) {
         atomicOr(a.status, ARGENT_STATUS_QUEUE_OVERFLOW);
       }
     }
-    __syncthreads();
   }
 }
 
