@@ -1312,7 +1312,13 @@ static int run_jobs(ArgentCtx* ctx, const std::vector<dev::DevJob>& jobs, const 
   rc = ensure_lane_streams(ctx, ctx->lanes);
   if (rc != ARGENT_OK) return rc;
   const int nlanes = ctx->lanes;
-  const int start = ctx->next_lane % nlanes;
+  // A joined batch with no overlapped batch in flight starts on lane 0: every
+  // lane is idle once the context stream reaches it, and a fixed first lane
+  // keeps its captured graph reusable whatever ran before (a 1-wave render in
+  // between would otherwise shift the lanes and force a new capture).
+  // Overlapped batches continue the rotation, so consecutive ones spread
+  // over the lanes.
+  const int start = (done == nullptr && !ctx->overlapped_pending) ? 0 : ctx->next_lane % nlanes;
   const int used = (int)std::min<size_t>((size_t)nlanes, waves.size());
   for (int k = 0; k < used; ++k) {
     rc = ensure_wave(ctx, (start + k) % nlanes, cap);
