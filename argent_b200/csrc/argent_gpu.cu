@@ -1204,17 +1204,25 @@ std::vector<dev::WaveDesc> plan_waves(const std::vector<dev::DevJob>& jobs, cons
     if (P == 0 || count == 0) continue;
     uint32_t depth = 0;
     for (uint32_t j : g) depth = std::max(depth, jobs[j].max_depth);
-    uint32_t pn_max = (uint32_t)std::min<uint64_t>(P, cap / k);
+    // A group takes the samples per pixel and wave that one of its renders
+    // would take alone in an empty wave (sn1), on fewer pixels per wave: the
+    // film then sums every pixel's samples in the same runs as the render
+    // alone, so its values are the same bit for bit.
+    const uint64_t pn1 = std::min<uint64_t>(P, cap);
+    const uint64_t sn1 = k > 1 ? std::max<uint64_t>(1, std::min<uint64_t>(count, cap / pn1)) : count;
+    uint32_t pn_max = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(P, cap / (k * (k > 1 ? sn1 : 1))));
     for (uint32_t p0 = 0; p0 < P; p0 += pn_max) {
       uint32_t pn = std::min(pn_max, P - p0);
       uint32_t s0 = 0;
       while (s0 < count) {
         uint64_t room = cap - cur.num_slots;
-        if (room < k * pn || cur.num_segments + k > ARGENT_MAX_SEGMENTS) {
+        uint64_t want = k > 1 ? std::min<uint64_t>(count - s0, sn1) : 1;
+        if (room < k * pn * want || cur.num_segments + k > ARGENT_MAX_SEGMENTS) {
           flush();
           room = cap;
         }
         uint32_t sn = (uint32_t)std::min<uint64_t>(count - s0, room / (k * pn));
+        if (k > 1) sn = (uint32_t)std::min<uint64_t>(sn, sn1);
         const uint32_t lead = cur.num_slots;
         for (uint64_t m = 0; m < k; ++m) {
           dev::DevSegment& sg = cur.seg[cur.num_segments++];

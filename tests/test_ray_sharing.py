@@ -1,9 +1,9 @@
 """Ray sharing in batches (argent_ctx_set_ray_sharing): metal variants of
 one piece under the same camera, seed and samples trace each common ray
 once.  argent renders every variant on its own (jobs.rs:595-713), so the
-reference for each film is its render alone: bit-identical where the batch
-gives its samples the same wave segments, equal to float rounding of the
-film sums where it groups them into other waves."""
+reference for each film is its render alone, bit for bit: the batch gives
+each pixel the same runs of samples per wave as the render alone (served
+requests, whose chunks the scheduler sizes, agree to float rounding)."""
 
 import numpy as np
 import pytest
@@ -85,11 +85,11 @@ def test_shared_batch_traces_fewer_rays():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("wave_paths", [1 << 18, 1 << 17])
-def test_shared_batch_over_many_waves_matches_to_rounding(wave_paths):
-    """Waves of 2^18 paths: alone each film takes two waves of 4 samples,
-    shared the three take eight waves of one sample each; waves of 2^17
-    paths also split the shared renders' pixels into chunks.  The film sums
-    group the same samples differently; they agree to float rounding."""
+def test_shared_batch_over_many_waves_equals_renders_alone(wave_paths):
+    """Waves of 2^18 (2^17) paths: alone each film takes two (four) waves of
+    4 (2) samples per pixel; shared, the three renders take the same runs of
+    samples per pixel on a third of the pixels per wave, so every film is
+    still bit for bit its render alone."""
     from argent_b200.gpu import Context, Piece
 
     wl = W.ring_still()
@@ -98,11 +98,7 @@ def test_shared_batch_over_many_waves_matches_to_rounding(wave_paths):
     descs = variants(wl)
     alone = films_of(ctx, piece, descs, wl, 8, batch=False)
     shared = films_of(ctx, piece, descs, wl, 8, share=True)
-    for (x1, a1, n1), (x2, a2, n2) in zip(shared, alone):
-        scale = np.abs(x2).max()
-        assert np.abs(x1 - x2).max() <= 1e-5 * scale
-        assert np.abs(a1 - a2).max() <= 1e-5 * max(np.abs(a2).max(), 1.0)
-        assert np.abs(n1 - n2).max() <= 1e-5 * max(np.abs(n2).max(), 1.0)
+    assert_films_equal(shared, alone)
 
 
 @pytest.mark.gpu
