@@ -1214,10 +1214,17 @@ std::vector<dev::WaveDesc> plan_waves(const std::vector<dev::DevJob>& jobs, cons
     for (uint32_t p0 = 0; p0 < P; p0 += pn_max) {
       uint32_t pn = std::min(pn_max, P - p0);
       uint32_t s0 = 0;
+      // The wave (index into `waves` once flushed) holding this pixel
+      // chunk's previous run of samples: a wave never holds two runs of the
+      // same pixels of a render, since k_film adds a segment's sums to its
+      // pixels without atomics.  (A single render's runs fill their waves,
+      // so only a group's shorter runs need the check.)
+      size_t placed_in = ~size_t(0);
       while (s0 < count) {
         uint64_t room = cap - cur.num_slots;
         uint64_t want = k > 1 ? std::min<uint64_t>(count - s0, sn1) : 1;
-        if (room < k * pn * want || cur.num_segments + k > ARGENT_MAX_SEGMENTS) {
+        if (room < k * pn * want || cur.num_segments + k > ARGENT_MAX_SEGMENTS ||
+            (k > 1 && placed_in == waves.size())) {
           flush();
           room = cap;
         }
@@ -1236,6 +1243,7 @@ std::vector<dev::WaveDesc> plan_waves(const std::vector<dev::DevJob>& jobs, cons
           cur.num_slots += pn * sn;
         }
         cur_depth = std::max(cur_depth, depth);
+        placed_in = waves.size();
         s0 += sn;
       }
     }
