@@ -672,10 +672,11 @@ int argent_ctx_set_graphs(ArgentCtx* ctx, int on);
  * that ray's closest hit or shadow visibility instead of being traced again;
  * a first hit on a material whose record equals the first render's (the
  * studio floor) takes that render's shading too.
- * Every hit record and radiance sample equals the unshared render's; a
- * film's sums may group its samples differently (other waves), which moves
- * its values by float rounding only.  Costs 33 bytes per path slot per lane
- * in use. */
+ * Every hit record and radiance sample equals the unshared render's, and a
+ * batch's films equal each render's own argent_render_pass bit for bit (the
+ * waves give every pixel the same runs of samples); a serve step's chunks
+ * agree with the render alone to float rounding, as unshared ones do.  Costs
+ * 33 bytes per path slot per lane in use. */
 int argent_ctx_set_ray_sharing(ArgentCtx* ctx, int on);
 /* Traversal visit counters: on = count, and reset to zero. */
 int argent_ctx_set_counting(ArgentCtx* ctx, int on);
