@@ -1196,6 +1196,17 @@ std::vector<dev::WaveDesc> plan_waves(const std::vector<dev::DevJob>& jobs, cons
     cur = dev::WaveDesc{};
     cur_depth = 0;
   };
+  // k_film adds each segment's sums to its pixels without atomics, so a wave
+  // never holds two segments over the same pixels of one film: another run
+  // of the same render's pixels (a group's runs are shorter than a wave), or
+  // a later batch item rendering into the same film.
+  auto clashes = [&](uint32_t job, uint32_t p0, uint32_t pn) {
+    for (uint32_t i = 0; i < cur.num_segments; ++i) {
+      const dev::DevSegment& q = cur.seg[i];
+      if (jobs[q.job].film_xyz == jobs[job].film_xyz && q.p0 < p0 + pn && p0 < q.p0 + q.pn) return true;
+    }
+    return false;
+  };
   for (const std::vector<uint32_t>& g : groups) {
     const uint32_t j0 = g[0];
     const uint64_t k = g.size();
@@ -1214,17 +1225,12 @@ std::vector<dev::WaveDesc> plan_waves(const std::vector<dev::DevJob>& jobs, cons
     for (uint32_t p0 = 0; p0 < P; p0 += pn_max) {
       uint32_t pn = std::min(pn_max, P - p0);
       uint32_t s0 = 0;
-      // The wave (index into `waves` once flushed) holding this pixel
-      // chunk's previous run of samples: a wave never holds two runs of the
-      // same pixels of a render, since k_film adds a segment's sums to its
-      // pixels without atomics.  (A single render's runs fill their waves,
-      // so only a group's shorter runs need the check.)
-      size_t placed_in = ~size_t(0);
       while (s0 < count) {
         uint64_t room = cap - cur.num_slots;
         uint64_t want = k > 1 ? std::min<uint64_t>(count - s0, sn1) : 1;
-        if (room < k * pn * want || cur.num_segments + k > ARGENT_MAX_SEGMENTS ||
-            (k > 1 && placed_in == waves.size())) {
+        bool clash = false;
+        for (uint32_t j : g) clash = clash || clashes(j, p0, pn);
+        if (room < k * pn * want || cur.num_segments + k > ARGENT_MAX_SEGMENTS || clash) {
           flush();
           room = cap;
         }
@@ -1243,7 +1249,6 @@ std::vector<dev::WaveDesc> plan_waves(const std::vector<dev::DevJob>& jobs, cons
           cur.num_slots += pn * sn;
         }
         cur_depth = std::max(cur_depth, depth);
-        placed_in = waves.size();
         s0 += sn;
       }
     }

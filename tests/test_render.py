@@ -139,6 +139,26 @@ def test_batch_equals_separate_passes():
 
 
 @pytest.mark.gpu
+def test_batch_items_sharing_a_film_equal_sequential_passes():
+    """Two items of one batch render into the same film (3 then 5 samples):
+    the film equals two render_pass calls in a row bit for bit.  The second
+    item's pixels never share a wave with the first's, since the film pass
+    adds a segment's sums without atomics."""
+    from argent_b200.gpu import Context, Film, Piece, Scene, render_batch, render_pass
+
+    wl = W.ring_still()
+    ctx = Context(0)
+    piece = Piece(ctx, wl.mesh)
+    scene = Scene(ctx, piece, wl.desc)
+    f, g = Film(ctx, wl.width, wl.height), Film(ctx, wl.width, wl.height)
+    render_pass(ctx, scene, wl.camera, f, wl.settings, 3, 7)
+    render_pass(ctx, scene, wl.camera, f, wl.settings, 5, 7)
+    render_batch(ctx, [(scene, wl.camera, g, wl.settings, 3, 7), (scene, wl.camera, g, wl.settings, 5, 7)])
+    assert f.samples() == g.samples() == 8
+    assert np.array_equal(f.xyz().view(np.uint32), g.xyz().view(np.uint32))
+
+
+@pytest.mark.gpu
 def test_gems_render_matches_oracle():
     """The gems workload (diamond + ruby/sapphire/emerald/garnet in an 18k
     setting, white studio, depth 32) at reduced size: 108 x 192, 8 spp."""
