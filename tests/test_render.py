@@ -154,7 +154,7 @@ def test_batch_items_sharing_a_film_equal_sequential_passes():
     render_pass(ctx, scene, wl.camera, f, wl.settings, 3, 7)
     render_pass(ctx, scene, wl.camera, f, wl.settings, 5, 7)
     render_batch(ctx, [(scene, wl.camera, g, wl.settings, 3, 7), (scene, wl.camera, g, wl.settings, 5, 7)])
-    assert f.samples() == g.samples() == 8
+    assert f.samples == g.samples == 8
     assert np.array_equal(f.xyz().view(np.uint32), g.xyz().view(np.uint32))
 
 
