@@ -353,10 +353,14 @@ int argent_trace_anyhit_device(ArgentCtx* ctx, ArgentPiece* piece, const ArgentR
 /*
  * One item of a batch: a render_pass call.  The items of one batch run as
  * one persistent launch sequence in which waves of different items
- * overlap.  Each item's film receives exactly what argent_render_pass would
- * give for the same arguments.  Replaces the per-frame `render_image` loops
- * of `render_reel` (argent/src/jobs.rs:595-713) and `sheet_prepared`
- * (jobs.rs:857-889).
+ * overlap.  Each item's film receives the samples argent_render_pass would
+ * render for the same arguments, each bit for bit; the film adds them in
+ * runs per wave, so where the batch packs an item's samples into other runs
+ * (an item that starts in a wave another item began) its film values differ
+ * from argent_render_pass's by float rounding only.  Items may share a film:
+ * they render one after another, as consecutive argent_render_pass calls
+ * would.  Replaces the per-frame `render_image` loops of `render_reel`
+ * (argent/src/jobs.rs:595-713) and `sheet_prepared` (jobs.rs:857-889).
  */
 typedef struct ArgentBatchItem {
   ArgentScene* scene;
