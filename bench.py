@@ -1239,7 +1239,10 @@ def main():
                 import gc
 
                 gc.collect()  # the still's context and its path state go before the extras' contexts
-                out["forms"] = form_comparisons(args, local)
+                try:
+                    out["forms"] = form_comparisons(args, local)
+                except Exception as e:  # the measured line stands; the legs report what stopped them
+                    out["forms"] = {"error": f"{type(e).__name__}: {e}"}
             print(json.dumps(out), flush=True)
     finally:
         if world > 1:
