@@ -409,3 +409,18 @@ def test_fp64_oracle_film_matches_cpu_restatement_at_c1():
     e = rel_rmse(xyz_gpu, xyz / 256)
     print("FP64 film, ring 256x256x256 relRMSE XYZ vs CPU restatement:", e)
     assert np.all(e <= 2e-3), e
+
+
+def test_oracle_render_is_independent_of_its_thread_count():
+    """The CPU baseline renders pixels in parallel; each pixel's samples are
+    summed by one thread in sample order, so the film is the same bit for bit
+    on one thread and on four (a band of the ring still, 2 spp; CPU)."""
+    import oracle as O
+
+    wl = W.ring_still(spp=2, width=96, height=96)
+    sc = O.Scene(wl.mesh, wl.desc.c)
+    one = sc.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, 2, wl.seed, rows=(40, 56), threads=1)
+    four = sc.render_pass(wl.camera, wl.settings, wl.width, wl.height, 0, 2, wl.seed, rows=(40, 56), threads=4)
+    for a, b in zip(one, four):
+        assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+    assert np.abs(one[3][40:56]).sum() > 0 and np.abs(one[3][:40]).sum() == 0
